@@ -1,0 +1,230 @@
+/*
+ * pmg_b200.h -- C ABI of the B200 implementation of ParMooN's 3D scalar
+ * convection-diffusion hot path: finite-element assembly (Galerkin / SUPG /
+ * mass forms) into a host-defined CSR pattern, and the geometric-multigrid
+ * preconditioned flexible GMRES solve.
+ *
+ * The entry points take plain pointers and sizes only.  Every call returns 0
+ * (PMG_OK) or a negative PMG_ERR_* code; nothing calls exit().  A handle owns
+ * one CUDA stream and the device mirrors of everything it was given; the
+ * caller keeps ownership of its host arrays.  Calls on one handle are not
+ * thread-safe (the reference is single-threaded and non-reentrant too).
+ *
+ * Which reference interface each entry point stands in for is given beside
+ * it (paths relative to the ParMooN source tree).
+ */
+#ifndef PMG_B200_H
+#define PMG_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- codes */
+#define PMG_OK                   0
+#define PMG_ERR_ARG             -1  /* bad argument / size / ordering */
+#define PMG_ERR_CUDA            -2  /* CUDA runtime error (message via pmg_last_error) */
+#define PMG_ERR_STATE           -3  /* call out of order (e.g. solve before assemble) */
+#define PMG_ERR_NOT_CONVERGED   -4  /* iteration limit reached before the tolerance */
+#define PMG_ERR_DIVERGED        -5  /* residual grew beyond SC_DIV_FACTOR * r0 */
+#define PMG_ERR_SLOT            -6  /* element coupling missing from the CSR pattern */
+#define PMG_ERR_NONFINITE       -7  /* NaN/Inf detected in assembled data or residual */
+#define PMG_ERR_SINGULAR        -8  /* zero pivot in the coarsest-level factorisation */
+#define PMG_ERR_UNSUPPORTED     -9  /* element/form/coefficient combination not built */
+
+/* ------------------------------------------------------------ elements */
+/* Element families (reference: include/FE3D/BF_C_H_Q1_3D.h, BF_C_H_Q2_3D.h,
+ * BF_C_T_P1_3D.h, BF_C_T_P2_3D.h).  Local basis ordering follows the
+ * reference tables: hexahedra are tensor-ordered (x fastest) on the nodes of
+ * [-1,1]^3, tetrahedra follow the reference vertex/edge numbering. */
+#define PMG_ELEM_Q1_HEX   1   /*  8 local dofs */
+#define PMG_ELEM_Q2_HEX   2   /* 27 local dofs */
+#define PMG_ELEM_P1_TET  11   /*  4 local dofs */
+#define PMG_ELEM_P2_TET  12   /* 10 local dofs */
+
+/* Local forms (reference: src/FE/ConvDiff3D.C:87-214, src/FE/TCD3D.C:37-421). */
+#define PMG_FORM_GALERKIN     1  /* BilinearAssemble:   A = eps grad.grad + (b.grad u) v + c u v ; f v */
+#define PMG_FORM_SUPG         2  /* BilinearAssemble_SD: Galerkin + delta (b.grad u + c u)(b.grad v) */
+#define PMG_FORM_MASS         3  /* MatrixMRhsAssemble: M = u v ; f v */
+#define PMG_FORM_MASS_SUPG    4  /* MatrixMRhsAssemble_SUPG: M = u (v + delta b.grad v) ; f (v + delta b.grad v) */
+#define PMG_FORM_STIFF_SUPG   5  /* MatricesAKRhsAssemble_SUPG (A part): SUPG stiffness, rhs f (v + delta b.grad v) */
+
+/* Coefficient descriptors: the device-evaluable stand-in for the host
+ * CoeffFct3D callback (include/General/Constants.h:148-149).  Coefficient
+ * order follows the reference: c0=eps, c1..c3=b, c4=c (reaction), c5=f. */
+#define PMG_COEF_CONST        0  /* eps, b, c, f constant */
+#define PMG_COEF_SINE_RHS     1  /* Laplace.h: f = 3 pi^2 eps sin(pi x) sin(pi y) sin(pi z) */
+#define PMG_COEF_LOGNORMAL    2  /* eps(x) = exp(sum_k a_k cos(2 pi k.x + phi_k)) ; b, c, f constant */
+#define PMG_COEF_CURL_FOURIER 3  /* b = curl psi, psi = sum of Fourier modes (scaled) ; eps, c, f constant */
+#define PMG_COEF_ROTATING     4  /* b = (-(y-.5), x-.5, 0.2 sin(2 pi t)) ; eps, c, f constant */
+#define PMG_COEF_AMC          5  /* amc.h: eps=1, f=(3 pi^2 - 0.1) e^{-0.1 t} sin(pi x) cos(pi y) cos(pi z) */
+
+typedef struct pmg_coeff_desc {
+    int    kind;          /* PMG_COEF_* */
+    double eps;           /* c0 */
+    double b[3];          /* c1..c3 (constant kinds) / scale (curl kind: b[0]) */
+    double c;             /* c4 */
+    double f;             /* c5 (constant kinds) */
+    double t;             /* current time for time-dependent kinds */
+    int    n_modes;       /* Fourier modes for LOGNORMAL / CURL_FOURIER */
+    const double *modes;  /* n_modes x 8 doubles: kx ky kz amp phase ax ay az (host pointer, copied) */
+} pmg_coeff_desc;
+
+/* ------------------------------------------------------------ solver knobs */
+/* POD mirror of the TDatabase::ParamDB fields the reference reads on this
+ * path (src/General/Database.C:660-780).  pmg_default_params fills the
+ * reference defaults. */
+#define PMG_SMOOTHER_JACOBI   1
+#define PMG_SMOOTHER_SSOR     3
+#define PMG_SMOOTHER_LEARNED 30  /* stencil-network smoother with SSOR fallback */
+#define PMG_COARSE_SSOR       3
+#define PMG_COARSE_DIRECT    17  /* dense LU of the coarsest level (reference: SolveExact) */
+#define PMG_PREC_FP64         0  /* V-cycle stores level matrices and vectors in FP64 */
+#define PMG_PREC_FP32         1  /* V-cycle in FP32, outer FGMRES / true residual in FP64 */
+
+typedef struct pmg_params {
+    int    smoother;           /* SC_SMOOTHER_SCALAR */
+    int    pre_smooth;         /* SC_PRE_SMOOTH_SCALAR */
+    int    post_smooth;        /* SC_POST_SMOOTH_SCALAR */
+    int    coarse_smoother;    /* SC_COARSE_SMOOTHER_SCALAR */
+    int    coarse_maxit;       /* SC_COARSE_MAXIT_SCALAR */
+    double coarse_red;         /* SC_COARSE_RED_FACTOR_SCALAR */
+    double smooth_omega;       /* SC_SMOOTH_DAMP_FACTOR_SCALAR (Parameters[0]) */
+    double gmg_damp;           /* SC_GMG_DAMP_FACTOR_SCALAR */
+    double lin_red;            /* SC_LIN_RED_FACTOR_SCALAR  (stop when |r| < lin_red |r0|) */
+    double lin_res_min;        /* SC_LIN_RES_NORM_MIN_SCALAR (stop when |r| < lin_res_min) */
+    int    lin_maxit;          /* SC_LIN_MAXIT_SCALAR */
+    int    restart;            /* SC_GMRES_RESTART */
+    double div_factor;         /* SC_DIV_FACTOR */
+    int    precision;          /* PMG_PREC_* (V-cycle storage/compute precision) */
+    int    sdfem_type;         /* SDFEM_TYPE (2 supported) */
+    int    poly_degree;        /* INTERNAL_POLYNOMIAL_DEGREE used in the SUPG delta */
+    double delta0;             /* DELTA0 */
+    int    reference_restart_rule; /* 1: FGMRES restart resets r0 like FgmresIte.C:546-566; 0: always relative to the first r0 */
+} pmg_params;
+
+typedef struct pmg_solve_stats {
+    int    iterations;         /* FGMRES iterations (= V-cycles applied) */
+    double res0;               /* |b - A x0| (FP64, all rows) */
+    double res_final;          /* true |b - A x| recomputed in FP64 after the solve */
+    double rel_res;            /* res_final / res0 */
+    double mean_contraction;   /* (res_final/res0)^(1/iterations) */
+    int    smoother_used;      /* PMG_SMOOTHER_* actually used (learned may fall back) */
+    double seconds;            /* device time of the solve (CUDA events) */
+} pmg_solve_stats;
+
+typedef struct pmg_handle_s *pmg_handle;
+
+/* ------------------------------------------------------------ lifecycle */
+void        pmg_default_params(pmg_params *p);
+const char *pmg_last_error(void);
+int         pmg_device_count(int *n);
+
+/* TSystemCD3D ctor (src/System/SystemCD3D.C:62-227): creates the per-level
+ * containers; levels are numbered 0 (coarsest) .. n_levels-1 (finest). */
+int pmg_create(pmg_handle *h, int n_levels, const pmg_params *p);
+int pmg_destroy(pmg_handle h);
+int pmg_set_params(pmg_handle h, const pmg_params *p);
+
+/* ------------------------------------------------------------ mesh / space */
+/* TFESpace3D (src/FE/FESpace3D.C:81-239): element->dof map of one level in the
+ * reference's GlobalNumbers + BeginIndex form flattened to n_cells x n_loc,
+ * plus each cell's vertex coordinates in the cell's own vertex order
+ * (8 vertices for hexahedra, 4 for tetrahedra; n_cells x n_vert x 3).
+ * Affine maps only (HexaAffin, TetraAffin): parallelepipeds / tetrahedra.
+ * brick != 0 declares every hexahedron axis-aligned (needed for SUPG on hexes,
+ * whose convection-direction mesh size uses the physical trilinear interpolant). */
+int pmg_set_level_mesh(pmg_handle h, int level, int elem_type, int n_cells,
+                       const int *elem_dof, const double *cell_vert, int brick);
+
+/* TSquareStructure3D + Sort (src/FE/SquareStructure3D.C:58-527,
+ * src/FE/SquareStructure.C:91-110): the CSR pattern of one level, columns
+ * sorted ascending in each row, rows [active_bound, n_rows) Dirichlet (one
+ * diagonal entry each).  The device keeps a mirror; the host keeps ownership. */
+int pmg_set_level_csr(pmg_handle h, int level, int n_rows, int active_bound,
+                      const int *row_ptr, const int *kcol);
+
+/* Optional multicolour ordering of the rows of one level for the parallel
+ * SSOR (n_rows colour ids in [0, n_colors)).  Rows sharing a matrix entry
+ * must have different colours.  Without it a greedy colouring is built. */
+int pmg_set_level_row_colors(pmg_handle h, int level, int n_colors, const int *colors);
+
+/* Prolongation from level-1 to level (GetProlongationMatrix3D,
+ * src/FE/FEDatabase3D.C:1656-1815, averaged by dof multiplicity as in
+ * Prolongate, src/FE/MGComponents3D.C:208-488).  n_fine rows, CSR.
+ * Restriction is its transpose (DefectRestriction, :732-1014). */
+int pmg_set_transfer(pmg_handle h, int level, int n_fine, int n_coarse,
+                     const int *p_row_ptr, const int *p_col, const double *p_val);
+
+/* Dirichlet values of one level (the BoundValueFunct3D callback evaluated at
+ * the dof nodes, AssembleMat3D.C:1031-1081): n_rows - active_bound values. */
+int pmg_set_dirichlet_values(pmg_handle h, int level, const double *values);
+
+/* CoeffFct3D stand-in (include/General/Constants.h:148-149). */
+int pmg_set_coefficients(pmg_handle h, const pmg_coeff_desc *c);
+
+/* ------------------------------------------------------------ assembly */
+/* TAssembleMat3D::Reset + Assemble3D (src/System/AssembleMat3D.C:261-535,
+ * 751-857, 913-1200) for one level with one local form; the matrix and rhs
+ * stay on the device.  entries_out / rhs_out, when non-NULL, receive host
+ * copies (TSquareMatrix3D::GetEntries() consumers).  level = -1: all levels
+ * (TSystemCD3D::Assemble, src/System/SystemCD3D.C:340-365). */
+int pmg_assemble(pmg_handle h, int level, int form, double *entries_out, double *rhs_out);
+
+/* Copy a level's matrix (or rhs) between host and device. */
+int pmg_get_matrix(pmg_handle h, int level, int which, double *entries_out);
+int pmg_set_matrix(pmg_handle h, int level, int which, const double *entries);
+int pmg_get_rhs(pmg_handle h, int level, double *rhs_out);
+/* which: 0 = system matrix A, 1 = mass matrix M (time-dependent problems) */
+
+/* TSystemTCD3D::AssembleSystMat (src/System/SystemTCD3D.C:260-326):
+ *   rhs := tau*theta4*f_new + tau*theta3*f_old + (M - tau*theta2*A) u_old  (active rows)
+ *   A   := M + tau*theta1*A on every level (active rows), Dirichlet rows untouched.
+ * f_old/u_old are host arrays of the finest level (NULL: use the device copies
+ * kept from the previous step). */
+int pmg_tcd_system(pmg_handle h, double tau, const double theta[4],
+                   const double *f_old, const double *u_old, double *rhs_out);
+
+/* ------------------------------------------------------------ kernels */
+/* MatVect_Scalar / Defect_Scalar plug-ins (src/FE/Blas2.C:86-126) on the
+ * finest level's FP64 matrix: y = A x, r = b - A x.  Host arrays. */
+int pmg_matvec(pmg_handle h, int level, const double *x, double *y);
+int pmg_defect(pmg_handle h, int level, const double *x, const double *b, double *r, double *norm);
+
+/* One multicolour SSOR sweep pair (forward+backward) on a level, FP64
+ * (TMGLevel3D::SSOR, src/FE/MGLevel3D.C:363-467, in colour order). */
+int pmg_ssor(pmg_handle h, int level, const double *rhs, double *sol, int n_sweeps);
+
+/* Prolongate (P c) and restrict (P^T d) between level-1 and level. */
+int pmg_prolongate(pmg_handle h, int level, const double *coarse, double *fine);
+int pmg_restrict(pmg_handle h, int level, const double *fine, double *coarse);
+
+/* ------------------------------------------------------------ solve */
+/* TFgmresIte::Iterate with TMultiGridScaIte (src/FE/FgmresIte.C:245-624,
+ * src/FE/MultiGridScaIte.C:89-130) on the finest level.  sol is the start
+ * vector on input (its Dirichlet part is overwritten by the rhs like
+ * SetDirichletNodes) and the solution on output; rhs == NULL uses the
+ * device-resident assembled rhs; sol == NULL keeps the solution on the
+ * device (start vector = assembled Dirichlet values, zero elsewhere). */
+int pmg_solve(pmg_handle h, double *sol, const double *rhs, pmg_solve_stats *stats);
+
+/* Copy the device-resident finest-level solution out. */
+int pmg_get_solution(pmg_handle h, double *sol_out);
+
+/* ------------------------------------------------------------ learned smoother */
+/* Lattice description for the stencil-network smoother of one level: for
+ * each dof its (i,j,k) index on the level's node lattice (nx x ny x nz). */
+int pmg_set_level_lattice(pmg_handle h, int level, int nx, int ny, int nz, const int *dof_ijk);
+/* Network weights (BF16-stored, see pmg_learned_num_params for the layout). */
+int pmg_learned_num_params(int *n);
+int pmg_set_learned_weights(pmg_handle h, const float *weights);
+
+/* ------------------------------------------------------------ timing */
+/* Device time in seconds of the last pmg_assemble / pmg_solve call, and the
+ * device time of the dominant kernel of the last assembly (CUDA events). */
+int pmg_last_timings(pmg_handle h, double *assemble_s, double *solve_s, double *assemble_kernel_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PMG_B200_H */
