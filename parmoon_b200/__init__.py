@@ -1,0 +1,304 @@
+"""parmoon_b200 -- B200 implementation of ParMooN's 3D scalar convection-
+diffusion hot path (assembly + multigrid-preconditioned FGMRES), driven
+through the C ABI of ``libpmg_b200.so`` (include/pmg_b200.h).
+
+The Python layer is a thin ctypes binding used by the tests and the
+benchmark; the C++ host binding with the reference class names lives in
+``parmoon_b200/shim``.  There is no CPU fallback: every call runs the CUDA
+library, and importing this package fails loudly if the library cannot be
+loaded.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpmg_b200.so")
+
+# ------------------------------------------------------------------ constants
+OK = 0
+ERR = {-1: "ARG", -2: "CUDA", -3: "STATE", -4: "NOT_CONVERGED", -5: "DIVERGED", -6: "SLOT",
+       -7: "NONFINITE", -8: "SINGULAR", -9: "UNSUPPORTED"}
+Q1_HEX, Q2_HEX, P1_TET, P2_TET = 1, 2, 11, 12
+FORM_GALERKIN, FORM_SUPG, FORM_MASS, FORM_MASS_SUPG, FORM_STIFF_SUPG = 1, 2, 3, 4, 5
+COEF_CONST, COEF_SINE_RHS, COEF_LOGNORMAL, COEF_CURL_FOURIER, COEF_ROTATING, COEF_AMC = range(6)
+SMOOTHER_JACOBI, SMOOTHER_SSOR, SMOOTHER_LEARNED = 1, 3, 30
+COARSE_SSOR, COARSE_DIRECT = 3, 17
+PREC_FP64, PREC_FP32 = 0, 1
+
+_i, _d, _p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("smoother", _i), ("pre_smooth", _i), ("post_smooth", _i), ("coarse_smoother", _i),
+                ("coarse_maxit", _i), ("coarse_red", _d), ("smooth_omega", _d), ("gmg_damp", _d),
+                ("lin_red", _d), ("lin_res_min", _d), ("lin_maxit", _i), ("restart", _i), ("div_factor", _d),
+                ("precision", _i), ("sdfem_type", _i), ("poly_degree", _i), ("delta0", _d),
+                ("reference_restart_rule", _i)]
+
+
+class CoeffDesc(ctypes.Structure):
+    _fields_ = [("kind", _i), ("eps", _d), ("b", _d * 3), ("c", _d), ("f", _d), ("t", _d), ("n_modes", _i),
+                ("modes", _p)]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [("iterations", _i), ("res0", _d), ("res_final", _d), ("rel_res", _d), ("mean_contraction", _d),
+                ("smoother_used", _i), ("seconds", _d)]
+
+
+class PmgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"pmg error {code} ({ERR.get(code, '?')}): {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load libpmg_b200.so (built in-tree by parmoon_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} missing: run `python -m parmoon_b200.build`")
+        _lib = ctypes.CDLL(LIB_PATH)
+        _lib.pmg_last_error.restype = ctypes.c_char_p
+    return _lib
+
+
+def _check(rc):
+    if rc != OK:
+        raise PmgError(rc, lib().pmg_last_error().decode())
+    return rc
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_p)
+
+
+def _c_i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _c_f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def default_params(**kw):
+    p = Params()
+    lib().pmg_default_params(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def coeff(kind=COEF_CONST, eps=1.0, b=(0.0, 0.0, 0.0), c=0.0, f=1.0, t=0.0, modes=None):
+    d = CoeffDesc()
+    d.kind, d.eps, d.c, d.f, d.t = kind, eps, c, f, t
+    for k in range(3):
+        d.b[k] = b[k]
+    if modes is not None:
+        m = _c_f64(modes).reshape(-1, 8)
+        d.n_modes, d.modes = m.shape[0], m.ctypes.data_as(_p)
+        d._keep = m
+    return d
+
+
+class Handle:
+    """One multigrid hierarchy on the current CUDA device (TSystemCD3D analogue)."""
+
+    def __init__(self, n_levels, params=None):
+        self.h = _p()
+        self.params = params if params is not None else default_params()
+        _check(lib().pmg_create(ctypes.byref(self.h), _i(n_levels), ctypes.byref(self.params)))
+        self.n_levels = n_levels
+        self.sizes = [None] * n_levels
+
+    def close(self):
+        if self.h:
+            lib().pmg_destroy(self.h)
+            self.h = _p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, params):
+        self.params = params
+        _check(lib().pmg_set_params(self.h, ctypes.byref(params)))
+
+    def set_level_csr(self, level, rowptr, kcol, active_bound):
+        rowptr, kcol = _c_i32(rowptr), _c_i32(kcol)
+        n = rowptr.size - 1
+        _check(lib().pmg_set_level_csr(self.h, _i(level), _i(n), _i(active_bound), _ptr(rowptr), _ptr(kcol)))
+        self.sizes[level] = (n, int(rowptr[-1]), active_bound)
+
+    def set_level_mesh(self, level, elem_type, elem_dof, cell_vert, brick=False):
+        elem_dof, cell_vert = _c_i32(elem_dof), _c_f64(cell_vert)
+        nloc = {Q1_HEX: 8, Q2_HEX: 27, P1_TET: 4, P2_TET: 10}[elem_type]
+        n_cells = elem_dof.size // nloc
+        if cell_vert.size != n_cells * 24:
+            raise ValueError("cell_vert must hold 8 vertex slots x 3 coordinates per cell")
+        _check(lib().pmg_set_level_mesh(self.h, _i(level), _i(elem_type), _i(n_cells), _ptr(elem_dof),
+                                        _ptr(cell_vert), _i(int(brick))))
+
+    def set_row_colors(self, level, colors, n_colors):
+        colors = _c_i32(colors)
+        _check(lib().pmg_set_level_row_colors(self.h, _i(level), _i(n_colors), _ptr(colors)))
+
+    def set_transfer(self, level, p_rowptr, p_col, p_val, n_coarse):
+        p_rowptr, p_col, p_val = _c_i32(p_rowptr), _c_i32(p_col), _c_f64(p_val)
+        _check(lib().pmg_set_transfer(self.h, _i(level), _i(p_rowptr.size - 1), _i(n_coarse), _ptr(p_rowptr),
+                                      _ptr(p_col), _ptr(p_val)))
+
+    def set_dirichlet_values(self, level, values):
+        values = _c_f64(values)
+        _check(lib().pmg_set_dirichlet_values(self.h, _i(level), _ptr(values)))
+
+    def set_coefficients(self, desc):
+        self._coef = desc
+        _check(lib().pmg_set_coefficients(self.h, ctypes.byref(desc)))
+
+    def assemble(self, level, form, copy_out=True):
+        """Assemble one level (level=-1: all); returns (entries, rhs) host copies if copy_out."""
+        if level >= 0 and copy_out:
+            n, nnz, _ = self.sizes[level]
+            e = np.empty(nnz)
+            r = np.empty(n)
+            _check(lib().pmg_assemble(self.h, _i(level), _i(form), _ptr(e), _ptr(r)))
+            return e, r
+        _check(lib().pmg_assemble(self.h, _i(level), _i(form), None, None))
+        return None
+
+    def get_matrix(self, level, which=0):
+        e = np.empty(self.sizes[level][1])
+        _check(lib().pmg_get_matrix(self.h, _i(level), _i(which), _ptr(e)))
+        return e
+
+    def set_matrix(self, level, entries, which=0):
+        entries = _c_f64(entries)
+        _check(lib().pmg_set_matrix(self.h, _i(level), _i(which), _ptr(entries)))
+
+    def get_rhs(self, level):
+        r = np.empty(self.sizes[level][0])
+        _check(lib().pmg_get_rhs(self.h, _i(level), _ptr(r)))
+        return r
+
+    def matvec(self, level, x):
+        x = _c_f64(x)
+        y = np.empty(self.sizes[level][0])
+        _check(lib().pmg_matvec(self.h, _i(level), _ptr(x), _ptr(y)))
+        return y
+
+    def defect(self, level, x, b):
+        x, b = _c_f64(x), _c_f64(b)
+        r = np.empty(self.sizes[level][0])
+        nrm = _d()
+        _check(lib().pmg_defect(self.h, _i(level), _ptr(x), _ptr(b), _ptr(r), ctypes.byref(nrm)))
+        return r, nrm.value
+
+    def ssor(self, level, rhs, sol, n_sweeps=1):
+        sol = np.array(sol, dtype=np.float64)
+        rhs = _c_f64(rhs)
+        _check(lib().pmg_ssor(self.h, _i(level), _ptr(rhs), _ptr(sol), _i(n_sweeps)))
+        return sol
+
+    def prolongate(self, level, coarse):
+        coarse = _c_f64(coarse)
+        fine = np.empty(self.sizes[level][0])
+        _check(lib().pmg_prolongate(self.h, _i(level), _ptr(coarse), _ptr(fine)))
+        return fine
+
+    def restrict(self, level, fine):
+        fine = _c_f64(fine)
+        coarse = np.empty(self.sizes[level - 1][0])
+        _check(lib().pmg_restrict(self.h, _i(level), _ptr(fine), _ptr(coarse)))
+        return coarse
+
+    def solve(self, sol=None, rhs=None, raise_on_error=True):
+        """FGMRES + V-cycle on the finest level; returns (solution or None, stats, status)."""
+        st = SolveStats()
+        if sol is not None:
+            sol = np.array(sol, dtype=np.float64)
+        rhs = None if rhs is None else _c_f64(rhs)
+        rc = lib().pmg_solve(self.h, _ptr(sol), _ptr(rhs), ctypes.byref(st))
+        if raise_on_error and rc != OK:
+            _check(rc)
+        return sol, st, rc
+
+    def get_solution(self):
+        x = np.empty(self.sizes[-1][0])
+        _check(lib().pmg_get_solution(self.h, _ptr(x)))
+        return x
+
+    def timings(self):
+        a, s, k = _d(), _d(), _d()
+        _check(lib().pmg_last_timings(self.h, ctypes.byref(a), ctypes.byref(s), ctypes.byref(k)))
+        return a.value, s.value, k.value
+
+
+# ------------------------------------------------------------------ structured set-up (host, C++)
+def struct_level(elem, n, jitter=0.0, seed=0):
+    nc, N, nl = _i(), _i(), _i()
+    _check(lib().pmg_struct_sizes(_i(elem), _i(n), ctypes.byref(nc), ctypes.byref(N), ctypes.byref(nl)))
+    ed = np.empty(nc.value * nl.value, dtype=np.int32)
+    cv = np.empty(nc.value * 24, dtype=np.float64)
+    xyz = np.empty(N.value * 3, dtype=np.float64)
+    lat = np.empty(N.value, dtype=np.int32)
+    ab = _i()
+    _check(lib().pmg_struct_build(_i(elem), _i(n), _d(jitter), ctypes.c_ulonglong(seed), _ptr(ed), _ptr(cv),
+                                  _ptr(xyz), _ptr(lat), ctypes.byref(ab)))
+    rp = np.empty(N.value + 1, dtype=np.int32)
+    _check(lib().pmg_struct_csr(_i(nc.value), _i(nl.value), _ptr(ed), N, ab, _ptr(rp), None))
+    kc = np.empty(int(rp[-1]), dtype=np.int32)
+    _check(lib().pmg_struct_csr(_i(nc.value), _i(nl.value), _ptr(ed), N, ab, _ptr(rp), _ptr(kc)))
+    colors = np.empty(N.value, dtype=np.int32)
+    ncol = _i()
+    _check(lib().pmg_struct_row_colors(_i(elem), _i(n), N, _ptr(lat), _ptr(colors), ctypes.byref(ncol)))
+    return dict(elem=elem, n=n, elem_dof=ed, cell_vert=cv, dof_xyz=xyz.reshape(-1, 3), dof_lat=lat, N=N.value,
+                active_bound=ab.value, n_cells=nc.value, rowptr=rp, kcol=kc, colors=colors, n_colors=ncol.value)
+
+
+def struct_prolongation(elem, nc, lat_c, lat_f):
+    lat_c, lat_f = _c_i32(lat_c), _c_i32(lat_f)
+    rp = np.empty(lat_f.size + 1, dtype=np.int32)
+    _check(lib().pmg_struct_prolongation(_i(elem), _i(nc), _ptr(lat_c), _i(lat_c.size), _ptr(lat_f), _i(lat_f.size),
+                                         _ptr(rp), None, None))
+    col = np.empty(int(rp[-1]), dtype=np.int32)
+    val = np.empty(int(rp[-1]), dtype=np.float64)
+    _check(lib().pmg_struct_prolongation(_i(elem), _i(nc), _ptr(lat_c), _i(lat_c.size), _ptr(lat_f), _i(lat_f.size),
+                                         _ptr(rp), _ptr(col), _ptr(val)))
+    return rp, col, val
+
+
+def struct_hierarchy(elem, n_fine, n_levels, jitter=0.0, seed=0):
+    """Levels coarse..fine of the unit cube with n_fine cells per direction on the finest."""
+    levels = []
+    for l in range(n_levels):
+        n = n_fine >> (n_levels - 1 - l)
+        L = struct_level(elem, n, jitter=jitter if l == n_levels - 1 else 0.0, seed=seed)
+        if l > 0:
+            L["P"] = struct_prolongation(elem, n // 2, levels[-1]["dof_lat"], L["dof_lat"])
+        levels.append(L)
+    return levels
+
+
+def load_hierarchy(handle, levels, dirichlet=None, lattice_colors=True):
+    """Hand a struct_hierarchy to a Handle: CSR, mesh, row colours, transfers, Dirichlet values.
+
+    dirichlet: function (x, y, z) -> values on the Dirichlet dofs (default 0)."""
+    for l, L in enumerate(levels):
+        handle.set_level_csr(l, L["rowptr"], L["kcol"], L["active_bound"])
+        handle.set_level_mesh(l, L["elem"], L["elem_dof"], L["cell_vert"], brick=L["elem"] in (Q1_HEX, Q2_HEX))
+        if lattice_colors:
+            handle.set_row_colors(l, L["colors"], L["n_colors"])
+        if l > 0:
+            rp, col, val = L["P"]
+            handle.set_transfer(l, rp, col, val, levels[l - 1]["N"])
+        xyz = L["dof_xyz"][L["active_bound"]:]
+        vals = np.zeros(len(xyz)) if dirichlet is None else dirichlet(xyz[:, 0], xyz[:, 1], xyz[:, 2])
+        handle.set_dirichlet_values(l, vals)

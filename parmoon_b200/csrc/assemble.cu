@@ -1,0 +1,519 @@
+// Finite-element assembly on the device (sm_100a).
+//
+// Replaces TAssembleMat3D::Reset + Assemble3D (src/System/AssembleMat3D.C:261-535)
+// with its local forms (src/FE/ConvDiff3D.C:87-214, src/FE/TCD3D.C:37-266) and
+// the scatter AddLocalSqMatToGlobal / AddLocalRhsToGlobal (:751-857, :913-1096).
+//
+// Layout and schedule:
+//   * elements are stored in colour order; the elements of one colour share
+//     no degree of freedom, so one launch per colour scatters without atomics;
+//   * a group of NLOC lanes handles one element (Q2: 27 lanes = one element
+//     per warp; Q1: 4 elements per warp; P2: 3; P1: 8);
+//   * the reference-element table u_l(q) = (d/dxi, d/deta, d/dzeta, value) of
+//     every basis function at every quadrature point lives in shared memory;
+//   * per quadrature point the form is a 4x4 matrix D_q acting on u
+//     (A_ij = sum_q u_i(q)^T D_q u_j(q)); lane j owns column j of the local
+//     matrix and accumulates all NLOC rows in registers;
+//   * the element -> CSR slot map (precomputed once per mesh by binary search
+//     in the sorted rows, replacing the linear search of AssembleMat3D.C:795-817)
+//     turns the scatter into plain loads/stores.
+#include "pmg_internal.h"
+#include "fe_tables.h"
+#include <cstdio>
+
+namespace pmg {
+
+// ----------------------------------------------------------------- coefficients
+// Device stand-in for the CoeffFct3D callback; c[0..6] = eps, b1, b2, b3, c, f, |b|.
+struct CoefDev {
+  int kind;
+  double eps, b[3], c, f, t;
+  int n_modes;
+  const double *modes;
+};
+
+__device__ __forceinline__ void coeff_eval(const CoefDev &C, double x, double y, double z, double *c) {
+  const double PI = 3.14159265358979323846;
+  c[0] = C.eps; c[1] = C.b[0]; c[2] = C.b[1]; c[3] = C.b[2]; c[4] = C.c; c[5] = C.f;
+  switch (C.kind) {
+    case PMG_COEF_SINE_RHS:
+      c[5] = 3 * PI * PI * C.eps * sin(PI * x) * sin(PI * y) * sin(PI * z);
+      break;
+    case PMG_COEF_LOGNORMAL: {
+      double g = 0;
+      for (int m = 0; m < C.n_modes; m++) {
+        const double *M = C.modes + 8 * m;
+        g += M[3] * cos(2 * PI * (M[0] * x + M[1] * y + M[2] * z) + M[4]);
+      }
+      c[0] = C.eps * exp(g);
+      break;
+    }
+    case PMG_COEF_CURL_FOURIER: {
+      double bx = 0, by = 0, bz = 0;
+      for (int m = 0; m < C.n_modes; m++) {
+        const double *M = C.modes + 8 * m;
+        double arg = 2 * PI * (M[0] * x + M[1] * y + M[2] * z) + M[4];
+        double s = -M[3] * sin(arg) * 2 * PI;
+        double gx = s * M[0], gy = s * M[1], gz = s * M[2];
+        bx += gy * M[7] - gz * M[6];
+        by += gz * M[5] - gx * M[7];
+        bz += gx * M[6] - gy * M[5];
+      }
+      c[1] = C.b[0] * bx; c[2] = C.b[0] * by; c[3] = C.b[0] * bz;
+      break;
+    }
+    case PMG_COEF_ROTATING:
+      c[1] = -(y - 0.5); c[2] = x - 0.5; c[3] = 0.2 * sin(2 * PI * C.t);
+      break;
+    case PMG_COEF_AMC:
+      c[0] = 1.0; c[1] = c[2] = c[3] = 0; c[4] = 0;
+      c[5] = (3. * PI * PI - 0.1) * exp(-0.1 * C.t) * sin(PI * x) * cos(PI * y) * cos(PI * z);
+      break;
+    default:
+      break;
+  }
+  c[6] = sqrt(c[1] * c[1] + c[2] * c[2] + c[3] * c[3]);
+}
+
+// SDFEM_TYPE 2 (src/FE/ConvDiff.C:591-611)
+__device__ __forceinline__ double sdfem_delta(double h, double eps, double b1, double b2, double b3, int poly,
+                                              double delta0) {
+  if (fabs(eps) < 1e-20) eps = 1e-20;
+  double nb = sqrt(b1 * b1 + b2 * b2 + b3 * b3);
+  if (!(nb > 0)) return 0.0;
+  double nu = 1.0 / poly;
+  double alpha = nu * nb * h / (2 * eps);
+  return delta0 * nu * h * (1 / tanh(alpha) - 1 / alpha) / (2 * nb);
+}
+
+// Mesh size in convection direction (src/FE/ConvDiff.C:373-470):
+// 2|b| / sum_i |b . grad phi_i(barycentre)| over the vertex basis.
+// Tetrahedra: phi_i are the barycentric coordinates (gradients from J^{-1}).
+// Axis-aligned bricks: phi_i trilinear, gradient at the centre (+-1/(4hx), ..).
+// Other hexahedra: the physical-coordinate trilinear interpolant is solved for.
+__device__ double hk_convection(bool hex, bool brick, const double *cv, const double *Ji, double b1, double b2,
+                                double b3) {
+  double nb = sqrt(b1 * b1 + b2 * b2 + b3 * b3), den = 0;
+  if (!hex) {
+    double g[4][3];
+    for (int a = 0; a < 3; a++) {
+      g[a + 1][0] = Ji[a * 3 + 0]; g[a + 1][1] = Ji[a * 3 + 1]; g[a + 1][2] = Ji[a * 3 + 2];
+    }
+    for (int d = 0; d < 3; d++) g[0][d] = -(g[1][d] + g[2][d] + g[3][d]);
+    for (int i = 0; i < 4; i++) den += fabs(b1 * g[i][0] + b2 * g[i][1] + b3 * g[i][2]);
+  } else if (brick) {
+    double hx = cv[3] - cv[0], hy = cv[10] - cv[1], hz = cv[14] - cv[2];  // v1-v0 (x), v3-v0 (y), v4-v0 (z)
+    double px = b1 / hx, py = b2 / hy, pz = b3 / hz;
+    den = 0.5 * (fabs(px + py + pz) + fabs(px + py - pz) + fabs(px - py + pz) + fabs(px - py - pz));
+  } else {
+    // general hexahedron: invert the 8x8 monomial matrix (1,x,y,z,xy,xz,yz,xyz)
+    double A[8][16], sx = 0, sy = 0, sz = 0;
+    for (int v = 0; v < 8; v++) {
+      double x = cv[3 * v], y = cv[3 * v + 1], z = cv[3 * v + 2];
+      sx += x; sy += y; sz += z;
+      double m[8] = {1, x, y, z, x * y, x * z, y * z, x * y * z};
+      for (int k = 0; k < 8; k++) { A[v][k] = m[k]; A[v][8 + k] = (k == v) ? 1.0 : 0.0; }
+    }
+    sx *= 0.125; sy *= 0.125; sz *= 0.125;
+    for (int k = 0; k < 8; k++) {
+      int p = k;
+      for (int i = k + 1; i < 8; i++) if (fabs(A[i][k]) > fabs(A[p][k])) p = i;
+      if (p != k) for (int j = 0; j < 16; j++) { double t = A[k][j]; A[k][j] = A[p][j]; A[p][j] = t; }
+      double inv = 1.0 / A[k][k];
+      for (int j = 0; j < 16; j++) A[k][j] *= inv;
+      for (int i = 0; i < 8; i++)
+        if (i != k) {
+          double f = A[i][k];
+          for (int j = 0; j < 16; j++) A[i][j] -= f * A[k][j];
+        }
+    }
+    for (int i = 0; i < 8; i++) {
+      double c1 = A[1][8 + i], c2 = A[2][8 + i], c3 = A[3][8 + i], c4 = A[4][8 + i], c5 = A[5][8 + i],
+             c6 = A[6][8 + i], c7 = A[7][8 + i];
+      double val = b1 * (c1 + c4 * sy + c5 * sz + c7 * sy * sz);
+      val += b2 * (c2 + c4 * sx + c6 * sz + c7 * sx * sz);
+      val += b3 * (c3 + c5 * sx + c6 * sy + c7 * sx * sy);
+      den += fabs(val);
+    }
+  }
+  if (den < 1e-10) {
+    // fall back to the cell diameter (CELL_MEASURE default branch)
+    int nv = hex ? 8 : 4;
+    double hK = 0;
+    for (int a = 0; a < nv; a++)
+      for (int b = a + 1; b < nv; b++) {
+        double dx = cv[3 * a] - cv[3 * b], dy = cv[3 * a + 1] - cv[3 * b + 1], dz = cv[3 * a + 2] - cv[3 * b + 2];
+        hK = fmax(hK, sqrt(dx * dx + dy * dy + dz * dz));
+      }
+    return hK;
+  }
+  return 2 * nb / den;
+}
+
+// ----------------------------------------------------------------- kernel
+template <int E> struct ET;
+template <> struct ET<PMG_ELEM_Q1_HEX> { static constexpr int NLOC = 8, NV = 8; static constexpr bool HEX = true; };
+template <> struct ET<PMG_ELEM_Q2_HEX> { static constexpr int NLOC = 27, NV = 8; static constexpr bool HEX = true; };
+template <> struct ET<PMG_ELEM_P1_TET> { static constexpr int NLOC = 4, NV = 4; static constexpr bool HEX = false; };
+template <> struct ET<PMG_ELEM_P2_TET> { static constexpr int NLOC = 10, NV = 4; static constexpr bool HEX = false; };
+
+constexpr int ASM_WARPS = 8;
+
+struct AsmArgs {
+  int n_elems;              // elements of this colour
+  const int *elem_dof;      // colour-sorted, n x NLOC (already offset to the colour)
+  const double *cell_vert;  // n x NV x 3
+  const int *slot;          // n x NLOC x NLOC
+  int Na;
+  double *entries, *rhs;
+  int form, poly, brick;
+  double delta0;
+  CoefDev coef;
+  const double *utab;  // NQ x NLOC x 4
+  const double *qtab;  // NQ x 4 : weight, xi, eta, zeta
+  int *flags;
+};
+
+template <int E, int NQ>
+__global__ void __launch_bounds__(ASM_WARPS * 32) k_assemble(AsmArgs a) {
+  constexpr int NLOC = ET<E>::NLOC, NV = ET<E>::NV, GPW = 32 / NLOC;
+  constexpr bool HEX = ET<E>::HEX;
+  constexpr int GS = NQ * 20;  // per-element scratch: D_q (16) + F_q (4)
+  extern __shared__ double sm[];
+  double *sU = sm;
+  double *sQ = sU + NQ * NLOC * 4;
+  double *sG = sQ + NQ * 4;
+  for (int k = threadIdx.x; k < NQ * NLOC * 4; k += blockDim.x) sU[k] = a.utab[k];
+  for (int k = threadIdx.x; k < NQ * 4; k += blockDim.x) sQ[k] = a.qtab[k];
+  __syncthreads();
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = lane / NLOC, t = lane - grp * NLOC;
+  const bool lane_used = grp < GPW;
+  double *G = sG + (size_t)(warp * GPW + (lane_used ? grp : 0)) * GS;
+  const bool supg = (a.form == PMG_FORM_SUPG || a.form == PMG_FORM_MASS_SUPG || a.form == PMG_FORM_STIFF_SUPG);
+
+  for (int base = (blockIdx.x * ASM_WARPS + warp) * GPW; base < a.n_elems; base += gridDim.x * ASM_WARPS * GPW) {
+    const int e = base + grp;
+    const bool valid = lane_used && e < a.n_elems;
+    if (valid) {
+      const double *cv = a.cell_vert + (size_t)e * NV * 3;
+      double J[9], x0[3];
+      if (HEX) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          J[d * 3 + 0] = (cv[3 + d] - cv[d]) * 0.5;
+          J[d * 3 + 1] = (cv[9 + d] - cv[d]) * 0.5;
+          J[d * 3 + 2] = (cv[12 + d] - cv[d]) * 0.5;
+          x0[d] = (cv[3 + d] + cv[9 + d] + cv[12 + d] - cv[d]) * 0.5;
+        }
+      } else {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          J[d * 3 + 0] = cv[3 + d] - cv[d];
+          J[d * 3 + 1] = cv[6 + d] - cv[d];
+          J[d * 3 + 2] = cv[9 + d] - cv[d];
+          x0[d] = cv[d];
+        }
+      }
+      double det = J[0] * J[4] * J[8] + J[1] * J[5] * J[6] + J[2] * J[3] * J[7] - J[2] * J[4] * J[6] -
+                   J[1] * J[3] * J[8] - J[0] * J[5] * J[7];
+      double rd = 1.0 / det, Ji[9];
+      Ji[0] = (J[4] * J[8] - J[5] * J[7]) * rd;
+      Ji[1] = (J[2] * J[7] - J[1] * J[8]) * rd;
+      Ji[2] = (J[1] * J[5] - J[2] * J[4]) * rd;
+      Ji[3] = (J[5] * J[6] - J[3] * J[8]) * rd;
+      Ji[4] = (J[0] * J[8] - J[2] * J[6]) * rd;
+      Ji[5] = (J[2] * J[3] - J[0] * J[5]) * rd;
+      Ji[6] = (J[3] * J[7] - J[4] * J[6]) * rd;
+      Ji[7] = (J[1] * J[6] - J[0] * J[7]) * rd;
+      Ji[8] = (J[0] * J[4] - J[1] * J[3]) * rd;
+      const double adet = fabs(det);
+      // K = Ji Ji^T (diffusion in reference gradients)
+      double K[9];
+#pragma unroll
+      for (int p = 0; p < 3; p++)
+#pragma unroll
+        for (int q = 0; q < 3; q++)
+          K[p * 3 + q] = Ji[p * 3 + 0] * Ji[q * 3 + 0] + Ji[p * 3 + 1] * Ji[q * 3 + 1] + Ji[p * 3 + 2] * Ji[q * 3 + 2];
+      double hconv = 0;
+      if (supg) {
+        // the reference caches the convection-direction size from the first
+        // quadrature point's b for the whole cell (ConvDiff.C:376-383)
+        double X = x0[0] + J[0] * sQ[1] + J[1] * sQ[2] + J[2] * sQ[3];
+        double Y = x0[1] + J[3] * sQ[1] + J[4] * sQ[2] + J[5] * sQ[3];
+        double Z = x0[2] + J[6] * sQ[1] + J[7] * sQ[2] + J[8] * sQ[3];
+        double c[7];
+        coeff_eval(a.coef, X, Y, Z, c);
+        hconv = hk_convection(HEX, a.brick != 0, cv, Ji, c[1], c[2], c[3]);
+      }
+      for (int q = t; q < NQ; q += NLOC) {
+        const double xi = sQ[q * 4 + 1], eta = sQ[q * 4 + 2], zeta = sQ[q * 4 + 3];
+        double X = x0[0] + J[0] * xi + J[1] * eta + J[2] * zeta;
+        double Y = x0[1] + J[3] * xi + J[4] * eta + J[5] * zeta;
+        double Z = x0[2] + J[6] * xi + J[7] * eta + J[8] * zeta;
+        double c[7];
+        coeff_eval(a.coef, X, Y, Z, c);
+        const double mult = sQ[q * 4] * adet;
+        double delta = supg ? sdfem_delta(hconv, c[0], c[1], c[2], c[3], a.poly, a.delta0) : 0.0;
+        double bh[3];  // b in reference gradients: b . (Ji^T g^) = (Ji b) . g^
+#pragma unroll
+        for (int p = 0; p < 3; p++) bh[p] = Ji[p * 3 + 0] * c[1] + Ji[p * 3 + 1] * c[2] + Ji[p * 3 + 2] * c[3];
+        double D[16];
+#pragma unroll
+        for (int k = 0; k < 16; k++) D[k] = 0.0;
+        if (a.form == PMG_FORM_MASS || a.form == PMG_FORM_MASS_SUPG) {
+          D[15] = 1.0;
+          if (a.form == PMG_FORM_MASS_SUPG)
+#pragma unroll
+            for (int p = 0; p < 3; p++) D[p * 4 + 3] = delta * bh[p];
+        } else {
+#pragma unroll
+          for (int p = 0; p < 3; p++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) D[p * 4 + r] = c[0] * K[p * 3 + r] + (supg ? delta * bh[p] * bh[r] : 0.0);
+#pragma unroll
+          for (int r = 0; r < 3; r++) D[12 + r] = bh[r];
+          D[15] = c[4];
+          if (supg)
+#pragma unroll
+            for (int p = 0; p < 3; p++) D[p * 4 + 3] = delta * c[4] * bh[p];
+        }
+        double *Gq = G + q * 20;
+#pragma unroll
+        for (int k = 0; k < 16; k++) Gq[k] = D[k] * mult;
+        const double fm = mult * c[5];
+        const bool supg_rhs = supg;
+        Gq[16] = supg_rhs ? fm * delta * bh[0] : 0.0;
+        Gq[17] = supg_rhs ? fm * delta * bh[1] : 0.0;
+        Gq[18] = supg_rhs ? fm * delta * bh[2] : 0.0;
+        Gq[19] = fm;
+      }
+    }
+    __syncwarp();
+    if (valid) {
+      double acc[NLOC];
+#pragma unroll
+      for (int i = 0; i < NLOC; i++) acc[i] = 0.0;
+      double racc = 0.0;
+      for (int q = 0; q < NQ; q++) {
+        const double *uj = sU + (q * NLOC + t) * 4;
+        const double *Dq = G + q * 20;
+        const double u0 = uj[0], u1 = uj[1], u2 = uj[2], u3 = uj[3];
+        const double T0 = Dq[0] * u0 + Dq[1] * u1 + Dq[2] * u2 + Dq[3] * u3;
+        const double T1 = Dq[4] * u0 + Dq[5] * u1 + Dq[6] * u2 + Dq[7] * u3;
+        const double T2 = Dq[8] * u0 + Dq[9] * u1 + Dq[10] * u2 + Dq[11] * u3;
+        const double T3 = Dq[12] * u0 + Dq[13] * u1 + Dq[14] * u2 + Dq[15] * u3;
+        racc += Dq[16] * u0 + Dq[17] * u1 + Dq[18] * u2 + Dq[19] * u3;
+        const double *ui = sU + q * NLOC * 4;
+#pragma unroll
+        for (int i = 0; i < NLOC; i++) {
+          const double2 p01 = *reinterpret_cast<const double2 *>(ui + i * 4);
+          const double2 p23 = *reinterpret_cast<const double2 *>(ui + i * 4 + 2);
+          acc[i] += p01.x * T0 + p01.y * T1 + p23.x * T2 + p23.y * T3;
+        }
+      }
+      // scatter through the slot map (no two elements of a colour share a row)
+      const int *dof = a.elem_dof + (size_t)e * NLOC;
+      const int *sl = a.slot + (size_t)e * NLOC * NLOC;
+      int bad = 0;
+#pragma unroll
+      for (int i = 0; i < NLOC; i++) {
+        const int di = __ldg(dof + i);
+        const int s = __ldg(sl + i * NLOC + t);
+        if (di < a.Na) {
+          if (s >= 0) a.entries[s] += acc[i];
+          else bad = 1;
+        } else if (i == t && s >= 0) {
+          a.entries[s] = 1.0;  // Dirichlet row: unit diagonal (AssembleMat3D.C:840-848)
+        }
+      }
+      if (a.rhs) {
+        const int dt = __ldg(dof + t);
+        if (dt < a.Na) a.rhs[dt] += racc;
+      }
+      if (bad) atomicOr(a.flags, 1);
+    }
+    __syncwarp();
+  }
+}
+
+// ----------------------------------------------------------------- slot map
+// slot[e][i][j] = position of column dof_j in the sorted CSR row dof_i
+// (-1 where the row is a Dirichlet row and j != i, or the pair is missing).
+__global__ void k_slot_map(int n_cells, int nloc, int Na, const int *__restrict__ elem_dof,
+                           const int *__restrict__ rowptr, const int *__restrict__ kcol, int *__restrict__ slot,
+                           int *flags) {
+  size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  size_t total = (size_t)n_cells * nloc * nloc;
+  if (tid >= total) return;
+  int e = (int)(tid / (nloc * nloc));
+  int r = (int)(tid % (nloc * nloc));
+  int i = r / nloc, j = r % nloc;
+  int row = elem_dof[(size_t)e * nloc + i], col = elem_dof[(size_t)e * nloc + j];
+  int lo = rowptr[row], hi = rowptr[row + 1] - 1, pos = -1;
+  while (lo <= hi) {
+    int mid = (lo + hi) >> 1, v = kcol[mid];
+    if (v == col) { pos = mid; break; }
+    if (v < col) lo = mid + 1; else hi = mid - 1;
+  }
+  if (pos < 0 && row < Na) atomicOr(flags, 2);
+  slot[tid] = pos;
+}
+
+int build_slot_map(Handle &h, Level &L) {
+  size_t total = (size_t)L.n_cells * L.nloc * L.nloc;
+  PMG_TRY(L.slot.alloc(total));
+  PMG_CUDA(cudaMemsetAsync(h.d_flags.p, 0, sizeof(int) * 4, h.stream));
+  int bs = 256;
+  size_t nb = (total + bs - 1) / bs;
+  k_slot_map<<<(unsigned)nb, bs, 0, h.stream>>>(L.n_cells, L.nloc, L.Na, L.elem_dof.p, L.rowptr.p, L.kcol.p,
+                                                   L.slot.p, h.d_flags.p);
+  PMG_CUDA(cudaGetLastError());
+  int flags[4];
+  PMG_CUDA(cudaMemcpyAsync(flags, h.d_flags.p, sizeof(flags), cudaMemcpyDeviceToHost, h.stream));
+  PMG_CUDA(cudaStreamSynchronize(h.stream));
+  if (flags[0] & 2) {
+    set_error("element coupling missing from the CSR pattern (AssembleMat3D.C:811-816 case)");
+    return PMG_ERR_SLOT;
+  }
+  return PMG_OK;
+}
+
+// ----------------------------------------------------------------- tables cache
+struct TableCache {
+  int elem = -1, rule = -1;
+  DBuf<double> utab, qtab;
+  int nq = 0;
+};
+static TableCache g_tab[4];
+
+static int rule_for(int elem) {
+  switch (elem) {
+    case PMG_ELEM_Q1_HEX: return RULE_GAUSS2;
+    case PMG_ELEM_Q2_HEX: return RULE_GAUSS3;
+    case PMG_ELEM_P1_TET: return RULE_KEAST4;
+    default: return RULE_KEAST11;
+  }
+}
+
+static int get_tables(int elem, int rule, TableCache *&out) {
+  int slot = elem == PMG_ELEM_Q1_HEX ? 0 : elem == PMG_ELEM_Q2_HEX ? 1 : elem == PMG_ELEM_P1_TET ? 2 : 3;
+  TableCache &T = g_tab[slot];
+  if (T.elem != elem || T.rule != rule) {
+    QuadRule q = make_rule(rule);
+    int nl = elem_nloc(elem);
+    std::vector<double> u((size_t)q.n * nl * 4), qt((size_t)q.n * 4);
+    for (int k = 0; k < q.n; k++) {
+      basis_eval(elem, q.x[k], q.y[k], q.z[k], &u[(size_t)k * nl * 4]);
+      qt[k * 4] = q.w[k]; qt[k * 4 + 1] = q.x[k]; qt[k * 4 + 2] = q.y[k]; qt[k * 4 + 3] = q.z[k];
+    }
+    PMG_TRY(T.utab.upload(u.data(), u.size(), 0));
+    PMG_TRY(T.qtab.upload(qt.data(), qt.size(), 0));
+    PMG_CUDA(cudaDeviceSynchronize());
+    T.elem = elem; T.rule = rule; T.nq = q.n;
+  }
+  out = &T;
+  return PMG_OK;
+}
+
+template <int E, int NQ>
+static int launch_assemble(Handle &h, Level &L, AsmArgs a) {
+  constexpr int NLOC = ET<E>::NLOC, GPW = 32 / NLOC;
+  size_t smem = sizeof(double) * ((size_t)NQ * NLOC * 4 + NQ * 4 + (size_t)ASM_WARPS * GPW * NQ * 20);
+  static bool attr_set = false;
+  if (!attr_set) {
+    PMG_CUDA(cudaFuncSetAttribute(k_assemble<E, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  int per_block = ASM_WARPS * GPW;
+  const int *ed0 = a.elem_dof;
+  const double *cv0 = a.cell_vert;
+  const int *sl0 = a.slot;
+  for (size_t c = 0; c + 1 < L.ecolor_ptr.size(); c++) {
+    int beg = L.ecolor_ptr[c], n = L.ecolor_ptr[c + 1] - beg;
+    if (n <= 0) continue;
+    AsmArgs b = a;
+    b.n_elems = n;
+    b.elem_dof = ed0 + (size_t)beg * NLOC;
+    b.cell_vert = cv0 + (size_t)beg * ET<E>::NV * 3;
+    b.slot = sl0 + (size_t)beg * NLOC * NLOC;
+    int blocks = (n + per_block - 1) / per_block;
+    int cap = h.num_sms * 8;
+    if (blocks > cap) blocks = cap;
+    k_assemble<E, NQ><<<blocks, ASM_WARPS * 32, smem, h.stream>>>(b);
+    PMG_CUDA(cudaGetLastError());
+  }
+  return PMG_OK;
+}
+
+// Assemble one level into `target` (A or M) and rhs_target (may be NULL).
+int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs, double *rhs_target) {
+  if (!L.has_mesh || !L.has_csr) {
+    set_error("assemble: level needs pmg_set_level_mesh and pmg_set_level_csr first");
+    return PMG_ERR_STATE;
+  }
+  if (form < PMG_FORM_GALERKIN || form > PMG_FORM_STIFF_SUPG) {
+    set_error("assemble: unknown form");
+    return PMG_ERR_ARG;
+  }
+  if ((form == PMG_FORM_SUPG || form == PMG_FORM_MASS_SUPG || form == PMG_FORM_STIFF_SUPG) &&
+      h.prm.sdfem_type != 2) {
+    set_error("assemble: only SDFEM_TYPE 2 is built");
+    return PMG_ERR_UNSUPPORTED;
+  }
+  if (!L.slot.p) PMG_TRY(build_slot_map(h, L));
+  TableCache *T = nullptr;
+  PMG_TRY(get_tables(L.elem, rule_for(L.elem), T));
+  PMG_CUDA(cudaMemsetAsync(target, 0, sizeof(double) * L.nnz, h.stream));
+  if (rhs_target && zero_rhs) PMG_CUDA(cudaMemsetAsync(rhs_target, 0, sizeof(double) * L.N, h.stream));
+  PMG_CUDA(cudaMemsetAsync(h.d_flags.p, 0, sizeof(int) * 4, h.stream));
+  AsmArgs a{};
+  a.elem_dof = L.elem_dof.p;
+  a.cell_vert = L.cell_vert.p;
+  a.slot = L.slot.p;
+  a.Na = L.Na;
+  a.entries = target;
+  a.rhs = rhs_target;
+  a.form = form;
+  a.poly = h.prm.poly_degree > 0 ? h.prm.poly_degree : (L.elem == PMG_ELEM_Q2_HEX || L.elem == PMG_ELEM_P2_TET ? 2 : 1);
+  a.brick = L.brick;
+  a.delta0 = h.prm.delta0;
+  a.coef.kind = h.coeff.kind;
+  a.coef.eps = h.coeff.eps;
+  for (int k = 0; k < 3; k++) a.coef.b[k] = h.coeff.b[k];
+  a.coef.c = h.coeff.c;
+  a.coef.f = h.coeff.f;
+  a.coef.t = h.coeff.t;
+  a.coef.n_modes = h.coeff.n_modes;
+  a.coef.modes = h.d_modes.p;
+  a.utab = T->utab.p;
+  a.qtab = T->qtab.p;
+  a.flags = h.d_flags.p;
+  switch (L.elem) {
+    case PMG_ELEM_Q1_HEX: PMG_TRY((launch_assemble<PMG_ELEM_Q1_HEX, 8>(h, L, a))); break;
+    case PMG_ELEM_Q2_HEX: PMG_TRY((launch_assemble<PMG_ELEM_Q2_HEX, 27>(h, L, a))); break;
+    case PMG_ELEM_P1_TET: PMG_TRY((launch_assemble<PMG_ELEM_P1_TET, 4>(h, L, a))); break;
+    case PMG_ELEM_P2_TET: PMG_TRY((launch_assemble<PMG_ELEM_P2_TET, 11>(h, L, a))); break;
+    default: set_error("assemble: unknown element"); return PMG_ERR_ARG;
+  }
+  return PMG_OK;
+}
+
+// rhs of Dirichlet rows = nodal boundary values (AssembleMat3D.C:1031-1081)
+__global__ void k_dirichlet_rhs(int Na, int N, const double *__restrict__ dv, double *__restrict__ rhs) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + Na;
+  if (i < N) rhs[i] = dv ? dv[i - Na] : 0.0;
+}
+
+int set_dirichlet_rows(Handle &h, Level &L, double *target, double *rhs_target) {
+  (void)target;
+  int n = L.N - L.Na;
+  if (n > 0 && rhs_target) {
+    k_dirichlet_rhs<<<(n + 255) / 256, 256, 0, h.stream>>>(L.Na, L.N, L.dirval.p, rhs_target);
+    PMG_CUDA(cudaGetLastError());
+  }
+  return PMG_OK;
+}
+
+}  // namespace pmg

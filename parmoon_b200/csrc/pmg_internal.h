@@ -1,0 +1,165 @@
+// Internal declarations of the B200 ParMooN CD3D library (not part of the ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+#include "../../include/pmg_b200.h"
+
+namespace pmg {
+
+// ------------------------------------------------------------- errors
+void set_error(const std::string &msg);
+#define PMG_CUDA(call)                                                            \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess) {                                                      \
+      pmg::set_error(std::string(#call) + ": " + cudaGetErrorString(e_));         \
+      return PMG_ERR_CUDA;                                                        \
+    }                                                                             \
+  } while (0)
+#define PMG_TRY(call)                                                             \
+  do {                                                                            \
+    int r_ = (call);                                                              \
+    if (r_ != PMG_OK) return r_;                                                  \
+  } while (0)
+
+// ------------------------------------------------------------- device buffers
+template <typename T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  int alloc(size_t count) {
+    if (count == n && p) return PMG_OK;
+    release();
+    if (count == 0) return PMG_OK;
+    PMG_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+    return PMG_OK;
+  }
+  int upload(const T *h, size_t count, cudaStream_t s) {
+    PMG_TRY(alloc(count));
+    if (count) PMG_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    return PMG_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { release(); }
+};
+
+// element descriptors
+struct ElemInfo {
+  int nloc, nvert, quad_default;
+};
+ElemInfo elem_info(int elem_type);
+
+// one multigrid level
+struct Level {
+  // sizes
+  int N = 0, Na = 0, nnz = 0, n_cells = 0, elem = 0, nloc = 0, nvert = 0, brick = 0;
+  bool has_mesh = false, has_csr = false, has_P = false, assembled = false;
+  // CSR pattern (rows sorted)
+  DBuf<int> rowptr, kcol, diagpos;
+  // matrices: A (system), M (mass, time-dependent), A32 (FP32 copy for the V-cycle)
+  DBuf<double> A, M, Astash;
+  DBuf<float> A32;
+  DBuf<double> invdiag;
+  DBuf<float> invdiag32;
+  // rhs / Dirichlet values
+  DBuf<double> rhs, dirval;
+  // mesh in element-colour order
+  DBuf<int> elem_dof;       // n_cells x nloc
+  DBuf<double> cell_vert;   // n_cells x nvert x 3
+  DBuf<int> slot;           // n_cells x nloc x nloc
+  std::vector<int> ecolor_ptr;  // element colour classes [ecolor_ptr[c], ecolor_ptr[c+1])
+  // multicolour SSOR row lists (active rows only), grouped by colour
+  DBuf<int> row_list;
+  std::vector<int> rcolor_ptr;
+  // transfer from level-1: P (N x Nc), R = P^T (Nc x N)
+  int Nc = 0;
+  DBuf<int> prp, pcol, rrp, rcol;
+  DBuf<double> pval, rval;
+  DBuf<float> pval32, rval32;
+  // work vectors of the V-cycle (FP64 and FP32)
+  DBuf<double> x64, f64, d64;
+  DBuf<float> x32, f32, d32;
+  // lattice (learned smoother)
+  int lat_n[3] = {0, 0, 0};
+  DBuf<int> dof_ijk;
+  // average row length (SpMV launch shape)
+  int avg_row = 0;
+};
+
+struct Handle {
+  pmg_params prm;
+  pmg_coeff_desc coeff{};
+  std::vector<double> modes;
+  DBuf<double> d_modes;
+  std::vector<Level> lv;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  int num_sms = 148;
+  // coarsest-level dense inverse (FP64)
+  DBuf<double> coarse_lu, coarse_inv;
+  DBuf<int> coarse_piv;
+  bool coarse_ready = false;
+  // FGMRES workspace
+  int krylov_n = 0, krylov_restart = 0;
+  DBuf<double> V, Z, w, sol, rhs, H, scal;
+  DBuf<double> red_partial;
+  DBuf<unsigned int> red_counter;
+  double *h_H = nullptr;  // pinned mirror of one Hessenberg column
+  // error flags written by kernels (slot lookups, non-finite values)
+  DBuf<int> d_flags;
+  // timing
+  cudaEvent_t ev[6];
+  double t_assemble = 0, t_solve = 0, t_assemble_kernel = 0;
+  // V-cycle graph
+  cudaGraphExec_t vgraph = nullptr;
+  int vgraph_prec = -1;
+  // learned smoother weights
+  DBuf<float> lw;
+  bool has_learned = false;
+  double *h_pinned = nullptr;
+  size_t h_pinned_n = 0;
+};
+
+// ------------------------------------------------------------- kernels (assemble.cu)
+int build_slot_map(Handle &h, Level &L);
+int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs, double *rhs_target);
+int set_dirichlet_rows(Handle &h, Level &L, double *target, double *rhs_target);
+
+// ------------------------------------------------------------- kernels (sparse.cu)
+template <typename T>
+int spmv(cudaStream_t s, const Level &L, const T *A, const T *x, T *y);
+template <typename T>
+int defect(cudaStream_t s, const Level &L, const T *A, const T *x, const T *f, T *d);
+template <typename T>
+int ssor_sweep(cudaStream_t s, const Level &L, const T *A, const T *invdiag, const T *f, T *x, double omega);
+template <typename T>
+int restrict_defect(cudaStream_t s, const Level &Lf, const Level &Lc, const T *rval, const T *d, T *fc);
+template <typename T>
+int prolongate_add(cudaStream_t s, const Level &Lf, const T *pval, const T *xc, T *xf, double damp);
+int compute_invdiag(cudaStream_t s, Level &L);
+int convert_f64_f32(cudaStream_t s, const double *a, float *b, size_t n);
+int convert_f32_f64(cudaStream_t s, const float *a, double *b, size_t n);
+int copy_dirichlet(cudaStream_t s, int Na, int N, const double *f, double *x);
+int dot(Handle &h, const double *a, const double *b, size_t n, double *result_dev);
+int axpy_dev(cudaStream_t s, size_t n, const double *alpha_dev, double sign, const double *x, double *y);
+int scale_by_inv_sqrt(cudaStream_t s, size_t n, const double *nrm2_dev, const double *x, double *y);
+int fill(cudaStream_t s, double *x, double v, size_t n);
+template <typename T>
+int zero(cudaStream_t s, T *x, size_t n);
+int check_finite(cudaStream_t s, const double *x, size_t n, int *flag);
+
+// ------------------------------------------------------------- solver (solver.cu)
+int coarse_factor(Handle &h);
+int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *st);
+
+// ------------------------------------------------------------- learned smoother (learned.cu)
+int learned_num_params();
+
+}  // namespace pmg
