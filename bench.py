@@ -1,0 +1,322 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 ParMooN CD3D hot path.
+
+Workload (one "step"): the convection-dominated CD3D problem with SUPG on
+Q2 hexahedra, 64^3 cells (2,146,689 dofs, 130,422,149 nnz on the finest of 5
+levels), eps = 1e-6, b = (1, 0.5, 0.25), c = 0, f = 1, u = 1 on x = 0 and
+u = 0 on the rest of the boundary, Gauss3 quadrature: assembly of all five
+levels (TSystemCD3D::Assemble) followed by FGMRES(20) preconditioned by one
+V-cycle SSOR(2,2) with a dense coarsest solve, run until the FP64 true
+residual satisfies |r| <= 1e-10 |r0| (TSystemCD3D::Solve).
+
+  value      device time of one step (assembly + solve), seconds, inputs
+             resident in HBM, FP32-stored V-cycle inside FP64 FGMRES
+  e2e        the same step through the C ABI with host buffers: start
+             vector and rhs copied in, solution copied out, inside the timer
+  extras     finest-level assembly Mnnz/s, plain FP64-GMG time, iterations,
+             FP64 residual, roofline of the dominant kernel (the FP32 SSOR
+             sweep of the finest level) and of the assembly kernel
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+For N > 1 (torchrun) every rank solves its own copy (replicas, weak scaling;
+the problem has no exchange step on one GPU), timing is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Time to 1e-10 FP64 residual & assembly Mnnz/s: learned/FP32 MG vs FP64 MG, 1 B200"
+N_CELLS, N_LEVELS = 64, 5
+EPS, B, F = 1e-6, (1.0, 0.5, 0.25), 1.0
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "pmg_ref")
+# bounded CPU sample for the reference: the same problem on 32^3 cells (4 levels)
+REF_SAMPLE = dict(order=2, levels=4, coarse_steps=2, problem="cdsupg", eps=EPS, b1=B[0], b2=B[1], b3=B[2],
+                  dump=0, transfer=0, restart=20, red=1e-10)
+N_FULL = (2 * N_CELLS + 1) ** 3
+N_SAMPLE = (2 * 32 + 1) ** 3
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            P = json.load(f)
+        return float(P.get("hbm_gbs", 6650.0)), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[3 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dirichlet(x, y, z):
+    return (np.abs(x) < 1e-12).astype(float)
+
+
+def setup(P, precision):
+    levels = P.struct_hierarchy(P.Q2_HEX, N_CELLS, N_LEVELS)
+    h = P.Handle(N_LEVELS, P.default_params(precision=precision))
+    h.set_coefficients(P.coeff(kind=P.COEF_CONST, eps=EPS, b=B, f=F))
+    P.load_hierarchy(h, levels, dirichlet=dirichlet)
+    return h, levels
+
+
+def run_reference_sample():
+    """One run of the compiled reference on the bounded sample; returns timings dict."""
+    with tempfile.TemporaryDirectory() as td:
+        cmd = [REF_BIN, "cd3d", td] + [f"{k}={v}" for k, v in REF_SAMPLE.items()]
+        t0 = time.perf_counter()
+        subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        wall = time.perf_counter() - t0
+        meta = {}
+        with open(os.path.join(td, "meta.txt")) as f:
+            for line in f:
+                k, kind, v = line.split()
+                if kind == "scalar":
+                    meta[k] = float(v)
+    t_asm = sum(v for k, v in meta.items() if k.endswith("_t_assemble"))
+    return dict(t_assemble=t_asm, t_assemble_fine=meta["L3_t_assemble"], t_solve=meta["t_solve"],
+                iterations=meta["solve_iterations"], rel_res=meta["res_final"] / meta["res0"], wall=wall)
+
+
+def ref_sample_desc():
+    return ("reference ParMooN (oracle/_ref/pmg_ref, -O3, 1 thread, sequential build) on the same problem at "
+            "32^3 cells / 4 levels (274,625 dofs): Assemble()+Solve() wall time, scaled by the dof ratio "
+            f"{N_FULL / N_SAMPLE:.3f} to 64^3 (multigrid work is O(N) per iteration)")
+
+
+def bench_reference(args, rank, world):
+    if rank != 0:
+        return
+    if not os.path.exists(REF_BIN):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/pmg_ref not built (make -C oracle/ref)"}))
+        return
+    for _ in range(args.warmup):
+        run_reference_sample()
+    runs = [run_reference_sample() for _ in range(args.steps)]
+    scale = N_FULL / N_SAMPLE
+    step = statistics.median([(r["t_assemble"] + r["t_solve"]) * scale for r in runs])
+    r0 = runs[0]
+    line = {"metric": METRIC, "value": step, "unit": "s", "impl": "reference", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "CD3D SUPG Q2 hexahedra 64^3 (5 levels), eps=1e-6, b=(1,.5,.25), FGMRES+GMG to 1e-10",
+                       "sample": "32^3 / 4 levels, scaled by dof ratio"},
+            "assembly_mnnz_s": 15837829 / r0["t_assemble_fine"] / 1e6, "iterations": r0["iterations"],
+            "rel_res": r0["rel_res"],
+            "cpu_baseline": {"value": step, "unit": "s", "cores": 1, "kind": "reference", "sample": ref_sample_desc()},
+            "e2e": {"value": step, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def bench_ours(args, rank, world, dist):
+    import ctypes
+    import parmoon_b200 as P
+    lib = P.lib()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    h, levels = setup(P, P.PREC_FP32)
+    Fl = levels[-1]
+    nnz_fine = int(Fl["rowptr"][-1])
+
+    def sync():
+        if dist is not None:
+            import torch
+            torch.cuda.synchronize()
+            dist.barrier()
+
+    def step():
+        h.assemble(-1, P.FORM_SUPG, copy_out=False)
+        t_asm, _, _ = h.timings()
+        _, st, rc = h.solve()
+        return t_asm + st.seconds, st, rc
+
+    for _ in range(args.warmup):
+        step()
+    sync()
+    cnt0 = ctypes.c_ulonglong()
+    lib.pmg_launch_count(ctypes.byref(cnt0))
+    times, stats = [], []
+    with ClockSampler(local) as clk:
+        t_wall = time.perf_counter()
+        for _ in range(args.steps):
+            t, st, rc = step()
+            if rc != 0:
+                raise RuntimeError(f"solve failed with status {rc}")
+            times.append(t)
+            stats.append(st)
+        t_wall = time.perf_counter() - t_wall
+    cnt1 = ctypes.c_ulonglong()
+    lib.pmg_launch_count(ctypes.byref(cnt1))
+    sync()
+    step_time = statistics.mean(times)
+    if dist is not None:
+        import torch
+        tt = torch.tensor([step_time], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        step_time = float(tt.item())
+
+    # finest-level assembly throughput (one Assemble() of the finest level)
+    asm_fine = []
+    for _ in range(3):
+        h.assemble(N_LEVELS - 1, P.FORM_SUPG, copy_out=False)
+        asm_fine.append(h.timings()[0])
+    t_asm_fine = min(asm_fine)
+
+    # roofline of the dominant kernel: the FP32 SSOR step on the finest level
+    hbm, peak_kind = peaks()
+    sec, by, fl = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    P._check(lib.pmg_time_kernel(h.h, 3, N_LEVELS - 1, 0, 5, ctypes.byref(sec), ctypes.byref(by), ctypes.byref(fl)))
+    ssor = dict(seconds=sec.value, bytes=by.value, gbs=by.value / sec.value / 1e9)
+    P._check(lib.pmg_time_kernel(h.h, 1, N_LEVELS - 1, 0, 5, ctypes.byref(sec), ctypes.byref(by), ctypes.byref(fl)))
+    spmv32 = dict(seconds=sec.value, bytes=by.value, gbs=by.value / sec.value / 1e9)
+    P._check(lib.pmg_time_kernel(h.h, 0, N_LEVELS - 1, 0, 5, ctypes.byref(sec), ctypes.byref(by), ctypes.byref(fl)))
+    spmv64 = dict(seconds=sec.value, bytes=by.value, gbs=by.value / sec.value / 1e9)
+    P._check(lib.pmg_time_kernel(h.h, 4, N_LEVELS - 1, P.FORM_SUPG, 3, ctypes.byref(sec), ctypes.byref(by),
+                                 ctypes.byref(fl)))
+    asm = dict(seconds=sec.value, bytes=by.value, gbs=by.value / sec.value / 1e9, tflops=fl.value / sec.value / 1e12)
+
+    # end to end through the C ABI with host buffers
+    N = Fl["N"]
+    e2e_t = []
+    for _ in range(max(1, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        h.assemble(-1, P.FORM_SUPG, copy_out=False)
+        rhs = h.get_rhs(N_LEVELS - 1)
+        sol0 = np.zeros(N)
+        x, st, rc = h.solve(sol=sol0, rhs=rhs)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e = statistics.median(e2e_t)
+
+    # plain FP64 GMG on the same problem (the method the FP32 V-cycle is compared with)
+    h.set_params(P.default_params(precision=P.PREC_FP64))
+    fp64 = []
+    for _ in range(2):
+        _, st64, rc64 = h.solve()
+        fp64.append((st64.seconds, st64.iterations, st64.rel_res, rc64))
+    fp64_s = min(x[0] for x in fp64)
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if os.path.exists(REF_BIN) and not args.no_cpu:
+            r = run_reference_sample()
+            v = (r["t_assemble"] + r["t_solve"]) * N_FULL / N_SAMPLE
+            cpu = {"value": v, "unit": "s", "cores": 1, "kind": "reference", "sample": ref_sample_desc(),
+                   "sample_assembly_mnnz_s": 15837829 / r["t_assemble_fine"] / 1e6,
+                   "sample_iterations": r["iterations"]}
+        st = stats[-1]
+        line = {
+            "metric": METRIC, "value": step_time, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_time * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+            "config": {"workload": "CD3D SUPG Q2 hexahedra 64^3 (5 levels), eps=1e-6, b=(1,.5,.25), f=1, "
+                                   "FGMRES(20) + V-cycle SSOR(2,2) FP32, dense coarse solve, to 1e-10",
+                       "n_dofs": N, "nnz_fine": nnz_fine, "levels": N_LEVELS,
+                       "l2": "inputs larger than L2 (finest matrix 1.04 GB FP64 values + 0.52 GB indices)",
+                       "parallelism": f"replicas x{world}"},
+            "iterations": st.iterations, "rel_res_fp64": st.rel_res, "res0": st.res0,
+            "assembly_mnnz_s": nnz_fine / t_asm_fine / 1e6, "assembly_fine_s": t_asm_fine,
+            "fp64_gmg": {"solve_s": fp64_s, "iterations": fp64[0][1], "rel_res": fp64[0][2], "status": fp64[0][3]},
+            "fp32_solve_s": statistics.mean(s.seconds for s in stats),
+            "wall_s_per_step": t_wall / args.steps,
+            "roofline": {"bound": "hbm", "kernel": "k_gs_color<32,float> (FP32 SSOR step, finest level)",
+                         "achieved": ssor["gbs"], "peak": hbm, "unit": "GB/s", "frac": ssor["gbs"] / hbm,
+                         "traffic": None, "peak_kind": peak_kind, "bytes_per_launch": ssor["bytes"],
+                         "launch_s": ssor["seconds"]},
+            "roofline_spmv64": {"achieved": spmv64["gbs"], "frac": spmv64["gbs"] / hbm, "bytes": spmv64["bytes"]},
+            "roofline_spmv32": {"achieved": spmv32["gbs"], "frac": spmv32["gbs"] / hbm, "bytes": spmv32["bytes"]},
+            "roofline_assembly": {"achieved_gbs": asm["gbs"], "frac_hbm": asm["gbs"] / hbm,
+                                  "achieved_tflops_fp64": asm["tflops"], "bytes": asm["bytes"], "launch_s": asm["seconds"]},
+            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": 2 * N * 8, "d2h_bytes_per_step": 2 * N * 8},
+            "gpu_launches": int(cnt1.value - cnt0.value),
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    h.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if args.impl == "ours" and world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = tdist
+    elif world > 1:
+        pass
+    if args.impl == "reference":
+        bench_reference(args, rank, world)
+    else:
+        bench_ours(args, rank, world, dist)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

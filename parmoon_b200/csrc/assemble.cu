@@ -102,8 +102,14 @@ __device__ double hk_convection(bool hex, bool brick, const double *cv, const do
     for (int d = 0; d < 3; d++) g[0][d] = -(g[1][d] + g[2][d] + g[3][d]);
     for (int i = 0; i < 4; i++) den += fabs(b1 * g[i][0] + b2 * g[i][1] + b3 * g[i][2]);
   } else if (brick) {
-    double hx = cv[3] - cv[0], hy = cv[10] - cv[1], hz = cv[14] - cv[2];  // v1-v0 (x), v3-v0 (y), v4-v0 (z)
-    double px = b1 / hx, py = b2 / hy, pz = b3 / hz;
+    // edge lengths from the bounding box (any vertex order of an axis-aligned cell)
+    double lo[3] = {cv[0], cv[1], cv[2]}, hi[3] = {cv[0], cv[1], cv[2]};
+    for (int v = 1; v < 8; v++)
+      for (int d = 0; d < 3; d++) {
+        lo[d] = fmin(lo[d], cv[3 * v + d]);
+        hi[d] = fmax(hi[d], cv[3 * v + d]);
+      }
+    double px = b1 / (hi[0] - lo[0]), py = b2 / (hi[1] - lo[1]), pz = b3 / (hi[2] - lo[2]);
     den = 0.5 * (fabs(px + py + pz) + fabs(px + py - pz) + fabs(px - py + pz) + fabs(px - py - pz));
   } else {
     // general hexahedron: invert the 8x8 monomial matrix (1,x,y,z,xy,xz,yz,xyz)
@@ -368,7 +374,7 @@ int build_slot_map(Handle &h, Level &L) {
   int bs = 256;
   size_t nb = (total + bs - 1) / bs;
   k_slot_map<<<(unsigned)nb, bs, 0, h.stream>>>(L.n_cells, L.nloc, L.Na, L.elem_dof.p, L.rowptr.p, L.kcol.p,
-                                                   L.slot.p, h.d_flags.p);
+                                                   L.slot.p, h.d_flags.p); count_launches(1);
   PMG_CUDA(cudaGetLastError());
   int flags[4];
   PMG_CUDA(cudaMemcpyAsync(flags, h.d_flags.p, sizeof(flags), cudaMemcpyDeviceToHost, h.stream));
@@ -441,7 +447,7 @@ static int launch_assemble(Handle &h, Level &L, AsmArgs a) {
     int blocks = (n + per_block - 1) / per_block;
     int cap = h.num_sms * 8;
     if (blocks > cap) blocks = cap;
-    k_assemble<E, NQ><<<blocks, ASM_WARPS * 32, smem, h.stream>>>(b);
+    k_assemble<E, NQ><<<blocks, ASM_WARPS * 32, smem, h.stream>>>(b); count_launches(1);
     PMG_CUDA(cudaGetLastError());
   }
   return PMG_OK;
@@ -510,7 +516,7 @@ int set_dirichlet_rows(Handle &h, Level &L, double *target, double *rhs_target) 
   (void)target;
   int n = L.N - L.Na;
   if (n > 0 && rhs_target) {
-    k_dirichlet_rhs<<<(n + 255) / 256, 256, 0, h.stream>>>(L.Na, L.N, L.dirval.p, rhs_target);
+    k_dirichlet_rhs<<<(n + 255) / 256, 256, 0, h.stream>>>(L.Na, L.N, L.dirval.p, rhs_target); count_launches(1);
     PMG_CUDA(cudaGetLastError());
   }
   return PMG_OK;

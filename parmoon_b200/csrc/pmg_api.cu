@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <numeric>
 
@@ -16,6 +17,10 @@ namespace pmg {
 
 static thread_local std::string g_err;
 void set_error(const std::string &msg) { g_err = msg; }
+
+static std::atomic<unsigned long long> g_launches{0};
+void count_launches(unsigned long long n) { g_launches += n; }
+unsigned long long launches_so_far() { return g_launches.load(); }
 
 int level_invdiag(cudaStream_t s, Level &L, int *flags);
 
@@ -565,6 +570,74 @@ int pmg_last_timings(pmg_handle hh, double *assemble_s, double *solve_s, double 
   if (assemble_s) *assemble_s = h->t_assemble;
   if (solve_s) *solve_s = h->t_solve;
   if (assemble_kernel_s) *assemble_kernel_s = h->t_assemble_kernel;
+  return PMG_OK;
+}
+
+int pmg_launch_count(unsigned long long *n) {
+  if (!n) return PMG_ERR_ARG;
+  *n = launches_so_far();
+  return PMG_OK;
+}
+
+int pmg_time_kernel(pmg_handle hh, int kernel, int level, int form, int reps, double *sec, double *bytes,
+                    double *flops) {
+  Handle *h = H(hh);
+  PMG_TRY(check_level(h, level));
+  Level &L = h->lv[level];
+  if (reps < 1 || !sec) return PMG_ERR_ARG;
+  if (!L.assembled && kernel != PMG_KERNEL_ASSEMBLE) { set_error("pmg_time_kernel: assemble first"); return PMG_ERR_STATE; }
+  const double N = L.N, nnz = L.nnz;
+  double by = 0, fl = 0;
+  DBuf<double> x64, y64;
+  DBuf<float> x32, y32;
+  cudaStream_t s = h->stream;
+  auto run = [&]() -> int {
+    switch (kernel) {
+      case PMG_KERNEL_SPMV64: return spmv<double>(s, L, L.A.p, x64.p, y64.p);
+      case PMG_KERNEL_SPMV32: return spmv<float>(s, L, L.A32.p, x32.p, y32.p);
+      case PMG_KERNEL_SSOR64: return ssor_sweep<double>(s, L, L.A.p, L.invdiag.p, y64.p, x64.p, 1.0);
+      case PMG_KERNEL_SSOR32: return ssor_sweep<float>(s, L, L.A32.p, L.invdiag32.p, y32.p, x32.p, 1.0);
+      case PMG_KERNEL_ASSEMBLE: return assemble_level(*h, L, form, L.A.p, true, L.rhs.p);
+      default: set_error("pmg_time_kernel: unknown kernel"); return PMG_ERR_ARG;
+    }
+  };
+  if (kernel == PMG_KERNEL_SPMV64 || kernel == PMG_KERNEL_SSOR64) {
+    PMG_TRY(x64.alloc(L.N)); PMG_TRY(y64.alloc(L.N));
+    PMG_TRY(fill(s, x64.p, 1.0, L.N)); PMG_TRY(fill(s, y64.p, 1.0, L.N));
+    if (kernel == PMG_KERNEL_SSOR64) PMG_TRY(level_invdiag(s, L, h->d_flags.p));
+    // CSR bytes: values + column indices + row pointers + x gather (once) + y write
+    double spmv_b = 12 * nnz + 4 * (N + 1) + 16 * N;
+    by = kernel == PMG_KERNEL_SPMV64 ? spmv_b : 2 * spmv_b + 16 * N;
+    fl = kernel == PMG_KERNEL_SPMV64 ? 2 * nnz : 4 * nnz;
+  } else if (kernel == PMG_KERNEL_SPMV32 || kernel == PMG_KERNEL_SSOR32) {
+    if (!L.A32.p || !L.invdiag32.p) { set_error("pmg_time_kernel: no FP32 copy (solve in FP32 first)"); return PMG_ERR_STATE; }
+    PMG_TRY(x32.alloc(L.N)); PMG_TRY(y32.alloc(L.N));
+    PMG_CUDA(cudaMemsetAsync(x32.p, 0, sizeof(float) * L.N, s));
+    PMG_CUDA(cudaMemsetAsync(y32.p, 0, sizeof(float) * L.N, s));
+    double spmv_b = 8 * nnz + 4 * (N + 1) + 8 * N;
+    by = kernel == PMG_KERNEL_SPMV32 ? spmv_b : 2 * spmv_b + 8 * N;
+    fl = kernel == PMG_KERNEL_SPMV32 ? 2 * nnz : 4 * nnz;
+  } else {
+    // coloured scatter per element: n_loc^2 (4 slot + 8 read + 8 write) + n_loc (4 dof + 16 rhs) + vertices
+    const double nl = L.nloc, nv = L.nvert;
+    by = L.n_cells * (nl * nl * 20 + nl * 20 + nv * 4 + nv * 24);
+    const double nq = L.elem == PMG_ELEM_Q1_HEX ? 8 : L.elem == PMG_ELEM_Q2_HEX ? 27 : L.elem == PMG_ELEM_P1_TET ? 4 : 11;
+    fl = L.n_cells * (nq * nl * nl * 8 + nq * nl * 32);  // 4 FMA per (q,i,j) + D_q u_j (16 FMA per q,j)
+  }
+  PMG_TRY(run());  // warm-up
+  PMG_CUDA(cudaEventRecord(h->ev[4], s));
+  for (int r = 0; r < reps; r++) PMG_TRY(run());
+  PMG_CUDA(cudaEventRecord(h->ev[5], s));
+  PMG_CUDA(cudaEventSynchronize(h->ev[5]));
+  float ms = 0;
+  PMG_CUDA(cudaEventElapsedTime(&ms, h->ev[4], h->ev[5]));
+  *sec = ms * 1e-3 / reps;
+  if (bytes) *bytes = by;
+  if (flops) *flops = fl;
+  if (kernel == PMG_KERNEL_ASSEMBLE) {
+    PMG_TRY(set_dirichlet_rows(*h, L, L.A.p, L.rhs.p));
+    PMG_CUDA(cudaStreamSynchronize(s));
+  }
   return PMG_OK;
 }
 

@@ -10,6 +10,9 @@ namespace pmg {
 
 // ------------------------------------------------------------- errors
 void set_error(const std::string &msg);
+// kernel-launch accounting (pmg_launch_count)
+void count_launches(unsigned long long n);
+unsigned long long launches_so_far();
 #define PMG_CUDA(call)                                                            \
   do {                                                                            \
     cudaError_t e_ = (call);                                                      \
@@ -120,6 +123,7 @@ struct Handle {
   // V-cycle graph
   cudaGraphExec_t vgraph = nullptr;
   int vgraph_prec = -1;
+  unsigned long long vgraph_kernels = 0;
   // learned smoother weights
   DBuf<float> lw;
   bool has_learned = false;

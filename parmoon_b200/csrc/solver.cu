@@ -139,9 +139,9 @@ int coarse_factor(Handle &h) {
   DBuf<double> work;
   PMG_TRY(work.alloc((size_t)n * n));
   PMG_CUDA(cudaMemsetAsync(h.d_flags.p, 0, sizeof(int) * 4, h.stream));
-  k_csr_to_dense<<<n, 256, 0, h.stream>>>(n, L.rowptr.p, L.kcol.p, L.A.p, h.coarse_lu.p);
-  k_dense_lu<<<1, 1024, 0, h.stream>>>(n, h.coarse_lu.p, h.coarse_piv.p, h.d_flags.p);
-  k_dense_inverse<<<(n * 32 + 255) / 256, 256, 0, h.stream>>>(n, h.coarse_lu.p, h.coarse_piv.p, work.p, h.coarse_inv.p);
+  k_csr_to_dense<<<n, 256, 0, h.stream>>>(n, L.rowptr.p, L.kcol.p, L.A.p, h.coarse_lu.p); count_launches(1);
+  k_dense_lu<<<1, 1024, 0, h.stream>>>(n, h.coarse_lu.p, h.coarse_piv.p, h.d_flags.p); count_launches(1);
+  k_dense_inverse<<<(n * 32 + 255) / 256, 256, 0, h.stream>>>(n, h.coarse_lu.p, h.coarse_piv.p, work.p, h.coarse_inv.p); count_launches(1);
   PMG_CUDA(cudaGetLastError());
   int flags[4];
   PMG_CUDA(cudaMemcpyAsync(flags, h.d_flags.p, sizeof(flags), cudaMemcpyDeviceToHost, h.stream));
@@ -182,7 +182,7 @@ static int vcycle(Handle &h, int i) {
   using PT = Prec<T>;
   if (i == 0) {
     if (h.prm.coarse_smoother == PMG_COARSE_DIRECT) {
-      k_dense_apply<T><<<(L.N * 32 + 255) / 256, 256, 0, s>>>(L.N, h.coarse_inv.p, PT::f(L), PT::x(L));
+      k_dense_apply<T><<<(L.N * 32 + 255) / 256, 256, 0, s>>>(L.N, h.coarse_inv.p, PT::f(L), PT::x(L)); count_launches(1);
       PMG_CUDA(cudaGetLastError());
     } else {
       int it = h.prm.coarse_maxit > 0 ? h.prm.coarse_maxit : 1;
@@ -257,6 +257,7 @@ static int capture_vcycle(Handle &h) {
   if (h.vgraph && h.vgraph_prec == h.prm.precision) return PMG_OK;
   if (h.vgraph) { cudaGraphExecDestroy(h.vgraph); h.vgraph = nullptr; }
   cudaGraph_t g;
+  const unsigned long long before = launches_so_far();
   PMG_CUDA(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal));
   int top = (int)h.lv.size() - 1;
   int rc = h.prm.precision == PMG_PREC_FP32 ? vcycle<float>(h, top) : vcycle<double>(h, top);
@@ -265,6 +266,9 @@ static int capture_vcycle(Handle &h) {
   PMG_CUDA(e);
   PMG_CUDA(cudaGraphInstantiate(&h.vgraph, g, 0));
   cudaGraphDestroy(g);
+  // kernels recorded during capture run at each replay, not now
+  h.vgraph_kernels = launches_so_far() - before;
+  count_launches(0ULL - h.vgraph_kernels);
   h.vgraph_prec = h.prm.precision;
   return PMG_OK;
 }
@@ -274,12 +278,14 @@ static int precondition(Handle &h, const double *v, double *z) {
   Level &F = h.lv.back();
   int nb = (F.N + 255) / 256;
   if (h.prm.precision == PMG_PREC_FP32) {
-    k_prec_in32<<<nb, 256, 0, h.stream>>>(F.Na, F.N, v, F.f32.p, F.x32.p);
+    k_prec_in32<<<nb, 256, 0, h.stream>>>(F.Na, F.N, v, F.f32.p, F.x32.p); count_launches(1);
     PMG_CUDA(cudaGraphLaunch(h.vgraph, h.stream));
-    k_prec_out32<<<nb, 256, 0, h.stream>>>(F.N, F.x32.p, z);
+    count_launches(h.vgraph_kernels);
+    k_prec_out32<<<nb, 256, 0, h.stream>>>(F.N, F.x32.p, z); count_launches(1);
   } else {
-    k_prec_in64<<<nb, 256, 0, h.stream>>>(F.Na, F.N, v, F.f64.p, F.x64.p);
+    k_prec_in64<<<nb, 256, 0, h.stream>>>(F.Na, F.N, v, F.f64.p, F.x64.p); count_launches(1);
     PMG_CUDA(cudaGraphLaunch(h.vgraph, h.stream));
+    count_launches(h.vgraph_kernels);
     PMG_CUDA(cudaMemcpyAsync(z, F.x64.p, sizeof(double) * F.N, cudaMemcpyDeviceToDevice, h.stream));
   }
   PMG_CUDA(cudaGetLastError());
@@ -406,7 +412,7 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
       for (int k = 0; k < mm; k++) hcol[k] = y[k];
       PMG_CUDA(cudaMemcpyAsync(sc + 1, hcol, sizeof(double) * mm, cudaMemcpyHostToDevice, s));
       size_t nb = (N + 255) / 256;
-      k_lincomb<<<(unsigned)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(N, mm, sc + 1, Z, N, h.sol.p);
+      k_lincomb<<<(unsigned)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(N, mm, sc + 1, Z, N, h.sol.p); count_launches(1);
       PMG_CUDA(cudaGetLastError());
       PMG_CUDA(cudaStreamSynchronize(s));  // hcol is reused below
     }

@@ -56,9 +56,9 @@ template <typename T, int MODE>
 static int launch_csr(cudaStream_t s, const Level &L, const T *A, const T *x, const T *f, T *y) {
   int W = pick_width(L);
   int g = grid_for(L.N, W, 148);
-  if (W == 32) k_csr<32, T, MODE><<<g, 256, 0, s>>>(L.N, L.rowptr.p, L.kcol.p, A, x, f, y);
-  else if (W == 16) k_csr<16, T, MODE><<<g, 256, 0, s>>>(L.N, L.rowptr.p, L.kcol.p, A, x, f, y);
-  else k_csr<8, T, MODE><<<g, 256, 0, s>>>(L.N, L.rowptr.p, L.kcol.p, A, x, f, y);
+  if (W == 32) { k_csr<32, T, MODE><<<g, 256, 0, s>>>(L.N, L.rowptr.p, L.kcol.p, A, x, f, y); count_launches(1); }
+  else if (W == 16) { k_csr<16, T, MODE><<<g, 256, 0, s>>>(L.N, L.rowptr.p, L.kcol.p, A, x, f, y); count_launches(1); }
+  else { k_csr<8, T, MODE><<<g, 256, 0, s>>>(L.N, L.rowptr.p, L.kcol.p, A, x, f, y); count_launches(1); }
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
@@ -105,7 +105,7 @@ __global__ void k_copy_dirichlet(int Na, int N, const T *__restrict__ f, T *__re
 template <typename T>
 int ssor_sweep(cudaStream_t s, const Level &L, const T *A, const T *invdiag, const T *f, T *x, double omega) {
   int nd = L.N - L.Na;
-  if (nd > 0) k_copy_dirichlet<T><<<(nd + 255) / 256, 256, 0, s>>>(L.Na, L.N, f, x);
+  if (nd > 0) { k_copy_dirichlet<T><<<(nd + 255) / 256, 256, 0, s>>>(L.Na, L.N, f, x); count_launches(1); }
   int W = pick_width(L);
   int nc = (int)L.rcolor_ptr.size() - 1;
   for (int pass = 0; pass < 2; pass++) {
@@ -115,9 +115,9 @@ int ssor_sweep(cudaStream_t s, const Level &L, const T *A, const T *invdiag, con
       if (n <= 0) continue;
       int g = grid_for(n, W, 148);
       const int *rows = L.row_list.p + beg;
-      if (W == 32) k_gs_color<32, T><<<g, 256, 0, s>>>(n, rows, L.rowptr.p, L.kcol.p, A, invdiag, f, x, (T)omega);
-      else if (W == 16) k_gs_color<16, T><<<g, 256, 0, s>>>(n, rows, L.rowptr.p, L.kcol.p, A, invdiag, f, x, (T)omega);
-      else k_gs_color<8, T><<<g, 256, 0, s>>>(n, rows, L.rowptr.p, L.kcol.p, A, invdiag, f, x, (T)omega);
+      if (W == 32) { k_gs_color<32, T><<<g, 256, 0, s>>>(n, rows, L.rowptr.p, L.kcol.p, A, invdiag, f, x, (T)omega); count_launches(1); }
+      else if (W == 16) { k_gs_color<16, T><<<g, 256, 0, s>>>(n, rows, L.rowptr.p, L.kcol.p, A, invdiag, f, x, (T)omega); count_launches(1); }
+      else { k_gs_color<8, T><<<g, 256, 0, s>>>(n, rows, L.rowptr.p, L.kcol.p, A, invdiag, f, x, (T)omega); count_launches(1); }
     }
   }
   PMG_CUDA(cudaGetLastError());
@@ -162,14 +162,14 @@ template <typename T>
 int restrict_defect(cudaStream_t s, const Level &Lf, const Level &Lc, const T *rval, const T *d, T *fc) {
   // R = P^T has up to 27 (Q1) / 125 (Q2) entries per coarse row
   int g = grid_for(Lc.N, 16, 148);
-  k_restrict<16, T><<<g, 256, 0, s>>>(Lc.N, Lc.Na, Lf.rrp.p, Lf.rcol.p, rval, d, fc);
+  k_restrict<16, T><<<g, 256, 0, s>>>(Lc.N, Lc.Na, Lf.rrp.p, Lf.rcol.p, rval, d, fc); count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
 template <typename T>
 int prolongate_add(cudaStream_t s, const Level &Lf, const T *pval, const T *xc, T *xf, double damp) {
   int g = grid_for(Lf.Na, 8, 148);
-  k_prolong_add<8, T><<<g, 256, 0, s>>>(Lf.Na, Lf.prp.p, Lf.pcol.p, pval, xc, xf, (T)damp);
+  k_prolong_add<8, T><<<g, 256, 0, s>>>(Lf.Na, Lf.prp.p, Lf.pcol.p, pval, xc, xf, (T)damp); count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
@@ -208,18 +208,18 @@ static int vec_grid(size_t n) {
   return (int)(b < 148 * 16 ? (b ? b : 1) : 148 * 16);
 }
 int convert_f64_f32(cudaStream_t s, const double *a, float *b, size_t n) {
-  k_f64_to_f32<<<vec_grid(n), 256, 0, s>>>(n, a, b);
+  k_f64_to_f32<<<vec_grid(n), 256, 0, s>>>(n, a, b); count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
 int convert_f32_f64(cudaStream_t s, const float *a, double *b, size_t n) {
-  k_f32_to_f64<<<vec_grid(n), 256, 0, s>>>(n, a, b);
+  k_f32_to_f64<<<vec_grid(n), 256, 0, s>>>(n, a, b); count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
 int copy_dirichlet(cudaStream_t s, int Na, int N, const double *f, double *x) {
   int nd = N - Na;
-  if (nd > 0) k_copy_dirichlet<double><<<(nd + 255) / 256, 256, 0, s>>>(Na, N, f, x);
+  if (nd > 0) { k_copy_dirichlet<double><<<(nd + 255) / 256, 256, 0, s>>>(Na, N, f, x); count_launches(1); }
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_dot(size_t n, const double *__r
 }
 
 int dot(Handle &h, const double *a, const double *b, size_t n, double *result_dev) {
-  k_dot<<<RED_BLOCKS, RED_THREADS, 0, h.stream>>>(n, a, b, h.red_partial.p, h.red_counter.p, result_dev);
+  k_dot<<<RED_BLOCKS, RED_THREADS, 0, h.stream>>>(n, a, b, h.red_partial.p, h.red_counter.p, result_dev); count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
@@ -277,7 +277,7 @@ __global__ void k_axpy_dev(size_t n, const double *__restrict__ alpha, double si
     y[i] += al * x[i];
 }
 int axpy_dev(cudaStream_t s, size_t n, const double *alpha_dev, double sign, const double *x, double *y) {
-  k_axpy_dev<<<vec_grid(n), 256, 0, s>>>(n, alpha_dev, sign, x, y);
+  k_axpy_dev<<<vec_grid(n), 256, 0, s>>>(n, alpha_dev, sign, x, y); count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
@@ -291,7 +291,7 @@ __global__ void k_scale_inv_sqrt(size_t n, const double *__restrict__ nrm2, cons
     y[i] = x[i] * s;
 }
 int scale_by_inv_sqrt(cudaStream_t s, size_t n, const double *nrm2_dev, const double *x, double *y) {
-  k_scale_inv_sqrt<<<vec_grid(n), 256, 0, s>>>(n, nrm2_dev, x, y);
+  k_scale_inv_sqrt<<<vec_grid(n), 256, 0, s>>>(n, nrm2_dev, x, y); count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
@@ -300,7 +300,7 @@ __global__ void k_fill(size_t n, double *x, double v) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) x[i] = v;
 }
 int fill(cudaStream_t s, double *x, double v, size_t n) {
-  k_fill<<<vec_grid(n), 256, 0, s>>>(n, x, v);
+  k_fill<<<vec_grid(n), 256, 0, s>>>(n, x, v); count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
@@ -317,7 +317,7 @@ __global__ void k_check_finite(size_t n, const double *x, int *flag) {
     if (!isfinite(x[i])) { atomicOr(flag, 8); return; }
 }
 int check_finite(cudaStream_t s, const double *x, size_t n, int *flag) {
-  k_check_finite<<<vec_grid(n), 256, 0, s>>>(n, x, flag);
+  k_check_finite<<<vec_grid(n), 256, 0, s>>>(n, x, flag); count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
@@ -330,7 +330,7 @@ int level_invdiag(cudaStream_t s, Level &L, int *flags) {
     PMG_TRY(L.invdiag32.alloc(L.N));
     i32 = L.invdiag32.p;
   }
-  k_invdiag<<<(L.N + 255) / 256, 256, 0, s>>>(L.N, L.diagpos.p, L.A.p, L.invdiag.p, i32, flags);
+  k_invdiag<<<(L.N + 255) / 256, 256, 0, s>>>(L.N, L.diagpos.p, L.A.p, L.invdiag.p, i32, flags); count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
