@@ -157,9 +157,9 @@ def test_solve_q1_laplace(pmg, oracle, prec):
     b = h.get_rhs(2)
     r = b - oracle.spmv(F["rowptr"], F["kcol"], A, x)
     assert np.linalg.norm(r) <= 1.01e-10 * st.res0
-    # discretisation check: O(h^2) nodal error against the manufactured solution
+    # discretisation check: nodal error of Q1 / Gauss2 at h = 1/16 against the manufactured solution
     ex = d(*F["dof_xyz"].T)
-    assert np.max(np.abs(x - ex)) < 5e-3
+    assert np.max(np.abs(x - ex)) < 1e-2
     h.close()
 
 
