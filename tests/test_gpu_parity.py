@@ -165,9 +165,9 @@ def test_solve_q1_laplace(pmg, oracle, prec):
 
 @pytest.mark.parametrize("prec", [0, 1])
 def test_solve_q2_supg_matches_direct(pmg, prec):
-    """C2's discretisation at 8^3 cells (Q2, SUPG, eps=1e-6): the iterate agrees with a dense solve."""
+    """C2's discretisation at 4^3 cells (Q2, SUPG, eps=1e-6): the iterate agrees with a dense solve."""
     dirichlet = lambda x, y, z: (np.abs(x) < 1e-12).astype(float)
-    h, levels = make_hierarchy(pmg, 2, 8, 3, 2, dict(kind=0, eps=1e-6, b=(1, .5, .25), f=1.0), prec=prec,
+    h, levels = make_hierarchy(pmg, 2, 4, 3, 2, dict(kind=0, eps=1e-6, b=(1, .5, .25), f=1.0), prec=prec,
                                dirichlet=dirichlet)
     _, st, rc = h.solve()
     assert rc == 0 and st.rel_res <= 1e-10
