@@ -262,7 +262,7 @@ def bench_ours(args, rank, world, dist):
             "metric": METRIC, "value": step_time, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_time * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
-            "config": {"workload": "CD3D SUPG Q2 hexahedra 64^3 (5 levels), eps=1e-6, b=(1,.5,.25), f=1, "
+            "config": {"workload": f"CD3D SUPG Q2 hexahedra {N_CELLS}^3 ({N_LEVELS} levels), eps=1e-6, b=(1,.5,.25), f=1, "
                                    "FGMRES(20) + V-cycle SSOR(2,2) FP32, dense coarse solve, to 1e-10",
                        "n_dofs": N, "nnz_fine": nnz_fine, "levels": N_LEVELS,
                        "l2": "inputs larger than L2 (finest matrix 1.04 GB FP64 values + 0.52 GB indices)",
@@ -296,7 +296,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--n-cells", type=int, default=64, help="cells per direction (64 = the benchmarked workload)")
+    ap.add_argument("--levels", type=int, default=5)
     args = ap.parse_args()
+    global N_CELLS, N_LEVELS, N_FULL
+    N_CELLS, N_LEVELS = args.n_cells, args.levels
+    N_FULL = (2 * N_CELLS + 1) ** 3
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None

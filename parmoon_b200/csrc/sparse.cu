@@ -21,6 +21,12 @@ namespace pmg {
 template <typename T>
 __device__ __forceinline__ T ldg(const T *p) { return __ldg(p); }
 
+// first row of this warp and rows covered by the whole grid, for W-lane row groups
+template <int W>
+__device__ __forceinline__ int warp_first_row() { return ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32 / W); }
+template <int W>
+__device__ __forceinline__ int rows_per_grid() { return (gridDim.x * blockDim.x >> 5) * (32 / W); }
+
 template <int W, typename T>
 __device__ __forceinline__ T group_sum(T v) {
 #pragma unroll
@@ -33,14 +39,17 @@ template <int W, typename T, int MODE>
 __global__ void __launch_bounds__(256) k_csr(int N, const int *__restrict__ rp, const int *__restrict__ kc,
                                              const T *__restrict__ a, const T *__restrict__ x,
                                              const T *__restrict__ f, T *__restrict__ y) {
+  // the row loop is warp-uniform so every lane reaches the shuffles
   const int lane = threadIdx.x & (W - 1);
-  const int groups = gridDim.x * (blockDim.x / W);
-  for (int row = (blockIdx.x * blockDim.x + threadIdx.x) / W; row < N; row += groups) {
-    const int beg = ldg(rp + row), end = ldg(rp + row + 1);
+  for (int base = warp_first_row<W>(); base < N; base += rows_per_grid<W>()) {
+    const int row = base + (threadIdx.x & 31) / W;
     T s = 0;
-    for (int k = beg + lane; k < end; k += W) s += ldg(a + k) * ldg(x + ldg(kc + k));
+    if (row < N) {
+      const int beg = ldg(rp + row), end = ldg(rp + row + 1);
+      for (int k = beg + lane; k < end; k += W) s += ldg(a + k) * ldg(x + ldg(kc + k));
+    }
     s = group_sum<W>(s);
-    if (lane == 0) y[row] = MODE ? ldg(f + row) - s : s;
+    if (lane == 0 && row < N) y[row] = MODE ? ldg(f + row) - s : s;
   }
 }
 
@@ -85,14 +94,16 @@ __global__ void __launch_bounds__(256) k_gs_color(int nrows, const int *__restri
                                                   const T *__restrict__ invd, const T *__restrict__ f, T *x,
                                                   T omega) {
   const int lane = threadIdx.x & (W - 1);
-  const int groups = gridDim.x * (blockDim.x / W);
-  for (int k = (blockIdx.x * blockDim.x + threadIdx.x) / W; k < nrows; k += groups) {
-    const int row = ldg(rows + k);
-    const int beg = ldg(rp + row), end = ldg(rp + row + 1);
+  for (int base = warp_first_row<W>(); base < nrows; base += rows_per_grid<W>()) {
+    const int k = base + (threadIdx.x & 31) / W;
+    const int row = k < nrows ? ldg(rows + k) : -1;
     T s = 0;
-    for (int j = beg + lane; j < end; j += W) s += ldg(a + j) * x[ldg(kc + j)];
+    if (row >= 0) {
+      const int beg = ldg(rp + row), end = ldg(rp + row + 1);
+      for (int j = beg + lane; j < end; j += W) s += ldg(a + j) * x[ldg(kc + j)];
+    }
     s = group_sum<W>(s);
-    if (lane == 0) x[row] += omega * (ldg(f + row) - s) * ldg(invd + row);
+    if (lane == 0 && row >= 0) x[row] += omega * (ldg(f + row) - s) * ldg(invd + row);
   }
 }
 
@@ -131,15 +142,15 @@ template <int W, typename T>
 __global__ void __launch_bounds__(256) k_restrict(int Nc, int Nac, const int *__restrict__ rp, const int *__restrict__ col,
                                                   const T *__restrict__ val, const T *__restrict__ d, T *__restrict__ fc) {
   const int lane = threadIdx.x & (W - 1);
-  const int groups = gridDim.x * (blockDim.x / W);
-  for (int row = (blockIdx.x * blockDim.x + threadIdx.x) / W; row < Nc; row += groups) {
+  for (int base = warp_first_row<W>(); base < Nc; base += rows_per_grid<W>()) {
+    const int row = base + (threadIdx.x & 31) / W;
     T s = 0;
     if (row < Nac) {
       const int beg = ldg(rp + row), end = ldg(rp + row + 1);
       for (int k = beg + lane; k < end; k += W) s += ldg(val + k) * ldg(d + ldg(col + k));
-      s = group_sum<W>(s);
     }
-    if (lane == 0) fc[row] = s;
+    s = group_sum<W>(s);
+    if (lane == 0 && row < Nc) fc[row] = s;
   }
 }
 
@@ -148,13 +159,15 @@ __global__ void __launch_bounds__(256) k_prolong_add(int Naf, const int *__restr
                                                      const T *__restrict__ val, const T *__restrict__ xc,
                                                      T *__restrict__ xf, T damp) {
   const int lane = threadIdx.x & (W - 1);
-  const int groups = gridDim.x * (blockDim.x / W);
-  for (int row = (blockIdx.x * blockDim.x + threadIdx.x) / W; row < Naf; row += groups) {
-    const int beg = ldg(rp + row), end = ldg(rp + row + 1);
+  for (int base = warp_first_row<W>(); base < Naf; base += rows_per_grid<W>()) {
+    const int row = base + (threadIdx.x & 31) / W;
     T s = 0;
-    for (int k = beg + lane; k < end; k += W) s += ldg(val + k) * ldg(xc + ldg(col + k));
+    if (row < Naf) {
+      const int beg = ldg(rp + row), end = ldg(rp + row + 1);
+      for (int k = beg + lane; k < end; k += W) s += ldg(val + k) * ldg(xc + ldg(col + k));
+    }
     s = group_sum<W>(s);
-    if (lane == 0) xf[row] += damp * s;
+    if (lane == 0 && row < Naf) xf[row] += damp * s;
   }
 }
 
