@@ -191,6 +191,21 @@ int pmg_tcd_system(pmg_handle h, double tau, const double theta[4],
 int pmg_matvec(pmg_handle h, int level, const double *x, double *y);
 int pmg_defect(pmg_handle h, int level, const double *x, const double *b, double *r, double *norm);
 
+/* Allocation-free variant of pmg_defect (no counterpart in the reference).
+ * For callers that must not have the library allocate device memory during a
+ * call: hosts whose GPU memory is owned by their own pool or framework
+ * allocator, and latency-critical loops that cannot absorb cudaFree's
+ * device-wide wait.  x, b, r and norm are DEVICE pointers (N, N, N and 1
+ * doubles) the caller owns; the call computes r = b - A x and norm = |r|_2 on
+ * the level's FP64 matrix and returns after the handle's stream is done.
+ * Its only scratch is a fixed array inside the library (512 KiB per GPU,
+ * kept until the process exits), shared by all calls: calls that overlap on
+ * the GPU race on it.  The first call on a device looks up the array's
+ * address (once per device).  Levels with more than PMG_NOALLOC_MAX_ROWS
+ * rows are rejected with PMG_ERR_ARG; it calls no allocating routine. */
+#define PMG_NOALLOC_MAX_ROWS 16777216
+int pmg_defect_noalloc(pmg_handle h, int level, const double *x, const double *b, double *r, double *norm);
+
 /* One multicolour SSOR sweep pair (forward+backward) on a level, FP64
  * (TMGLevel3D::SSOR, src/FE/MGLevel3D.C:363-467, in colour order). */
 int pmg_ssor(pmg_handle h, int level, const double *rhs, double *sol, int n_sweeps);
