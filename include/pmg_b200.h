@@ -242,16 +242,17 @@ int pmg_last_timings(pmg_handle h, double *assemble_s, double *solve_s, double *
 /* Time one device kernel family on `level` with CUDA events on the handle's
  * stream (reps launches after one warm-up) and report its algorithmic bytes
  * and flops per launch:
- *   PMG_KERNEL_SPMV64 / SPMV32     CSR y = A x (FP64 / FP32 values)
- *   PMG_KERNEL_SSOR64 / SSOR32     one SSOR step = forward + backward colour sweeps
+ *   PMG_KERNEL_SPMV64 / SPMV32     y = A x on the solve's SELL-32 copy (FP64 / FP32 values)
+ *   PMG_KERNEL_SSOR64 / SSOR32     one SSOR step = forward + backward colour sweeps (SELL-32)
+ *   PMG_KERNEL_CSR_SPMV64          y = A x on the CSR pattern (the pmg_matvec plug-in)
  *   PMG_KERNEL_ASSEMBLE            the level's assembly kernel launches (form = current SUPG/Galerkin choice in arg)
- * The matrix must be assembled (for SPMV32/SSOR32, a solve with
- * PMG_PREC_FP32 must have created the FP32 copy). */
+ * The matrix must be assembled. */
 #define PMG_KERNEL_SPMV64    0
 #define PMG_KERNEL_SPMV32    1
 #define PMG_KERNEL_SSOR64    2
 #define PMG_KERNEL_SSOR32    3
 #define PMG_KERNEL_ASSEMBLE  4
+#define PMG_KERNEL_CSR_SPMV64 5
 int pmg_time_kernel(pmg_handle h, int kernel, int level, int form, int reps,
                     double *seconds_per_launch, double *bytes_per_launch, double *flops_per_launch);
 

@@ -8,6 +8,7 @@
 #include "fe_tables.h"
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <atomic>
 #include <mutex>
@@ -84,6 +85,8 @@ static int upload_row_colors(Handle *h, Level &L, int ncolors, const std::vector
   for (int r = 0; r < L.Na; r++) list[fp[color[r]]++] = r;
   PMG_TRY(L.row_list.upload(list.data(), list.size(), h->stream));
   L.rcolor_ptr = ptr;
+  L.h_row_list = list;
+  L.sell_ready = false;
   PMG_CUDA(cudaStreamSynchronize(h->stream));
   return PMG_OK;
 }
@@ -149,6 +152,10 @@ int pmg_create(pmg_handle *out, int n_levels, const pmg_params *p) {
   if (rc == PMG_OK && cudaMemset(h->red_counter.p, 0, sizeof(unsigned)) != cudaSuccess) rc = PMG_ERR_CUDA;
   if (rc == PMG_OK && cudaMallocHost(&h->h_H, sizeof(double) * 256) != cudaSuccess) rc = PMG_ERR_CUDA;
   if (rc != PMG_OK) { pmg_destroy(reinterpret_cast<pmg_handle>(h)); return rc; }
+  {
+    const char *ng = getenv("PMG_NO_GRAPH");
+    h->use_graph = !(ng && ng[0] == '1');
+  }
   h->coeff.kind = PMG_COEF_CONST;
   h->coeff.eps = 1.0;
   h->coeff.f = 1.0;
@@ -265,6 +272,9 @@ int pmg_set_level_csr(pmg_handle hh, int level, int n_rows, int active_bound, co
   int ncol = 0;
   std::vector<int> color = color_rows(n_rows, active_bound, row_ptr, kcol, ncol);
   PMG_TRY(upload_row_colors(h, L, ncol, color));
+  L.h_rowptr.assign(row_ptr, row_ptr + n_rows + 1);
+  L.h_kcol.assign(kcol, kcol + nnz);
+  L.sell_ready = false;
   L.has_csr = true;
   L.has_mesh = false;
   L.slot.release();
@@ -280,9 +290,7 @@ int pmg_set_level_row_colors(pmg_handle hh, int level, int n_colors, const int *
   Level &L = h->lv[level];
   if (!L.has_csr || !colors || n_colors < 1) { set_error("pmg_set_level_row_colors: bad state/arguments"); return PMG_ERR_ARG; }
   // verify: no two coupled active rows share a colour
-  std::vector<int> rp(L.N + 1), kc(L.nnz);
-  PMG_CUDA(cudaMemcpy(rp.data(), L.rowptr.p, sizeof(int) * (L.N + 1), cudaMemcpyDeviceToHost));
-  PMG_CUDA(cudaMemcpy(kc.data(), L.kcol.p, sizeof(int) * L.nnz, cudaMemcpyDeviceToHost));
+  const std::vector<int> &rp = L.h_rowptr, &kc = L.h_kcol;
   std::vector<int> c(colors, colors + L.N);
   for (int r = 0; r < L.Na; r++) {
     if (c[r] < 0 || c[r] >= n_colors) { set_error("pmg_set_level_row_colors: colour out of range"); return PMG_ERR_ARG; }
@@ -389,6 +397,7 @@ static int assemble_one(Handle *h, int level, int form, double *entries_out, dou
   if (flags[0] & 1) { set_error("assemble: element coupling missing from the CSR pattern"); return PMG_ERR_SLOT; }
   if (!mass) {
     L.assembled = true;
+    L.sell_val_fresh32 = L.sell_val_fresh64 = false;
     if (level == 0) h->coarse_ready = false;
   }
   if (entries_out) PMG_CUDA(cudaMemcpyAsync(entries_out, target, sizeof(double) * L.nnz, cudaMemcpyDeviceToHost, h->stream));
@@ -435,6 +444,7 @@ int pmg_set_matrix(pmg_handle hh, int level, int which, const double *in) {
   else {
     PMG_TRY(L.A.upload(in, L.nnz, h->stream));
     L.assembled = true;
+    L.sell_val_fresh32 = L.sell_val_fresh64 = false;
     if (level == 0) h->coarse_ready = false;
   }
   PMG_CUDA(cudaStreamSynchronize(h->stream));
@@ -593,24 +603,25 @@ int pmg_time_kernel(pmg_handle hh, int kernel, int level, int form, int reps, do
   cudaStream_t s = h->stream;
   auto run = [&]() -> int {
     switch (kernel) {
-      case PMG_KERNEL_SPMV64: return spmv<double>(s, L, L.A.p, x64.p, y64.p);
-      case PMG_KERNEL_SPMV32: return spmv<float>(s, L, L.A32.p, x32.p, y32.p);
-      case PMG_KERNEL_SSOR64: return ssor_sweep<double>(s, L, L.A.p, L.invdiag.p, y64.p, x64.p, 1.0);
-      case PMG_KERNEL_SSOR32: return ssor_sweep<float>(s, L, L.A32.p, L.invdiag32.p, y32.p, x32.p, 1.0);
+      case PMG_KERNEL_SPMV64: return sell_spmv<double>(s, L, x64.p, nullptr, y64.p, 0, h->num_sms);
+      case PMG_KERNEL_SPMV32: return sell_spmv<float>(s, L, x32.p, nullptr, y32.p, 0, h->num_sms);
+      case PMG_KERNEL_SSOR64: return sell_ssor<double>(s, L, y64.p, x64.p, 1.0, h->num_sms);
+      case PMG_KERNEL_SSOR32: return sell_ssor<float>(s, L, y32.p, x32.p, 1.0, h->num_sms);
+      case PMG_KERNEL_CSR_SPMV64: return spmv<double>(s, L, L.A.p, x64.p, y64.p);
       case PMG_KERNEL_ASSEMBLE: return assemble_level(*h, L, form, L.A.p, true, L.rhs.p);
       default: set_error("pmg_time_kernel: unknown kernel"); return PMG_ERR_ARG;
     }
   };
-  if (kernel == PMG_KERNEL_SPMV64 || kernel == PMG_KERNEL_SSOR64) {
+  if (kernel == PMG_KERNEL_SPMV64 || kernel == PMG_KERNEL_SSOR64 || kernel == PMG_KERNEL_CSR_SPMV64) {
     PMG_TRY(x64.alloc(L.N)); PMG_TRY(y64.alloc(L.N));
     PMG_TRY(fill(s, x64.p, 1.0, L.N)); PMG_TRY(fill(s, y64.p, 1.0, L.N));
-    if (kernel == PMG_KERNEL_SSOR64) PMG_TRY(level_invdiag(s, L, h->d_flags.p));
+    if (kernel != PMG_KERNEL_CSR_SPMV64) PMG_TRY(sell_values<double>(*h, L));
     // CSR bytes: values + column indices + row pointers + x gather (once) + y write
     double spmv_b = 12 * nnz + 4 * (N + 1) + 16 * N;
-    by = kernel == PMG_KERNEL_SPMV64 ? spmv_b : 2 * spmv_b + 16 * N;
-    fl = kernel == PMG_KERNEL_SPMV64 ? 2 * nnz : 4 * nnz;
+    by = kernel == PMG_KERNEL_SSOR64 ? 2 * spmv_b + 16 * N : spmv_b;
+    fl = kernel == PMG_KERNEL_SSOR64 ? 4 * nnz : 2 * nnz;
   } else if (kernel == PMG_KERNEL_SPMV32 || kernel == PMG_KERNEL_SSOR32) {
-    if (!L.A32.p || !L.invdiag32.p) { set_error("pmg_time_kernel: no FP32 copy (solve in FP32 first)"); return PMG_ERR_STATE; }
+    PMG_TRY(sell_values<float>(*h, L));
     PMG_TRY(x32.alloc(L.N)); PMG_TRY(y32.alloc(L.N));
     PMG_CUDA(cudaMemsetAsync(x32.p, 0, sizeof(float) * L.N, s));
     PMG_CUDA(cudaMemsetAsync(y32.p, 0, sizeof(float) * L.N, s));
@@ -635,6 +646,7 @@ int pmg_time_kernel(pmg_handle hh, int kernel, int level, int form, int reps, do
   if (bytes) *bytes = by;
   if (flops) *flops = fl;
   if (kernel == PMG_KERNEL_ASSEMBLE) {
+    L.sell_val_fresh32 = L.sell_val_fresh64 = false;
     PMG_TRY(set_dirichlet_rows(*h, L, L.A.p, L.rhs.p));
     PMG_CUDA(cudaStreamSynchronize(s));
   }

@@ -27,6 +27,39 @@ unsigned long long launches_so_far();
     if (r_ != PMG_OK) return r_;                                                  \
   } while (0)
 
+// ------------------------------------------------------------- programmatic dependent launch
+// Kernels of the solve are launched with programmatic stream serialization:
+// a kernel may be scheduled while its predecessor drains and waits in
+// pdl_wait() (griddepcontrol.wait, sm_90+) until the predecessor has completed
+// and its writes are visible, so nothing is read or written before that.
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_wait() {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+__device__ __forceinline__ void pdl_trigger() {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
+template <typename... KArgs, typename... Args>
+static inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                     Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+#endif
+
 // ------------------------------------------------------------- device buffers
 template <typename T>
 struct DBuf {
@@ -94,6 +127,16 @@ struct Level {
   DBuf<int> dof_ijk;
   // average row length (SpMV launch shape)
   int avg_row = 0;
+  // host copies of the pattern and of the colour row lists (SELL set-up)
+  std::vector<int> h_rowptr, h_kcol, h_row_list;
+  // SELL-32 copy for the solve (see sell.cu)
+  bool sell_ready = false, sell_val_fresh32 = false, sell_val_fresh64 = false;
+  int sell_nslices = 0;
+  long sell_nnz = 0;
+  std::vector<int> sell_group;  // slice range of each colour group (+ Dirichlet group)
+  DBuf<int> sell_perm, sell_ptr, sell_col;
+  DBuf<float> sell_val32, sell_invd32;
+  DBuf<double> sell_val64, sell_invd64;
 };
 
 struct Handle {
@@ -124,6 +167,7 @@ struct Handle {
   cudaGraphExec_t vgraph = nullptr;
   int vgraph_prec = -1;
   unsigned long long vgraph_kernels = 0;
+  bool use_graph = true;  // PMG_NO_GRAPH=1 launches the V-cycle kernels directly (profilers)
   // learned smoother weights
   DBuf<float> lw;
   bool has_learned = false;
@@ -158,6 +202,15 @@ int fill(cudaStream_t s, double *x, double v, size_t n);
 template <typename T>
 int zero(cudaStream_t s, T *x, size_t n);
 int check_finite(cudaStream_t s, const double *x, size_t n, int *flag);
+
+// ------------------------------------------------------------- SELL-32 (sell.cu)
+int build_sell(Handle &h, Level &L);
+template <typename T>
+int sell_values(Handle &h, Level &L);
+template <typename T>
+int sell_spmv(cudaStream_t s, const Level &L, const T *x, const T *f, T *y, int mode, int num_sms);
+template <typename T>
+int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, int num_sms);
 
 // ------------------------------------------------------------- solver (solver.cu)
 int coarse_factor(Handle &h);

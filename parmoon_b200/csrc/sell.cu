@@ -1,0 +1,278 @@
+// SELL-32 storage of the level matrices for the solve (sm_100a).
+//
+// The assembled matrix stays in the host's CSR pattern (that is what the
+// slot map scatters into and what pmg_get_matrix returns).  For the solve
+// every level also keeps a sliced-ELLPACK copy built once per pattern:
+//
+//   * rows are grouped by SSOR colour (Dirichlet rows form a last group),
+//     sorted inside a group by decreasing length (ties: increasing row), and
+//     cut into slices of 32 rows; a group is padded with empty rows to a
+//     multiple of 32, so every colour owns a whole number of slices;
+//   * slice s stores its 32 rows column-major with the slice's maximum row
+//     length L_s: entry j of lane l sits at slice_ptr[s] + 32 j + l, so a warp
+//     reads 128 contiguous bytes (FP32) per step; padding has value 0 and a
+//     valid column, so no masking is needed.
+//
+// A block of SELL_K warps owns one slice (each warp takes every SELL_K-th
+// column step of the 32 rows), so every row keeps several independent
+// load chains in flight; the CSR kernels with a W-lane group per row stall
+// on the row pointer of every row.  Vectors stay in the host's dof
+// numbering: the kernels gather x through L2 and write each result row once.
+//
+// An SSOR step is one launch per colour and direction (2 x 27 launches for
+// Q2), captured in the V-cycle's CUDA graph and chained with programmatic
+// dependent launch.
+#include "pmg_internal.h"
+#include <algorithm>
+#include <cstdlib>
+#include <numeric>
+
+namespace pmg {
+
+int build_sell(Handle &h, Level &L) {
+  if (L.sell_ready) return PMG_OK;
+  const int N = L.N;
+  const std::vector<int> &rp = L.h_rowptr, &kc = L.h_kcol;
+  if ((int)rp.size() != N + 1) {
+    set_error("build_sell: host copy of the CSR pattern missing");
+    return PMG_ERR_STATE;
+  }
+  // groups: colours of the active rows, then the Dirichlet rows
+  const int nc = (int)L.rcolor_ptr.size() - 1;
+  std::vector<int> perm;
+  std::vector<int> group_slice(nc + 2, 0);
+  perm.reserve((size_t)N + 32 * (nc + 1));
+  std::vector<int> rows;
+  for (int g = 0; g <= nc; g++) {
+    rows.clear();
+    if (g < nc) rows.assign(L.h_row_list.begin() + L.rcolor_ptr[g], L.h_row_list.begin() + L.rcolor_ptr[g + 1]);
+    else for (int r = L.Na; r < N; r++) rows.push_back(r);
+    std::stable_sort(rows.begin(), rows.end(), [&](int a, int b) {
+      int la = rp[a + 1] - rp[a], lb = rp[b + 1] - rp[b];
+      return la > lb || (la == lb && a < b);
+    });
+    group_slice[g] = (int)(perm.size() / 32);
+    perm.insert(perm.end(), rows.begin(), rows.end());
+    while (perm.size() % 32) perm.push_back(-1);
+  }
+  group_slice[nc + 1] = (int)(perm.size() / 32);
+  const int nslices = (int)(perm.size() / 32);
+  std::vector<int> sptr(nslices + 1, 0);
+  long total = 0;
+  for (int s = 0; s < nslices; s++) {
+    int lmax = 0;
+    for (int l = 0; l < 32; l++) {
+      int r = perm[(size_t)s * 32 + l];
+      if (r >= 0) lmax = std::max(lmax, rp[r + 1] - rp[r]);
+    }
+    sptr[s] = (int)total;
+    total += 32L * lmax;
+    if (total > 2147483647L) {
+      set_error("build_sell: padded matrix exceeds 2^31 entries");
+      return PMG_ERR_UNSUPPORTED;
+    }
+  }
+  sptr[nslices] = (int)total;
+  std::vector<int> col((size_t)total);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int s = 0; s < nslices; s++) {
+    const int off = sptr[s], lmax = (sptr[s + 1] - off) / 32;
+    for (int l = 0; l < 32; l++) {
+      const int r = perm[(size_t)s * 32 + l];
+      const int len = r >= 0 ? rp[r + 1] - rp[r] : 0;
+      for (int j = 0; j < lmax; j++)
+        col[(size_t)off + 32 * j + l] = j < len ? kc[rp[r] + j] : (r >= 0 ? r : 0);
+    }
+  }
+  PMG_TRY(L.sell_perm.upload(perm.data(), perm.size(), h.stream));
+  PMG_TRY(L.sell_ptr.upload(sptr.data(), sptr.size(), h.stream));
+  PMG_TRY(L.sell_col.upload(col.data(), col.size(), h.stream));
+  PMG_CUDA(cudaStreamSynchronize(h.stream));
+  L.sell_group = group_slice;
+  L.sell_nslices = nslices;
+  L.sell_nnz = total;
+  L.sell_ready = true;
+  L.sell_val_fresh32 = L.sell_val_fresh64 = false;
+  return PMG_OK;
+}
+
+// values of the CSR matrix into the slice layout (and the permuted inverse diagonal)
+template <typename T>
+__global__ void k_csr_to_sell(int nslices, const int *__restrict__ perm, const int *__restrict__ sptr,
+                              const int *__restrict__ rp, const double *__restrict__ a, const int *__restrict__ dpos,
+                              T *__restrict__ val, T *__restrict__ invd) {
+  const int lane = threadIdx.x & 31;
+  for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nslices; s += (gridDim.x * blockDim.x) >> 5) {
+    const int off = sptr[s], lmax = (sptr[s + 1] - off) >> 5;
+    const int r = perm[s * 32 + lane];
+    const int beg = r >= 0 ? rp[r] : 0, len = r >= 0 ? rp[r + 1] - beg : 0;
+    for (int j = 0; j < lmax; j++) val[off + 32 * j + lane] = j < len ? (T)a[beg + j] : (T)0;
+    T dv = (T)1;
+    if (r >= 0) {
+      const double d = a[dpos[r]];
+      dv = (T)(d != 0.0 ? 1.0 / d : 1.0);
+    }
+    invd[s * 32 + lane] = dv;
+  }
+}
+
+template <typename T>
+int sell_values(Handle &h, Level &L) {
+  const bool f32 = sizeof(T) == 4;
+  if (f32 ? L.sell_val_fresh32 : L.sell_val_fresh64) return PMG_OK;
+  PMG_TRY(build_sell(h, L));
+  T *val, *invd;
+  if (f32) {
+    PMG_TRY(L.sell_val32.alloc(L.sell_nnz));
+    PMG_TRY(L.sell_invd32.alloc((size_t)L.sell_nslices * 32));
+    val = reinterpret_cast<T *>(L.sell_val32.p);
+    invd = reinterpret_cast<T *>(L.sell_invd32.p);
+  } else {
+    PMG_TRY(L.sell_val64.alloc(L.sell_nnz));
+    PMG_TRY(L.sell_invd64.alloc((size_t)L.sell_nslices * 32));
+    val = reinterpret_cast<T *>(L.sell_val64.p);
+    invd = reinterpret_cast<T *>(L.sell_invd64.p);
+  }
+  int blocks = std::min((L.sell_nslices + 7) / 8, h.num_sms * 16);
+  k_csr_to_sell<T><<<std::max(blocks, 1), 256, 0, h.stream>>>(L.sell_nslices, L.sell_perm.p, L.sell_ptr.p, L.rowptr.p,
+                                                                L.A.p, L.diagpos.p, val, invd); count_launches(1);
+  PMG_CUDA(cudaGetLastError());
+  if (f32) L.sell_val_fresh32 = true; else L.sell_val_fresh64 = true;
+  return PMG_OK;
+}
+template int sell_values<float>(Handle &, Level &);
+template int sell_values<double>(Handle &, Level &);
+
+// A block of K warps owns one slice: warp w accumulates the column steps
+// j = w, w+K, ... of the slice's 32 rows (coalesced 32-wide loads), the K
+// partial sums meet in shared memory and warp 0 finishes the rows.  K warps
+// per slice keep K times more loads in flight than one thread per row, which
+// a single colour (1/27 of the rows) needs to stream at HBM rate.
+constexpr int SELL_K = 4;
+
+// y = A x (MODE 0) or d = f - A x (MODE 1) over slices [s0, s1)
+template <typename T, int MODE>
+__global__ void __launch_bounds__(32 * SELL_K) k_sell_mv(int s0, int s1, const int *__restrict__ perm,
+                                                         const int *__restrict__ sptr, const int *__restrict__ col,
+                                                         const T *__restrict__ val, const T *__restrict__ x,
+                                                         const T *__restrict__ f, T *__restrict__ y) {
+  __shared__ T part[SELL_K][32];
+  pdl_wait();
+  pdl_trigger();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int s = s0 + blockIdx.x; s < s1; s += gridDim.x) {
+    const int off = __ldg(sptr + s), lmax = (__ldg(sptr + s + 1) - off) >> 5;
+    const int *c = col + off + lane;
+    const T *v = val + off + lane;
+    T sum = 0;
+#pragma unroll 4
+    for (int j = w; j < lmax; j += SELL_K) sum += __ldg(v + 32 * j) * __ldg(x + __ldg(c + 32 * j));
+    part[w][lane] = sum;
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+      for (int k = 1; k < SELL_K; k++) sum += part[k][lane];
+      const int r = __ldg(perm + s * 32 + lane);
+      if (r >= 0) y[r] = MODE ? __ldg(f + r) - sum : sum;
+    }
+    __syncthreads();
+  }
+}
+
+// Gauss-Seidel update of the rows of one colour (slices [s0, s1))
+template <typename T>
+__global__ void __launch_bounds__(32 * SELL_K) k_sell_gs(int s0, int s1, const int *__restrict__ perm,
+                                                         const int *__restrict__ sptr, const int *__restrict__ col,
+                                                         const T *__restrict__ val, const T *__restrict__ invd,
+                                                         const T *__restrict__ f, T *x, T omega) {
+  __shared__ T part[SELL_K][32];
+  pdl_wait();
+  pdl_trigger();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int s = s0 + blockIdx.x; s < s1; s += gridDim.x) {
+    const int off = __ldg(sptr + s), lmax = (__ldg(sptr + s + 1) - off) >> 5;
+    const int *c = col + off + lane;
+    const T *v = val + off + lane;
+    T sum = 0;
+#pragma unroll 4
+    for (int j = w; j < lmax; j += SELL_K) sum += __ldg(v + 32 * j) * x[__ldg(c + 32 * j)];
+    part[w][lane] = sum;
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+      for (int k = 1; k < SELL_K; k++) sum += part[k][lane];
+      const int r = __ldg(perm + s * 32 + lane);
+      if (r >= 0) x[r] += omega * (__ldg(f + r) - sum) * __ldg(invd + s * 32 + lane);
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T>
+__global__ void k_sell_copy_dirichlet(int Na, int N, const T *__restrict__ f, T *__restrict__ x) {
+  pdl_wait();
+  pdl_trigger();
+  int i = blockIdx.x * blockDim.x + threadIdx.x + Na;
+  if (i < N) x[i] = f[i];
+}
+
+static int slice_grid(int nslices, int num_sms) {
+  int cap = num_sms * 64;  // 16 resident blocks of 4 warps per SM, 4 waves
+  return std::max(1, std::min(nslices, cap));
+}
+
+template <typename T>
+static const T *sell_val(const Level &L) {
+  if (sizeof(T) == 4) return reinterpret_cast<const T *>(L.sell_val32.p);
+  return reinterpret_cast<const T *>(L.sell_val64.p);
+}
+template <typename T>
+static const T *sell_invd(const Level &L) {
+  if (sizeof(T) == 4) return reinterpret_cast<const T *>(L.sell_invd32.p);
+  return reinterpret_cast<const T *>(L.sell_invd64.p);
+}
+
+template <typename T>
+int sell_spmv(cudaStream_t s, const Level &L, const T *x, const T *f, T *y, int mode, int num_sms) {
+  const int n = L.sell_nslices;
+  if (mode)
+    PMG_CUDA(launch_pdl(k_sell_mv<T, 1>, dim3(slice_grid(n, num_sms)), dim3(32 * SELL_K), 0, s, 0, n,
+                        (const int *)L.sell_perm.p, (const int *)L.sell_ptr.p, (const int *)L.sell_col.p,
+                        sell_val<T>(L), x, f, y));
+  else
+    PMG_CUDA(launch_pdl(k_sell_mv<T, 0>, dim3(slice_grid(n, num_sms)), dim3(32 * SELL_K), 0, s, 0, n,
+                        (const int *)L.sell_perm.p, (const int *)L.sell_ptr.p, (const int *)L.sell_col.p,
+                        sell_val<T>(L), x, f, y));
+  count_launches(1);
+  PMG_CUDA(cudaGetLastError());
+  return PMG_OK;
+}
+template int sell_spmv<float>(cudaStream_t, const Level &, const float *, const float *, float *, int, int);
+template int sell_spmv<double>(cudaStream_t, const Level &, const double *, const double *, double *, int, int);
+
+// one SSOR step: Dirichlet rows from f, forward over the colours, backward
+template <typename T>
+int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, int num_sms) {
+  const int nc = (int)L.sell_group.size() - 2;  // active colours
+  const int nd = L.N - L.Na;
+  if (nd > 0) {
+    PMG_CUDA(launch_pdl(k_sell_copy_dirichlet<T>, dim3((nd + 255) / 256), dim3(256), 0, s, L.Na, L.N, f, x));
+    count_launches(1);
+  }
+  for (int pass = 0; pass < 2; pass++)
+    for (int cc = 0; cc < nc; cc++) {
+      const int c = pass == 0 ? cc : nc - 1 - cc;
+      const int s0 = L.sell_group[c], s1 = L.sell_group[c + 1];
+      if (s1 <= s0) continue;
+      PMG_CUDA(launch_pdl(k_sell_gs<T>, dim3(slice_grid(s1 - s0, num_sms)), dim3(32 * SELL_K), 0, s, s0, s1,
+                          (const int *)L.sell_perm.p, (const int *)L.sell_ptr.p, (const int *)L.sell_col.p,
+                          sell_val<T>(L), sell_invd<T>(L), f, x, (T)omega));
+      count_launches(1);
+    }
+  PMG_CUDA(cudaGetLastError());
+  return PMG_OK;
+}
+template int sell_ssor<float>(cudaStream_t, const Level &, const float *, float *, double, int);
+template int sell_ssor<double>(cudaStream_t, const Level &, const double *, double *, double, int);
+
+}  // namespace pmg

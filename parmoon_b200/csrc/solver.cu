@@ -15,6 +15,7 @@
 // The V-cycle is captured once per solve into a CUDA graph and replayed for
 // every preconditioner application (hundreds of small colour launches).
 #include "pmg_internal.h"
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -23,18 +24,31 @@ namespace pmg {
 int level_invdiag(cudaStream_t s, Level &L, int *flags);
 
 // ----------------------------------------------------------------- coarse LU
-// One CTA factors the n x n row-major matrix in place (partial pivoting).
-__global__ void __launch_bounds__(1024) k_dense_lu(int n, double *A, int *piv, int *flags) {
+// Blocked right-looking LU with partial pivoting (panel width LU_NB), row-major
+// n x n in global memory:
+//   k_lu_panel   one block factors the (n-k0) x nb panel held in shared memory
+//   k_lu_swap    applies the panel's row interchanges to the other columns
+//   k_lu_trsm    U12 = L11^{-1} A12 (one thread per column)
+//   k_lu_gemm    A22 -= L21 U12 (32 x 32 output tiles)
+// then the inverse is formed column tile by column tile (k_lu_inverse):
+// P e_c, forward substitution with L, back substitution with U, the
+// right-hand sides kept in shared memory.
+constexpr int LU_NB = 32;
+constexpr int LU_MAX_N = 864;  // panel (n x 32 doubles) must fit in 227 KB of shared memory
+
+__global__ void __launch_bounds__(1024) k_lu_panel(int n, int k0, int nb, double *A, int *piv, int *flags) {
+  extern __shared__ double S[];  // m x nb, row-major
   __shared__ double sval[32];
   __shared__ int sidx[32];
   __shared__ int spiv;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int k = 0; k < n; k++) {
-    // pivot search in column k
+  const int m = n - k0, tid = threadIdx.x, nt = blockDim.x;
+  for (int t = tid; t < m * nb; t += nt) S[t] = A[(size_t)(k0 + t / nb) * n + k0 + t % nb];
+  __syncthreads();
+  for (int j = 0; j < nb; j++) {
     double best = -1.0;
-    int bi = k;
-    for (int i = k + tid; i < n; i += nt) {
-      double v = fabs(A[(size_t)i * n + k]);
+    int bi = j;
+    for (int i = j + tid; i < m; i += nt) {
+      double v = fabs(S[i * nb + j]);
       if (v > best) { best = v; bi = i; }
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -46,64 +60,123 @@ __global__ void __launch_bounds__(1024) k_dense_lu(int n, double *A, int *piv, i
     __syncthreads();
     if (tid == 0) {
       double b = -1.0;
-      int p = k;
-      for (int w = 0; w < (nt + 31) / 32; w++)
+      int p = j;
+      for (int w = 0; w < nt / 32; w++)
         if (sval[w] > b || (sval[w] == b && sidx[w] < p)) { b = sval[w]; p = sidx[w]; }
       spiv = p;
-      piv[k] = p;
+      piv[k0 + j] = k0 + p;
       if (!(b > 0.0)) atomicOr(flags, 16);
     }
     __syncthreads();
     const int p = spiv;
-    if (p != k)
-      for (int j = tid; j < n; j += nt) {
-        double t = A[(size_t)k * n + j];
-        A[(size_t)k * n + j] = A[(size_t)p * n + j];
-        A[(size_t)p * n + j] = t;
-      }
-    __syncthreads();
-    const double inv = 1.0 / A[(size_t)k * n + k];
-    for (int i = k + 1 + tid; i < n; i += nt) A[(size_t)i * n + k] *= inv;
-    __syncthreads();
-    const int m = n - k - 1;
-    for (int t = tid; t < m * m; t += nt) {
-      int i = k + 1 + t / m, j = k + 1 + t % m;
-      A[(size_t)i * n + j] -= A[(size_t)i * n + k] * A[(size_t)k * n + j];
+    if (p != j && tid < nb) {
+      double t = S[j * nb + tid];
+      S[j * nb + tid] = S[p * nb + tid];
+      S[p * nb + tid] = t;
     }
     __syncthreads();
+    const double d = S[j * nb + j];
+    const double inv = d != 0.0 ? 1.0 / d : 0.0;
+    for (int i = j + 1 + tid; i < m; i += nt) S[i * nb + j] *= inv;
+    __syncthreads();
+    const int w = nb - j - 1;
+    if (w > 0)
+      for (int t = tid; t < (m - j - 1) * w; t += nt) {
+        const int i = j + 1 + t / w, c = j + 1 + t % w;
+        S[i * nb + c] -= S[i * nb + j] * S[j * nb + c];
+      }
+    __syncthreads();
+  }
+  for (int t = tid; t < m * nb; t += nt) A[(size_t)(k0 + t / nb) * n + k0 + t % nb] = S[t];
+}
+
+// row interchanges of panel k0 on the columns outside the panel
+__global__ void k_lu_swap(int n, int k0, int nb, double *A, const int *__restrict__ piv) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n || (c >= k0 && c < k0 + nb)) return;
+  for (int j = 0; j < nb; j++) {
+    const int p = piv[k0 + j];
+    if (p != k0 + j) {
+      double t = A[(size_t)(k0 + j) * n + c];
+      A[(size_t)(k0 + j) * n + c] = A[(size_t)p * n + c];
+      A[(size_t)p * n + c] = t;
+    }
   }
 }
 
-// Column c of the inverse: solve L U x = P e_c, one warp per column.
-__global__ void k_dense_inverse(int n, const double *__restrict__ LU, const int *__restrict__ piv, double *work,
-                                double *Inv) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  double *y = work + (size_t)warp * n;
-  // b = P e_c: apply the row swaps to e_c
-  for (int i = lane; i < n; i += 32) y[i] = (i == warp) ? 1.0 : 0.0;
+// U12 = L11^{-1} A12 for the columns right of the panel
+__global__ void k_lu_trsm(int n, int k0, int nb, double *A) {
+  __shared__ double L11[LU_NB][LU_NB];
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) L11[t / nb][t % nb] = A[(size_t)(k0 + t / nb) * n + k0 + t % nb];
+  __syncthreads();
+  const int c = k0 + nb + blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  double y[LU_NB];
+#pragma unroll
+  for (int i = 0; i < LU_NB; i++) y[i] = i < nb ? A[(size_t)(k0 + i) * n + c] : 0.0;
+#pragma unroll
+  for (int i = 1; i < LU_NB; i++)
+#pragma unroll
+    for (int j = 0; j < LU_NB; j++)
+      if (j < i && i < nb) y[i] -= L11[i][j] * y[j];
+#pragma unroll
+  for (int i = 0; i < LU_NB; i++)
+    if (i < nb) A[(size_t)(k0 + i) * n + c] = y[i];
+}
+
+// A22 -= L21 U12 on 32 x 32 tiles (k0+nb <= row, col < n)
+__global__ void __launch_bounds__(256) k_lu_gemm(int n, int k0, int nb, double *A) {
+  __shared__ double Ls[32][LU_NB + 1], Us[LU_NB][33];
+  const int r0 = k0 + nb + blockIdx.y * 32, c0 = k0 + nb + blockIdx.x * 32;
+  for (int t = threadIdx.x; t < 32 * LU_NB; t += blockDim.x) {
+    const int a = t / LU_NB, b = t % LU_NB;
+    Ls[a][b] = (r0 + a < n && b < nb) ? A[(size_t)(r0 + a) * n + k0 + b] : 0.0;
+    const int u = t / 32, v = t % 32;
+    Us[u][v] = (u < nb && c0 + v < n) ? A[(size_t)(k0 + u) * n + c0 + v] : 0.0;
+  }
+  __syncthreads();
+  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;  // 8 rows per pass
+  for (int a = ty; a < 32; a += 8) {
+    const int r = r0 + a, c = c0 + tx;
+    if (r >= n || c >= n) continue;
+    double s = 0.0;
+#pragma unroll 8
+    for (int k = 0; k < LU_NB; k++) s += Ls[a][k] * Us[k][tx];
+    A[(size_t)r * n + c] -= s;
+  }
+}
+
+// 16 columns of the inverse per block: y = P e_c, L y' = y, U x = y'
+constexpr int INV_COLS = 16;
+__global__ void __launch_bounds__(32 * INV_COLS) k_lu_inverse(int n, const double *__restrict__ LU,
+                                                              const int *__restrict__ piv, double *Inv) {
+  extern __shared__ double Y[];  // n x INV_COLS
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * INV_COLS + w;
+  for (int i = lane; i < n; i += 32) Y[i * INV_COLS + w] = (i == c) ? 1.0 : 0.0;
   __syncwarp();
   if (lane == 0)
     for (int k = 0; k < n; k++) {
-      int p = piv[k];
-      if (p != k) { double t = y[k]; y[k] = y[p]; y[p] = t; }
+      const int p = piv[k];
+      if (p != k) { double t = Y[k * INV_COLS + w]; Y[k * INV_COLS + w] = Y[p * INV_COLS + w]; Y[p * INV_COLS + w] = t; }
     }
   __syncwarp();
-  for (int i = 1; i < n; i++) {  // unit lower triangle
-    double s = 0;
-    for (int j = lane; j < i; j += 32) s += LU[(size_t)i * n + j] * y[j];
+  for (int i = 1; i < n; i++) {
+    double s = 0.0;
+    for (int j = lane; j < i; j += 32) s += LU[(size_t)i * n + j] * Y[j * INV_COLS + w];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) y[i] -= s;
+    if (lane == 0) Y[i * INV_COLS + w] -= s;
     __syncwarp();
   }
-  for (int i = n - 1; i >= 0; i--) {  // upper triangle
-    double s = 0;
-    for (int j = i + 1 + lane; j < n; j += 32) s += LU[(size_t)i * n + j] * y[j];
+  for (int i = n - 1; i >= 0; i--) {
+    double s = 0.0;
+    for (int j = i + 1 + lane; j < n; j += 32) s += LU[(size_t)i * n + j] * Y[j * INV_COLS + w];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) y[i] = (y[i] - s) / LU[(size_t)i * n + i];
+    if (lane == 0) Y[i * INV_COLS + w] = (Y[i * INV_COLS + w] - s) / LU[(size_t)i * n + i];
     __syncwarp();
   }
-  for (int i = lane; i < n; i += 32) Inv[(size_t)i * n + warp] = y[i];
+  if (c < n)
+    for (int i = lane; i < n; i += 32) Inv[(size_t)i * n + c] = Y[i * INV_COLS + w];
 }
 
 __global__ void k_csr_to_dense(int n, const int *__restrict__ rp, const int *__restrict__ kc, const double *__restrict__ a,
@@ -118,6 +191,8 @@ __global__ void k_csr_to_dense(int n, const int *__restrict__ rp, const int *__r
 // x = Inv f  (dense GEMV in FP64; f, x in T)
 template <typename T>
 __global__ void __launch_bounds__(256) k_dense_apply(int n, const double *__restrict__ Inv, const T *__restrict__ f, T *x) {
+  pdl_wait();
+  pdl_trigger();
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= n) return;
   double s = 0;
@@ -128,20 +203,38 @@ __global__ void __launch_bounds__(256) k_dense_apply(int n, const double *__rest
 
 int coarse_factor(Handle &h) {
   Level &L = h.lv[0];
-  int n = L.N;
-  if (n > 4096) {
-    set_error("coarsest level too large for the dense direct solve (n > 4096)");
+  const int n = L.N;
+  if (n > LU_MAX_N) {
+    set_error("coarsest level too large for the dense direct solve (n > 864); use the SSOR coarse smoother");
     return PMG_ERR_UNSUPPORTED;
   }
   PMG_TRY(h.coarse_lu.alloc((size_t)n * n));
   PMG_TRY(h.coarse_inv.alloc((size_t)n * n));
   PMG_TRY(h.coarse_piv.alloc(n));
-  DBuf<double> work;
-  PMG_TRY(work.alloc((size_t)n * n));
   PMG_CUDA(cudaMemsetAsync(h.d_flags.p, 0, sizeof(int) * 4, h.stream));
   k_csr_to_dense<<<n, 256, 0, h.stream>>>(n, L.rowptr.p, L.kcol.p, L.A.p, h.coarse_lu.p); count_launches(1);
-  k_dense_lu<<<1, 1024, 0, h.stream>>>(n, h.coarse_lu.p, h.coarse_piv.p, h.d_flags.p); count_launches(1);
-  k_dense_inverse<<<(n * 32 + 255) / 256, 256, 0, h.stream>>>(n, h.coarse_lu.p, h.coarse_piv.p, work.p, h.coarse_inv.p); count_launches(1);
+  static bool attr = false;
+  if (!attr) {
+    PMG_CUDA(cudaFuncSetAttribute(k_lu_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, LU_MAX_N * LU_NB * 8));
+    PMG_CUDA(cudaFuncSetAttribute(k_lu_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, LU_MAX_N * INV_COLS * 8));
+    attr = true;
+  }
+  for (int k0 = 0; k0 < n; k0 += LU_NB) {
+    const int nb = std::min(LU_NB, n - k0);
+    k_lu_panel<<<1, 1024, (size_t)(n - k0) * nb * 8, h.stream>>>(n, k0, nb, h.coarse_lu.p, h.coarse_piv.p, h.d_flags.p);
+    k_lu_swap<<<(n + 255) / 256, 256, 0, h.stream>>>(n, k0, nb, h.coarse_lu.p, h.coarse_piv.p);
+    count_launches(2);
+    const int rest = n - k0 - nb;
+    if (rest > 0) {
+      k_lu_trsm<<<(rest + 127) / 128, 128, 0, h.stream>>>(n, k0, nb, h.coarse_lu.p);
+      dim3 g((rest + 31) / 32, (rest + 31) / 32);
+      k_lu_gemm<<<g, 256, 0, h.stream>>>(n, k0, nb, h.coarse_lu.p);
+      count_launches(2);
+    }
+  }
+  k_lu_inverse<<<(n + INV_COLS - 1) / INV_COLS, 32 * INV_COLS, (size_t)n * INV_COLS * 8, h.stream>>>(
+      n, h.coarse_lu.p, h.coarse_piv.p, h.coarse_inv.p);
+  count_launches(1);
   PMG_CUDA(cudaGetLastError());
   int flags[4];
   PMG_CUDA(cudaMemcpyAsync(flags, h.d_flags.p, sizeof(flags), cudaMemcpyDeviceToHost, h.stream));
@@ -182,24 +275,26 @@ static int vcycle(Handle &h, int i) {
   using PT = Prec<T>;
   if (i == 0) {
     if (h.prm.coarse_smoother == PMG_COARSE_DIRECT) {
-      k_dense_apply<T><<<(L.N * 32 + 255) / 256, 256, 0, s>>>(L.N, h.coarse_inv.p, PT::f(L), PT::x(L)); count_launches(1);
+      PMG_CUDA(launch_pdl(k_dense_apply<T>, dim3((L.N * 32 + 255) / 256), dim3(256), 0, s, L.N,
+                          (const double *)h.coarse_inv.p, (const T *)PT::f(L), PT::x(L)));
+      count_launches(1);
       PMG_CUDA(cudaGetLastError());
     } else {
       int it = h.prm.coarse_maxit > 0 ? h.prm.coarse_maxit : 1;
-      for (int k = 0; k < it; k++) PMG_TRY(ssor_sweep<T>(s, L, PT::A(L), PT::invd(L), PT::f(L), PT::x(L), h.prm.smooth_omega));
+      for (int k = 0; k < it; k++) PMG_TRY(sell_ssor<T>(s, L, PT::f(L), PT::x(L), h.prm.smooth_omega, h.num_sms));
     }
     return PMG_OK;
   }
   Level &C = h.lv[i - 1];
   for (int k = 0; k < h.prm.pre_smooth; k++)
-    PMG_TRY(ssor_sweep<T>(s, L, PT::A(L), PT::invd(L), PT::f(L), PT::x(L), h.prm.smooth_omega));
-  PMG_TRY(defect<T>(s, L, PT::A(L), PT::x(L), PT::f(L), PT::d(L)));
+    PMG_TRY(sell_ssor<T>(s, L, PT::f(L), PT::x(L), h.prm.smooth_omega, h.num_sms));
+  PMG_TRY(sell_spmv<T>(s, L, PT::x(L), PT::f(L), PT::d(L), 1, h.num_sms));
   PMG_TRY(restrict_defect<T>(s, L, C, PT::R(L), PT::d(L), PT::f(C)));
   PMG_TRY(zero<T>(s, PT::x(C), C.N));
   PMG_TRY(vcycle<T>(h, i - 1));
   PMG_TRY(prolongate_add<T>(s, L, PT::P(L), PT::x(C), PT::x(L), h.prm.gmg_damp));
   for (int k = 0; k < h.prm.post_smooth; k++)
-    PMG_TRY(ssor_sweep<T>(s, L, PT::A(L), PT::invd(L), PT::f(L), PT::x(L), h.prm.smooth_omega));
+    PMG_TRY(sell_ssor<T>(s, L, PT::f(L), PT::x(L), h.prm.smooth_omega, h.num_sms));
   return PMG_OK;
 }
 
@@ -237,23 +332,26 @@ static int prepare_levels(Handle &h) {
     }
     PMG_TRY(L.x64.alloc(L.N)); PMG_TRY(L.f64.alloc(L.N)); PMG_TRY(L.d64.alloc(L.N));
     if (fp32) {
-      PMG_TRY(L.A32.alloc(L.nnz));
-      PMG_TRY(convert_f64_f32(h.stream, L.A.p, L.A32.p, L.nnz));
+      PMG_TRY(sell_values<float>(h, L));
       PMG_TRY(L.x32.alloc(L.N)); PMG_TRY(L.f32.alloc(L.N)); PMG_TRY(L.d32.alloc(L.N));
-      if (i > 0) {
+      if (i > 0 && !L.pval32.p) {
         PMG_TRY(L.pval32.alloc(L.pval.n));
         PMG_TRY(convert_f64_f32(h.stream, L.pval.p, L.pval32.p, L.pval.n));
         PMG_TRY(L.rval32.alloc(L.rval.n));
         PMG_TRY(convert_f64_f32(h.stream, L.rval.p, L.rval32.p, L.rval.n));
       }
+    } else {
+      PMG_TRY(sell_values<double>(h, L));
     }
-    PMG_TRY(level_invdiag(h.stream, L, h.d_flags.p));
   }
+  // the outer Krylov method multiplies with the FP64 finest matrix
+  PMG_TRY(sell_values<double>(h, h.lv.back()));
   if (h.prm.coarse_smoother == PMG_COARSE_DIRECT && !h.coarse_ready) PMG_TRY(coarse_factor(h));
   return PMG_OK;
 }
 
 static int capture_vcycle(Handle &h) {
+  if (!h.use_graph) return PMG_OK;
   if (h.vgraph && h.vgraph_prec == h.prm.precision) return PMG_OK;
   if (h.vgraph) { cudaGraphExecDestroy(h.vgraph); h.vgraph = nullptr; }
   cudaGraph_t g;
@@ -277,15 +375,24 @@ static int capture_vcycle(Handle &h) {
 static int precondition(Handle &h, const double *v, double *z) {
   Level &F = h.lv.back();
   int nb = (F.N + 255) / 256;
+  const int top = (int)h.lv.size() - 1;
   if (h.prm.precision == PMG_PREC_FP32) {
     k_prec_in32<<<nb, 256, 0, h.stream>>>(F.Na, F.N, v, F.f32.p, F.x32.p); count_launches(1);
-    PMG_CUDA(cudaGraphLaunch(h.vgraph, h.stream));
-    count_launches(h.vgraph_kernels);
+    if (h.use_graph) {
+      PMG_CUDA(cudaGraphLaunch(h.vgraph, h.stream));
+      count_launches(h.vgraph_kernels);
+    } else {
+      PMG_TRY(vcycle<float>(h, top));
+    }
     k_prec_out32<<<nb, 256, 0, h.stream>>>(F.N, F.x32.p, z); count_launches(1);
   } else {
     k_prec_in64<<<nb, 256, 0, h.stream>>>(F.Na, F.N, v, F.f64.p, F.x64.p); count_launches(1);
-    PMG_CUDA(cudaGraphLaunch(h.vgraph, h.stream));
-    count_launches(h.vgraph_kernels);
+    if (h.use_graph) {
+      PMG_CUDA(cudaGraphLaunch(h.vgraph, h.stream));
+      count_launches(h.vgraph_kernels);
+    } else {
+      PMG_TRY(vcycle<double>(h, top));
+    }
     PMG_CUDA(cudaMemcpyAsync(z, F.x64.p, sizeof(double) * F.N, cudaMemcpyDeviceToDevice, h.stream));
   }
   PMG_CUDA(cudaGetLastError());
@@ -310,6 +417,9 @@ static void givens(double &dx, double &dy, double &cs, double &sn) {
 
 int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *st) {
   if (h.lv.empty()) { set_error("solve: no levels"); return PMG_ERR_STATE; }
+  // the solve's device time covers everything below: per-solve set-up (SELL
+  // values, coarsest factorisation), the iteration and the final true residual
+  PMG_CUDA(cudaEventRecord(h.ev[2], h.stream));
   PMG_TRY(prepare_levels(h));
   PMG_TRY(capture_vcycle(h));
   Level &F = h.lv.back();
@@ -333,7 +443,6 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
   else PMG_TRY(zero<double>(s, h.sol.p, N));
   // Dirichlet part of the start vector = rhs (TSystemCD3D::Assemble copies it, SystemCD3D.C:361)
   PMG_TRY(copy_dirichlet(s, F.Na, F.N, h.rhs.p, h.sol.p));
-  PMG_CUDA(cudaEventRecord(h.ev[2], s));
 
   double *V = h.V.p, *Z = h.Z.p, *w = h.w.p;
   double *Hd = h.H.p;  // column i at Hd + i*(m+1); scratch scalars after (m+1)^2
@@ -342,7 +451,7 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
   double *hcol = h.h_H;
 
   auto residual = [&](double *out_vec, double &nrm) -> int {
-    PMG_TRY(defect<double>(s, F, F.A.p, h.sol.p, h.rhs.p, out_vec));
+    PMG_TRY(sell_spmv<double>(s, F, h.sol.p, h.rhs.p, out_vec, 1, h.num_sms));
     PMG_TRY(dot(h, out_vec, out_vec, N, sc));
     PMG_CUDA(cudaMemcpyAsync(hcol, sc, sizeof(double), cudaMemcpyDeviceToHost, s));
     PMG_CUDA(cudaStreamSynchronize(s));
@@ -368,7 +477,7 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
     for (i = 0; i < m && j <= maxit; i++, j++) {
       double *vi = V + (size_t)i * N, *zi = Z + (size_t)i * N;
       PMG_TRY(precondition(h, vi, zi));
-      PMG_TRY(spmv<double>(s, F, F.A.p, zi, w));
+      PMG_TRY(sell_spmv<double>(s, F, zi, nullptr, w, 0, h.num_sms));
       double *Hc = Hd + (size_t)i * (m + 1);
       for (int k = 0; k <= i; k++) {
         PMG_TRY(dot(h, w, V + (size_t)k * N, N, Hc + k));
@@ -420,9 +529,9 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
     PMG_TRY(residual(V, beta));  // restart
     r0 = beta;
   }
-  PMG_CUDA(cudaEventRecord(h.ev[3], s));
   double res_final;
   PMG_TRY(residual(w, res_final));
+  PMG_CUDA(cudaEventRecord(h.ev[3], s));
   float ms = 0;
   PMG_CUDA(cudaEventElapsedTime(&ms, h.ev[2], h.ev[3]));
   h.t_solve = ms * 1e-3;

@@ -141,6 +141,8 @@ template int ssor_sweep<float>(cudaStream_t, const Level &, const float *, const
 template <int W, typename T>
 __global__ void __launch_bounds__(256) k_restrict(int Nc, int Nac, const int *__restrict__ rp, const int *__restrict__ col,
                                                   const T *__restrict__ val, const T *__restrict__ d, T *__restrict__ fc) {
+  pdl_wait();
+  pdl_trigger();
   const int lane = threadIdx.x & (W - 1);
   for (int base = warp_first_row<W>(); base < Nc; base += rows_per_grid<W>()) {
     const int row = base + (threadIdx.x & 31) / W;
@@ -158,6 +160,8 @@ template <int W, typename T>
 __global__ void __launch_bounds__(256) k_prolong_add(int Naf, const int *__restrict__ rp, const int *__restrict__ col,
                                                      const T *__restrict__ val, const T *__restrict__ xc,
                                                      T *__restrict__ xf, T damp) {
+  pdl_wait();
+  pdl_trigger();
   const int lane = threadIdx.x & (W - 1);
   for (int base = warp_first_row<W>(); base < Naf; base += rows_per_grid<W>()) {
     const int row = base + (threadIdx.x & 31) / W;
@@ -175,14 +179,18 @@ template <typename T>
 int restrict_defect(cudaStream_t s, const Level &Lf, const Level &Lc, const T *rval, const T *d, T *fc) {
   // R = P^T has up to 27 (Q1) / 125 (Q2) entries per coarse row
   int g = grid_for(Lc.N, 16, 148);
-  k_restrict<16, T><<<g, 256, 0, s>>>(Lc.N, Lc.Na, Lf.rrp.p, Lf.rcol.p, rval, d, fc); count_launches(1);
+  PMG_CUDA(launch_pdl(k_restrict<16, T>, dim3(g), dim3(256), 0, s, Lc.N, Lc.Na, (const int *)Lf.rrp.p,
+                      (const int *)Lf.rcol.p, rval, d, fc));
+  count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
 template <typename T>
 int prolongate_add(cudaStream_t s, const Level &Lf, const T *pval, const T *xc, T *xf, double damp) {
   int g = grid_for(Lf.Na, 8, 148);
-  k_prolong_add<8, T><<<g, 256, 0, s>>>(Lf.Na, Lf.prp.p, Lf.pcol.p, pval, xc, xf, (T)damp); count_launches(1);
+  PMG_CUDA(launch_pdl(k_prolong_add<8, T>, dim3(g), dim3(256), 0, s, Lf.Na, (const int *)Lf.prp.p,
+                      (const int *)Lf.pcol.p, pval, xc, xf, (T)damp));
+  count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
