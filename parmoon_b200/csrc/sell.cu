@@ -145,18 +145,18 @@ template int sell_values<double>(Handle &, Level &);
 
 // A block of K warps owns one slice: warp w accumulates the column steps
 // j = w, w+K, ... of the slice's 32 rows (coalesced 32-wide loads), the K
-// partial sums meet in shared memory and warp 0 finishes the rows.  K warps
-// per slice keep K times more loads in flight than one thread per row, which
-// a single colour (1/27 of the rows) needs to stream at HBM rate.
-constexpr int SELL_K = 4;
+// partial sums meet in shared memory and warp 0 finishes the rows.  K is
+// chosen per launch (4, 8 or 16): small colours get more warps per slice so
+// that each warp's chain of dependent loads (column index, then x) stays
+// short; large colours already fill the GPU with K = 4.
 
 // y = A x (MODE 0) or d = f - A x (MODE 1) over slices [s0, s1)
-template <typename T, int MODE>
-__global__ void __launch_bounds__(32 * SELL_K) k_sell_mv(int s0, int s1, const int *__restrict__ perm,
-                                                         const int *__restrict__ sptr, const int *__restrict__ col,
-                                                         const T *__restrict__ val, const T *__restrict__ x,
-                                                         const T *__restrict__ f, T *__restrict__ y) {
-  __shared__ T part[SELL_K][32];
+template <typename T, int MODE, int K>
+__global__ void __launch_bounds__(32 * K) k_sell_mv(int s0, int s1, const int *__restrict__ perm,
+                                                    const int *__restrict__ sptr, const int *__restrict__ col,
+                                                    const T *__restrict__ val, const T *__restrict__ x,
+                                                    const T *__restrict__ f, T *__restrict__ y) {
+  __shared__ T part[K][32];
   pdl_wait();
   pdl_trigger();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -166,12 +166,12 @@ __global__ void __launch_bounds__(32 * SELL_K) k_sell_mv(int s0, int s1, const i
     const T *v = val + off + lane;
     T sum = 0;
 #pragma unroll 4
-    for (int j = w; j < lmax; j += SELL_K) sum += __ldg(v + 32 * j) * __ldg(x + __ldg(c + 32 * j));
+    for (int j = w; j < lmax; j += K) sum += __ldg(v + 32 * j) * __ldg(x + __ldg(c + 32 * j));
     part[w][lane] = sum;
     __syncthreads();
     if (w == 0) {
 #pragma unroll
-      for (int k = 1; k < SELL_K; k++) sum += part[k][lane];
+      for (int k = 1; k < K; k++) sum += part[k][lane];
       const int r = __ldg(perm + s * 32 + lane);
       if (r >= 0) y[r] = MODE ? __ldg(f + r) - sum : sum;
     }
@@ -180,12 +180,12 @@ __global__ void __launch_bounds__(32 * SELL_K) k_sell_mv(int s0, int s1, const i
 }
 
 // Gauss-Seidel update of the rows of one colour (slices [s0, s1))
-template <typename T>
-__global__ void __launch_bounds__(32 * SELL_K) k_sell_gs(int s0, int s1, const int *__restrict__ perm,
-                                                         const int *__restrict__ sptr, const int *__restrict__ col,
-                                                         const T *__restrict__ val, const T *__restrict__ invd,
-                                                         const T *__restrict__ f, T *x, T omega) {
-  __shared__ T part[SELL_K][32];
+template <typename T, int K>
+__global__ void __launch_bounds__(32 * K) k_sell_gs(int s0, int s1, const int *__restrict__ perm,
+                                                    const int *__restrict__ sptr, const int *__restrict__ col,
+                                                    const T *__restrict__ val, const T *__restrict__ invd,
+                                                    const T *__restrict__ f, T *x, T omega) {
+  __shared__ T part[K][32];
   pdl_wait();
   pdl_trigger();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -194,18 +194,33 @@ __global__ void __launch_bounds__(32 * SELL_K) k_sell_gs(int s0, int s1, const i
     const int *c = col + off + lane;
     const T *v = val + off + lane;
     T sum = 0;
-#pragma unroll 4
-    for (int j = w; j < lmax; j += SELL_K) sum += __ldg(v + 32 * j) * x[__ldg(c + 32 * j)];
+#pragma unroll(K <= 4 ? 16 : 8)
+    for (int j = w; j < lmax; j += K) sum += __ldg(v + 32 * j) * x[__ldg(c + 32 * j)];
     part[w][lane] = sum;
     __syncthreads();
     if (w == 0) {
 #pragma unroll
-      for (int k = 1; k < SELL_K; k++) sum += part[k][lane];
+      for (int k = 1; k < K; k++) sum += part[k][lane];
       const int r = __ldg(perm + s * 32 + lane);
       if (r >= 0) x[r] += omega * (__ldg(f + r) - sum) * __ldg(invd + s * 32 + lane);
     }
     __syncthreads();
   }
+}
+
+// warps per slice for a launch over `slices` slices: the smallest K (>= 2)
+// that still gives every SM 32 warps
+static int pick_k(int slices, int num_sms) {
+  static int kmin = -1;
+  if (kmin < 0) {
+    const char *e = getenv("PMG_SELL_KMIN");
+    kmin = e ? atoi(e) : 2;
+    if (kmin != 4 && kmin != 8 && kmin != 16) kmin = 2;
+  }
+  const long want = 32L * num_sms;  // warps to keep the load pipes busy
+  int k = kmin;
+  while (k < 16 && (long)slices * k < want) k *= 2;
+  return k;
 }
 
 template <typename T>
@@ -216,8 +231,8 @@ __global__ void k_sell_copy_dirichlet(int Na, int N, const T *__restrict__ f, T 
   if (i < N) x[i] = f[i];
 }
 
-static int slice_grid(int nslices, int num_sms) {
-  int cap = num_sms * 64;  // 16 resident blocks of 4 warps per SM, 4 waves
+static int slice_grid(int nslices, int num_sms, int k) {
+  int cap = num_sms * (256 / k);  // 64 resident warps per SM, 4 waves
   return std::max(1, std::min(nslices, cap));
 }
 
@@ -232,19 +247,25 @@ static const T *sell_invd(const Level &L) {
   return reinterpret_cast<const T *>(L.sell_invd64.p);
 }
 
+template <typename T, int MODE, int K>
+static cudaError_t launch_mv(cudaStream_t s, const Level &L, const T *x, const T *f, T *y, int num_sms) {
+  const int n = L.sell_nslices;
+  return launch_pdl(k_sell_mv<T, MODE, K>, dim3(slice_grid(n, num_sms, K)), dim3(32 * K), 0, s, 0, n,
+                    (const int *)L.sell_perm.p, (const int *)L.sell_ptr.p, (const int *)L.sell_col.p, sell_val<T>(L),
+                    x, f, y);
+}
+
 template <typename T>
 int sell_spmv(cudaStream_t s, const Level &L, const T *x, const T *f, T *y, int mode, int num_sms) {
-  const int n = L.sell_nslices;
-  if (mode)
-    PMG_CUDA(launch_pdl(k_sell_mv<T, 1>, dim3(slice_grid(n, num_sms)), dim3(32 * SELL_K), 0, s, 0, n,
-                        (const int *)L.sell_perm.p, (const int *)L.sell_ptr.p, (const int *)L.sell_col.p,
-                        sell_val<T>(L), x, f, y));
-  else
-    PMG_CUDA(launch_pdl(k_sell_mv<T, 0>, dim3(slice_grid(n, num_sms)), dim3(32 * SELL_K), 0, s, 0, n,
-                        (const int *)L.sell_perm.p, (const int *)L.sell_ptr.p, (const int *)L.sell_col.p,
-                        sell_val<T>(L), x, f, y));
+  int k = pick_k(L.sell_nslices, num_sms);
+  cudaError_t e;
+  if (k < 4) k = 4;  // a full-matrix product has enough slices for K = 4
+  if (mode) e = k == 16 ? launch_mv<T, 1, 16>(s, L, x, f, y, num_sms) : k == 8 ? launch_mv<T, 1, 8>(s, L, x, f, y, num_sms)
+                                                                             : launch_mv<T, 1, 4>(s, L, x, f, y, num_sms);
+  else e = k == 16 ? launch_mv<T, 0, 16>(s, L, x, f, y, num_sms) : k == 8 ? launch_mv<T, 0, 8>(s, L, x, f, y, num_sms)
+                                                                          : launch_mv<T, 0, 4>(s, L, x, f, y, num_sms);
+  PMG_CUDA(e);
   count_launches(1);
-  PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
 template int sell_spmv<float>(cudaStream_t, const Level &, const float *, const float *, float *, int, int);
@@ -264,9 +285,15 @@ int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, in
       const int c = pass == 0 ? cc : nc - 1 - cc;
       const int s0 = L.sell_group[c], s1 = L.sell_group[c + 1];
       if (s1 <= s0) continue;
-      PMG_CUDA(launch_pdl(k_sell_gs<T>, dim3(slice_grid(s1 - s0, num_sms)), dim3(32 * SELL_K), 0, s, s0, s1,
-                          (const int *)L.sell_perm.p, (const int *)L.sell_ptr.p, (const int *)L.sell_col.p,
-                          sell_val<T>(L), sell_invd<T>(L), f, x, (T)omega));
+      const int k = pick_k(s1 - s0, num_sms);
+      cudaError_t e;
+#define PMG_GS(K_)                                                                                              \
+  launch_pdl(k_sell_gs<T, K_>, dim3(slice_grid(s1 - s0, num_sms, K_)), dim3(32 * K_), 0, s, s0, s1,           \
+             (const int *)L.sell_perm.p, (const int *)L.sell_ptr.p, (const int *)L.sell_col.p, sell_val<T>(L),  \
+             sell_invd<T>(L), f, x, (T)omega)
+      e = k == 16 ? PMG_GS(16) : k == 8 ? PMG_GS(8) : k == 4 ? PMG_GS(4) : PMG_GS(2);
+#undef PMG_GS
+      PMG_CUDA(e);
       count_launches(1);
     }
   PMG_CUDA(cudaGetLastError());

@@ -532,6 +532,7 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
   double res_final;
   PMG_TRY(residual(w, res_final));
   PMG_CUDA(cudaEventRecord(h.ev[3], s));
+  PMG_CUDA(cudaEventSynchronize(h.ev[3]));
   float ms = 0;
   PMG_CUDA(cudaEventElapsedTime(&ms, h.ev[2], h.ev[3]));
   h.t_solve = ms * 1e-3;
