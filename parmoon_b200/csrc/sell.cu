@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(32 * K) k_sell_gs(int s0, int s1, const int *_
     const int *c = col + off + lane;
     const T *v = val + off + lane;
     T sum = 0;
-#pragma unroll(K <= 4 ? 16 : 8)
+#pragma unroll 8
     for (int j = w; j < lmax; j += K) sum += __ldg(v + 32 * j) * x[__ldg(c + 32 * j)];
     part[w][lane] = sum;
     __syncthreads();
@@ -208,14 +208,15 @@ __global__ void __launch_bounds__(32 * K) k_sell_gs(int s0, int s1, const int *_
   }
 }
 
-// warps per slice for a launch over `slices` slices: the smallest K (>= 2)
-// that still gives every SM 32 warps
+// warps per slice for a launch over `slices` slices: the smallest K (>= 4;
+// K = 2 and deeper unrolling measured slower on the 64^3 finest level) that
+// still gives every SM 32 warps
 static int pick_k(int slices, int num_sms) {
   static int kmin = -1;
   if (kmin < 0) {
     const char *e = getenv("PMG_SELL_KMIN");
-    kmin = e ? atoi(e) : 2;
-    if (kmin != 4 && kmin != 8 && kmin != 16) kmin = 2;
+    kmin = e ? atoi(e) : 4;
+    if (kmin != 2 && kmin != 8 && kmin != 16) kmin = 4;
   }
   const long want = 32L * num_sms;  // warps to keep the load pipes busy
   int k = kmin;
