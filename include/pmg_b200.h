@@ -101,6 +101,8 @@ typedef struct pmg_params {
     int    poly_degree;        /* INTERNAL_POLYNOMIAL_DEGREE used in the SUPG delta */
     double delta0;             /* DELTA0 */
     int    reference_restart_rule; /* 1: FGMRES restart resets r0 like FgmresIte.C:546-566; 0: always relative to the first r0 */
+    int    problem_linear;     /* INTERNAL_PROBLEM_LINEAR: 1 -> Q1 Gauss2 / Q2 Gauss3 / P1 Keast4 / P2 Keast11,
+                                  0 -> Q1 Gauss3 / Q2 Gauss4 / P1 Keast11 (FEDatabase3D.C:1203-1309) */
 } pmg_params;
 
 typedef struct pmg_solve_stats {
@@ -177,13 +179,23 @@ int pmg_set_matrix(pmg_handle h, int level, int which, const double *entries);
 int pmg_get_rhs(pmg_handle h, int level, double *rhs_out);
 /* which: 0 = system matrix A, 1 = mass matrix M (time-dependent problems) */
 
-/* TSystemTCD3D::AssembleSystMat (src/System/SystemTCD3D.C:260-326):
- *   rhs := tau*theta4*f_new + tau*theta3*f_old + (M - tau*theta2*A) u_old  (active rows)
- *   A   := M + tau*theta1*A on every level (active rows), Dirichlet rows untouched.
- * f_old/u_old are host arrays of the finest level (NULL: use the device copies
- * kept from the previous step). */
+/* TSystemTCD3D::AssembleSystMat (src/System/SystemTCD3D.C:260-326), after
+ * pmg_assemble of the mass form (AssembleMRhs) and of the stiffness form at
+ * the new time (AssembleARhs):
+ *   B := tau*theta3*f_old + tau*theta4*f_new + (M - tau*theta2*A) u_old   (active rows)
+ *   B := f_new, start vector := f_new                                  (Dirichlet rows)
+ *   A := M + tau*theta1*A on every level (active rows; A is kept for
+ *   pmg_tcd_restore).  B becomes the finest level's rhs for pmg_solve, whose
+ *   start vector (sol == NULL) is u_old.  f_old / u_old: host arrays of the
+ *   finest level, or NULL for the device copies (f_old = the rhs of the
+ *   previous pmg_tcd_system call or of the mass assembly, u_old = the last
+ *   solution).  rhs_out (optional) receives B. */
 int pmg_tcd_system(pmg_handle h, double tau, const double theta[4],
                    const double *f_old, const double *u_old, double *rhs_out);
+
+/* TSystemTCD3D::RestoreMassMat (src/System/SystemTCD3D.C:328-347): the
+ * stiffness matrices saved by pmg_tcd_system are put back on every level. */
+int pmg_tcd_restore(pmg_handle h);
 
 /* ------------------------------------------------------------ kernels */
 /* MatVect_Scalar / Defect_Scalar plug-ins (src/FE/Blas2.C:86-126) on the

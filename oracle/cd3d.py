@@ -202,3 +202,15 @@ def fgmres_mg(levels, rhs, sol0=None, pre=2, post=2, coarse_maxit=10, coarse_red
                              _i(maxit), _i(restart), _d(div), _i(int(reference_restart_rule)), _ptr(hist),
                              ctypes.byref(res))
     return sol, it, res.value, hist
+
+
+def errors(elem, elem_dof, cell_vert, sol, quad, exact_kind, t=0.0):
+    """(L2, H1-semi) errors of a finite-element function (GetErrors + L2H1Errors restated)."""
+    elem_dof = np.ascontiguousarray(elem_dof, dtype=np.int32)
+    out = np.zeros(2)
+    rc = lib().orc_errors(_i(elem), _i(elem_dof.size // nloc_of(elem)), _ptr(elem_dof),
+                          _ptr(np.ascontiguousarray(cell_vert, dtype=np.float64)),
+                          _ptr(np.ascontiguousarray(sol, dtype=np.float64)), _i(quad), _i(exact_kind), _d(t), _ptr(out))
+    if rc != 0:
+        raise RuntimeError("orc_errors failed")
+    return out

@@ -35,7 +35,7 @@ class Params(ctypes.Structure):
                 ("coarse_maxit", _i), ("coarse_red", _d), ("smooth_omega", _d), ("gmg_damp", _d),
                 ("lin_red", _d), ("lin_res_min", _d), ("lin_maxit", _i), ("restart", _i), ("div_factor", _d),
                 ("precision", _i), ("sdfem_type", _i), ("poly_degree", _i), ("delta0", _d),
-                ("reference_restart_rule", _i)]
+                ("reference_restart_rule", _i), ("problem_linear", _i)]
 
 
 class CoeffDesc(ctypes.Structure):
@@ -229,6 +229,18 @@ class Handle:
         if raise_on_error and rc != OK:
             _check(rc)
         return sol, st, rc
+
+    def tcd_system(self, tau, theta, f_old=None, u_old=None):
+        """TSystemTCD3D::AssembleSystMat on the device; returns the right-hand side B."""
+        th = (ctypes.c_double * 4)(*theta)
+        f_old = None if f_old is None else _c_f64(f_old)
+        u_old = None if u_old is None else _c_f64(u_old)
+        B = np.empty(self.sizes[-1][0])
+        _check(lib().pmg_tcd_system(self.h, _d(tau), th, _ptr(f_old), _ptr(u_old), _ptr(B)))
+        return B
+
+    def tcd_restore(self):
+        _check(lib().pmg_tcd_restore(self.h))
 
     def get_solution(self):
         x = np.empty(self.sizes[-1][0])

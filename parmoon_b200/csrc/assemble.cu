@@ -394,12 +394,14 @@ struct TableCache {
 };
 static TableCache g_tab[4];
 
-static int rule_for(int elem) {
+// quadrature rule of the reference (TFEDatabase3D::GetOrig, FEDatabase3D.C:1203-1309):
+// degree N_terms * polynomial degree with N_terms = 2 (INTERNAL_PROBLEM_LINEAR) or 3
+static int rule_for(int elem, int problem_linear) {
   switch (elem) {
-    case PMG_ELEM_Q1_HEX: return RULE_GAUSS2;
-    case PMG_ELEM_Q2_HEX: return RULE_GAUSS3;
-    case PMG_ELEM_P1_TET: return RULE_KEAST4;
-    default: return RULE_KEAST11;
+    case PMG_ELEM_Q1_HEX: return problem_linear ? RULE_GAUSS2 : RULE_GAUSS3;
+    case PMG_ELEM_Q2_HEX: return problem_linear ? RULE_GAUSS3 : RULE_GAUSS4;
+    case PMG_ELEM_P1_TET: return problem_linear ? RULE_KEAST4 : RULE_KEAST11;
+    default: return problem_linear ? RULE_KEAST11 : -1;  // P5Tetra (degree 6) is not built
   }
 }
 
@@ -470,7 +472,12 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
   }
   if (!L.slot.p) PMG_TRY(build_slot_map(h, L));
   TableCache *T = nullptr;
-  PMG_TRY(get_tables(L.elem, rule_for(L.elem), T));
+  const int rule = rule_for(L.elem, h.prm.problem_linear);
+  if (rule < 0) {
+    set_error("assemble: the degree-6 tetrahedral rule (P2 with INTERNAL_PROBLEM_LINEAR = 0) is not built");
+    return PMG_ERR_UNSUPPORTED;
+  }
+  PMG_TRY(get_tables(L.elem, rule, T));
   PMG_CUDA(cudaMemsetAsync(target, 0, sizeof(double) * L.nnz, h.stream));
   if (rhs_target && zero_rhs) PMG_CUDA(cudaMemsetAsync(rhs_target, 0, sizeof(double) * L.N, h.stream));
   PMG_CUDA(cudaMemsetAsync(h.d_flags.p, 0, sizeof(int) * 4, h.stream));
@@ -496,12 +503,15 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
   a.utab = T->utab.p;
   a.qtab = T->qtab.p;
   a.flags = h.d_flags.p;
-  switch (L.elem) {
-    case PMG_ELEM_Q1_HEX: PMG_TRY((launch_assemble<PMG_ELEM_Q1_HEX, 8>(h, L, a))); break;
-    case PMG_ELEM_Q2_HEX: PMG_TRY((launch_assemble<PMG_ELEM_Q2_HEX, 27>(h, L, a))); break;
-    case PMG_ELEM_P1_TET: PMG_TRY((launch_assemble<PMG_ELEM_P1_TET, 4>(h, L, a))); break;
-    case PMG_ELEM_P2_TET: PMG_TRY((launch_assemble<PMG_ELEM_P2_TET, 11>(h, L, a))); break;
-    default: set_error("assemble: unknown element"); return PMG_ERR_ARG;
+  switch (L.elem * 1000 + T->nq) {
+    case PMG_ELEM_Q1_HEX * 1000 + 8: PMG_TRY((launch_assemble<PMG_ELEM_Q1_HEX, 8>(h, L, a))); break;
+    case PMG_ELEM_Q1_HEX * 1000 + 27: PMG_TRY((launch_assemble<PMG_ELEM_Q1_HEX, 27>(h, L, a))); break;
+    case PMG_ELEM_Q2_HEX * 1000 + 27: PMG_TRY((launch_assemble<PMG_ELEM_Q2_HEX, 27>(h, L, a))); break;
+    case PMG_ELEM_Q2_HEX * 1000 + 64: PMG_TRY((launch_assemble<PMG_ELEM_Q2_HEX, 64>(h, L, a))); break;
+    case PMG_ELEM_P1_TET * 1000 + 4: PMG_TRY((launch_assemble<PMG_ELEM_P1_TET, 4>(h, L, a))); break;
+    case PMG_ELEM_P1_TET * 1000 + 11: PMG_TRY((launch_assemble<PMG_ELEM_P1_TET, 11>(h, L, a))); break;
+    case PMG_ELEM_P2_TET * 1000 + 11: PMG_TRY((launch_assemble<PMG_ELEM_P2_TET, 11>(h, L, a))); break;
+    default: set_error("assemble: no kernel for this element / quadrature rule"); return PMG_ERR_UNSUPPORTED;
   }
   return PMG_OK;
 }

@@ -16,7 +16,7 @@
 
 namespace pmg {
 
-enum { RULE_GAUSS2 = 2, RULE_GAUSS3 = 3, RULE_KEAST4 = 104, RULE_KEAST5 = 105, RULE_KEAST11 = 111 };
+enum { RULE_GAUSS2 = 2, RULE_GAUSS3 = 3, RULE_GAUSS4 = 4, RULE_KEAST4 = 104, RULE_KEAST5 = 105, RULE_KEAST11 = 111 };
 
 struct QuadRule {
   int n = 0;
@@ -28,11 +28,18 @@ inline QuadRule make_rule(int rule) {
   auto push = [&](double w, double x, double y, double z) {
     q.w.push_back(w); q.x.push_back(x); q.y.push_back(y); q.z.push_back(z); q.n++;
   };
-  if (rule == RULE_GAUSS2 || rule == RULE_GAUSS3) {
+  if (rule == RULE_GAUSS2 || rule == RULE_GAUSS3 || rule == RULE_GAUSS4) {
     int n = rule;
-    double gw[3], gx[3];
+    double gw[4], gx[4];
     if (n == 2) { gw[0] = gw[1] = 1.0; gx[0] = -1.0 / std::sqrt(3.0); gx[1] = 1.0 / std::sqrt(3.0); }
-    else { gw[0] = gw[2] = 5.0 / 9.0; gw[1] = 8.0 / 9.0; gx[0] = -std::sqrt(0.6); gx[1] = 0; gx[2] = std::sqrt(0.6); }
+    else if (n == 3) { gw[0] = gw[2] = 5.0 / 9.0; gw[1] = 8.0 / 9.0; gx[0] = -std::sqrt(0.6); gx[1] = 0; gx[2] = std::sqrt(0.6); }
+    else {
+      // 4-point Gauss-Legendre: nodes +-sqrt(3/7 -+ 2/7 sqrt(6/5)), weights (18 +- sqrt(30))/36
+      double a = std::sqrt(3.0 / 7.0 - 2.0 / 7.0 * std::sqrt(1.2)), b = std::sqrt(3.0 / 7.0 + 2.0 / 7.0 * std::sqrt(1.2));
+      double wa = (18.0 + std::sqrt(30.0)) / 36.0, wb = (18.0 - std::sqrt(30.0)) / 36.0;
+      gx[0] = -b; gx[1] = -a; gx[2] = a; gx[3] = b;
+      gw[0] = wb; gw[1] = wa; gw[2] = wa; gw[3] = wb;
+    }
     for (int i = 0; i < n; i++)
       for (int j = 0; j < n; j++)
         for (int k = 0; k < n; k++) push(gw[i] * gw[j] * gw[k], gx[k], gx[j], gx[i]);

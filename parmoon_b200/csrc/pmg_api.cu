@@ -126,6 +126,7 @@ void pmg_default_params(pmg_params *p) {
   p->poly_degree = 0;                    // 0: element degree
   p->delta0 = 1.0;                       // DELTA0 (Database.C:480)
   p->reference_restart_rule = 0;
+  p->problem_linear = 1;                 // the configs' quadrature (Gauss2 for Q1, Gauss3 for Q2)
 }
 
 int pmg_create(pmg_handle *out, int n_levels, const pmg_params *p) {
@@ -395,6 +396,11 @@ static int assemble_one(Handle *h, int level, int form, double *entries_out, dou
   PMG_CUDA(cudaMemcpyAsync(flags, h->d_flags.p, sizeof(flags), cudaMemcpyDeviceToHost, h->stream));
   PMG_CUDA(cudaStreamSynchronize(h->stream));
   if (flags[0] & 1) { set_error("assemble: element coupling missing from the CSR pattern"); return PMG_ERR_SLOT; }
+  if (mass && level == (int)h->lv.size() - 1) {
+    // f(t_0) of the mass assembly is the first f_old of the theta scheme (AssembleMRhs)
+    PMG_TRY(h->tcd_fold.alloc(L.N));
+    PMG_CUDA(cudaMemcpyAsync(h->tcd_fold.p, L.rhs.p, sizeof(double) * L.N, cudaMemcpyDeviceToDevice, h->stream));
+  }
   if (!mass) {
     L.assembled = true;
     L.sell_val_fresh32 = L.sell_val_fresh64 = false;
@@ -653,10 +659,6 @@ int pmg_time_kernel(pmg_handle hh, int kernel, int level, int form, int reps, do
   return PMG_OK;
 }
 
-int pmg_tcd_system(pmg_handle, double, const double *, const double *, const double *, double *) {
-  set_error("pmg_tcd_system: not built yet");
-  return PMG_ERR_UNSUPPORTED;
-}
 int pmg_set_level_lattice(pmg_handle, int, int, int, int, const int *) {
   set_error("pmg_set_level_lattice: not built yet");
   return PMG_ERR_UNSUPPORTED;

@@ -173,6 +173,9 @@ struct Handle {
   bool has_learned = false;
   double *h_pinned = nullptr;
   size_t h_pinned_n = 0;
+  // time-dependent state (tcd.cu): previous rhs, start vector preset, system assembled
+  DBuf<double> tcd_fold;
+  bool sol_preset = false, tcd_active = false;
 };
 
 // ------------------------------------------------------------- kernels (assemble.cu)

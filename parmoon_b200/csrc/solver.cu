@@ -440,7 +440,8 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
   if (rhs_host) PMG_CUDA(cudaMemcpyAsync(h.rhs.p, rhs_host, sizeof(double) * N, cudaMemcpyHostToDevice, s));
   else PMG_CUDA(cudaMemcpyAsync(h.rhs.p, F.rhs.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
   if (sol_host) PMG_CUDA(cudaMemcpyAsync(h.sol.p, sol_host, sizeof(double) * N, cudaMemcpyHostToDevice, s));
-  else PMG_TRY(zero<double>(s, h.sol.p, N));
+  else if (!h.sol_preset) PMG_TRY(zero<double>(s, h.sol.p, N));  // (pmg_tcd_system presets u_old)
+  h.sol_preset = false;
   // Dirichlet part of the start vector = rhs (TSystemCD3D::Assemble copies it, SystemCD3D.C:361)
   PMG_TRY(copy_dirichlet(s, F.Na, F.N, h.rhs.p, h.sol.p));
 
