@@ -239,12 +239,30 @@ int pmg_solve(pmg_handle h, double *sol, const double *rhs, pmg_solve_stats *sta
 int pmg_get_solution(pmg_handle h, double *sol_out);
 
 /* ------------------------------------------------------------ learned smoother */
-/* Lattice description for the stencil-network smoother of one level: for
- * each dof its (i,j,k) index on the level's node lattice (nx x ny x nz). */
-int pmg_set_level_lattice(pmg_handle h, int level, int nx, int ny, int nz, const int *dof_ijk);
-/* Network weights (BF16-stored, see pmg_learned_num_params for the layout). */
+/* No counterpart in the reference.  A stencil network maps each node's
+ * normalised matrix stencil to a 27-point correction stencil W; with
+ * params.smoother = PMG_SMOOTHER_LEARNED every pre/post smoothing step is
+ * x += omega W (f - A x).  The solve measures the per-cycle contraction of
+ * the first cycles with SSOR and with the learned step and keeps SSOR when
+ * the learned one contracts worse (stats.smoother_used tells which ran).
+ * Levels need one dof per node of a cubic n1^3 lattice (Q1 hexahedra):
+ * dof_lat[d] = i + n1 (j + n1 k) for dof d. */
+int pmg_set_level_lattice(pmg_handle h, int level, int nx, int ny, int nz, const int *dof_lat);
+/* Network parameters: conv 27->32, 32->32, 32->27 (3x3x3 each) with biases,
+ * flat FP32 array [W1 b1 W2 b2 W3 b3], W laid out [c_out][c_in][27]. */
 int pmg_learned_num_params(int *n);
 int pmg_set_learned_weights(pmg_handle h, const float *weights);
+int pmg_get_learned_weights(pmg_handle h, float *weights);
+/* Stencil W of a level, 27 x N floats (lattice order, channel-major). */
+int pmg_learned_stencil(pmg_handle h, int level, float *W_out);
+/* One training step on a level from n_samples (error, residual = A error)
+ * pairs in device memory (n_samples x N doubles each): loss = mean |A (e -
+ * W r)|^2 / |r|^2; lr > 0 applies an Adam step on the device. */
+int pmg_learned_train_step(pmg_handle h, int level, int n_samples, const double *e_dev, const double *r_dev, float lr,
+                           double *loss_out, float *grad_out);
+/* One V-cycle z = MG(v) (the preconditioner) on device vectors of the
+ * finest level (TMultiGridScaIte::Iterate with zero start). */
+int pmg_vcycle(pmg_handle h, const double *v_dev, double *z_dev);
 
 /* ------------------------------------------------------------ timing */
 /* Device time in seconds of the last pmg_assemble / pmg_solve call, and the

@@ -242,6 +242,37 @@ class Handle:
     def tcd_restore(self):
         _check(lib().pmg_tcd_restore(self.h))
 
+    # ---------------------------------------------------------------- learned smoother
+    def set_lattice(self, level, n1, dof_lat):
+        dof_lat = _c_i32(dof_lat)
+        _check(lib().pmg_set_level_lattice(self.h, _i(level), _i(n1), _i(n1), _i(n1), _ptr(dof_lat)))
+
+    def set_learned_weights(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _check(lib().pmg_set_learned_weights(self.h, _ptr(w)))
+
+    def get_learned_weights(self):
+        w = np.empty(learned_num_params(), dtype=np.float32)
+        _check(lib().pmg_get_learned_weights(self.h, _ptr(w)))
+        return w
+
+    def learned_stencil(self, level):
+        W = np.empty(27 * self.sizes[level][0], dtype=np.float32)
+        _check(lib().pmg_learned_stencil(self.h, _i(level), _ptr(W)))
+        return W.reshape(27, -1)
+
+    def learned_train_step(self, level, e_ptr, r_ptr, n_samples, lr, want_grad=False):
+        """One device training step from device arrays (n_samples x N doubles); returns (loss, grad or None)."""
+        loss = _d()
+        g = np.empty(learned_num_params(), dtype=np.float32) if want_grad else None
+        _check(lib().pmg_learned_train_step(self.h, _i(level), _i(n_samples), _p(e_ptr), _p(r_ptr),
+                                            ctypes.c_float(lr), ctypes.byref(loss), _ptr(g)))
+        return loss.value, g
+
+    def vcycle(self, v_ptr, z_ptr):
+        """z = MG(v) on device vectors of the finest level."""
+        _check(lib().pmg_vcycle(self.h, _p(v_ptr), _p(z_ptr)))
+
     def get_solution(self):
         x = np.empty(self.sizes[-1][0])
         _check(lib().pmg_get_solution(self.h, _ptr(x)))
@@ -251,6 +282,12 @@ class Handle:
         a, s, k = _d(), _d(), _d()
         _check(lib().pmg_last_timings(self.h, ctypes.byref(a), ctypes.byref(s), ctypes.byref(k)))
         return a.value, s.value, k.value
+
+
+def learned_num_params():
+    n = _i()
+    _check(lib().pmg_learned_num_params(ctypes.byref(n)))
+    return n.value
 
 
 # ------------------------------------------------------------------ structured set-up (host, C++)

@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <cstdio>
 #include <cstring>
 #include <atomic>
 #include <mutex>
@@ -26,6 +27,19 @@ unsigned long long launches_so_far() { return g_launches.load(); }
 int level_invdiag(cudaStream_t s, Level &L, int *flags);
 
 static Handle *H(pmg_handle h) { return reinterpret_cast<Handle *>(h); }
+
+// PMG_TRACE=1 prints the progress of the set-up calls (diagnostics)
+static bool tracing() {
+  static int t = -1;
+  if (t < 0) { const char *e = getenv("PMG_TRACE"); t = (e && e[0] == '1') ? 1 : 0; }
+  return t == 1;
+}
+#define PMG_TRACE_AT(tag) do { if (tracing()) { fprintf(stderr, "[pmg] %s:%d %s\n", __func__, __LINE__, tag); fflush(stderr); } } while (0)
+
+static void invalidate_graphs(Handle *h) {
+  if (h->vgraph) { cudaGraphExecDestroy(h->vgraph); h->vgraph = nullptr; }
+  if (h->vgraph_ssor) { cudaGraphExecDestroy(h->vgraph_ssor); h->vgraph_ssor = nullptr; }
+}
 
 static int check_level(Handle *h, int level) {
   if (!h) { set_error("null handle"); return PMG_ERR_ARG; }
@@ -169,6 +183,7 @@ int pmg_destroy(pmg_handle hh) {
   if (!h) return PMG_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->vgraph) cudaGraphExecDestroy(h->vgraph);
+  if (h->vgraph_ssor) cudaGraphExecDestroy(h->vgraph_ssor);
   for (int k = 0; k < 6; k++) if (h->ev[k]) cudaEventDestroy(h->ev[k]);
   if (h->h_H) cudaFreeHost(h->h_H);
   h->lv.clear();
@@ -186,7 +201,7 @@ int pmg_set_params(pmg_handle hh, const pmg_params *p) {
                      p->smooth_omega != h->prm.smooth_omega || p->gmg_damp != h->prm.gmg_damp ||
                      p->coarse_maxit != h->prm.coarse_maxit || p->smoother != h->prm.smoother;
   h->prm = *p;
-  if (graph_shape && h->vgraph) { cudaGraphExecDestroy(h->vgraph); h->vgraph = nullptr; }
+  if (graph_shape) invalidate_graphs(h);
   return PMG_OK;
 }
 
@@ -238,6 +253,7 @@ int pmg_set_level_mesh(pmg_handle hh, int level, int elem_type, int n_cells, con
 
 int pmg_set_level_csr(pmg_handle hh, int level, int n_rows, int active_bound, const int *row_ptr, const int *kcol) {
   Handle *h = H(hh);
+  PMG_TRACE_AT("enter");
   PMG_TRY(check_level(h, level));
   if (n_rows <= 0 || active_bound < 0 || active_bound > n_rows || !row_ptr || !kcol) {
     set_error("pmg_set_level_csr: bad sizes");
@@ -258,6 +274,7 @@ int pmg_set_level_csr(pmg_handle hh, int level, int n_rows, int active_bound, co
     }
     if (dpos[r] < 0) { set_error("pmg_set_level_csr: missing diagonal entry"); return PMG_ERR_ARG; }
   }
+  PMG_TRACE_AT("validated");
   Level &L = h->lv[level];
   L.N = n_rows;
   L.Na = active_bound;
@@ -268,20 +285,25 @@ int pmg_set_level_csr(pmg_handle hh, int level, int n_rows, int active_bound, co
   PMG_TRY(L.diagpos.upload(dpos.data(), n_rows, h->stream));
   PMG_TRY(L.A.alloc(nnz));
   PMG_TRY(L.rhs.alloc(n_rows));
+  PMG_TRACE_AT("uploaded");
   PMG_CUDA(cudaMemsetAsync(L.A.p, 0, sizeof(double) * nnz, h->stream));
   PMG_CUDA(cudaMemsetAsync(L.rhs.p, 0, sizeof(double) * n_rows, h->stream));
   int ncol = 0;
   std::vector<int> color = color_rows(n_rows, active_bound, row_ptr, kcol, ncol);
+  PMG_TRACE_AT("coloured");
   PMG_TRY(upload_row_colors(h, L, ncol, color));
+  PMG_TRACE_AT("colours uploaded");
   L.h_rowptr.assign(row_ptr, row_ptr + n_rows + 1);
   L.h_kcol.assign(kcol, kcol + nnz);
+  PMG_TRACE_AT("host copies");
   L.sell_ready = false;
   L.has_csr = true;
   L.has_mesh = false;
   L.slot.release();
   L.assembled = false;
   h->coarse_ready = false;
-  if (h->vgraph) { cudaGraphExecDestroy(h->vgraph); h->vgraph = nullptr; }
+  invalidate_graphs(h);
+  PMG_TRACE_AT("done");
   return PMG_OK;
 }
 
@@ -302,7 +324,7 @@ int pmg_set_level_row_colors(pmg_handle hh, int level, int n_colors, const int *
       }
   }
   PMG_TRY(upload_row_colors(h, L, n_colors, c));
-  if (h->vgraph) { cudaGraphExecDestroy(h->vgraph); h->vgraph = nullptr; }
+  invalidate_graphs(h);
   return PMG_OK;
 }
 
@@ -340,7 +362,7 @@ int pmg_set_transfer(pmg_handle hh, int level, int n_fine, int n_coarse, const i
   PMG_CUDA(cudaStreamSynchronize(h->stream));
   L.Nc = n_coarse;
   L.has_P = true;
-  if (h->vgraph) { cudaGraphExecDestroy(h->vgraph); h->vgraph = nullptr; }
+  invalidate_graphs(h);
   return PMG_OK;
 }
 
@@ -404,6 +426,7 @@ static int assemble_one(Handle *h, int level, int form, double *entries_out, dou
   if (!mass) {
     L.assembled = true;
     L.sell_val_fresh32 = L.sell_val_fresh64 = false;
+    L.lw_fresh = false;
     if (level == 0) h->coarse_ready = false;
   }
   if (entries_out) PMG_CUDA(cudaMemcpyAsync(entries_out, target, sizeof(double) * L.nnz, cudaMemcpyDeviceToHost, h->stream));
@@ -451,6 +474,7 @@ int pmg_set_matrix(pmg_handle hh, int level, int which, const double *in) {
     PMG_TRY(L.A.upload(in, L.nnz, h->stream));
     L.assembled = true;
     L.sell_val_fresh32 = L.sell_val_fresh64 = false;
+    L.lw_fresh = false;
     if (level == 0) h->coarse_ready = false;
   }
   PMG_CUDA(cudaStreamSynchronize(h->stream));
@@ -653,23 +677,11 @@ int pmg_time_kernel(pmg_handle hh, int kernel, int level, int form, int reps, do
   if (flops) *flops = fl;
   if (kernel == PMG_KERNEL_ASSEMBLE) {
     L.sell_val_fresh32 = L.sell_val_fresh64 = false;
+    L.lw_fresh = false;
     PMG_TRY(set_dirichlet_rows(*h, L, L.A.p, L.rhs.p));
     PMG_CUDA(cudaStreamSynchronize(s));
   }
   return PMG_OK;
-}
-
-int pmg_set_level_lattice(pmg_handle, int, int, int, int, const int *) {
-  set_error("pmg_set_level_lattice: not built yet");
-  return PMG_ERR_UNSUPPORTED;
-}
-int pmg_learned_num_params(int *n) {
-  if (n) *n = 0;
-  return PMG_ERR_UNSUPPORTED;
-}
-int pmg_set_learned_weights(pmg_handle, const float *) {
-  set_error("learned smoother: not built yet");
-  return PMG_ERR_UNSUPPORTED;
 }
 
 }  // extern "C"

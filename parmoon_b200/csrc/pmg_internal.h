@@ -122,9 +122,11 @@ struct Level {
   // work vectors of the V-cycle (FP64 and FP32)
   DBuf<double> x64, f64, d64;
   DBuf<float> x32, f32, d32;
-  // lattice (learned smoother)
+  // lattice and stencil of the learned smoother (learned.cu)
   int lat_n[3] = {0, 0, 0};
-  DBuf<int> dof_ijk;
+  DBuf<int> dof_ijk, lat_dof, tpos;
+  DBuf<float> lw_stencil;
+  bool lw_fresh = false;
   // average row length (SpMV launch shape)
   int avg_row = 0;
   // host copies of the pattern and of the colour row lists (SELL set-up)
@@ -137,6 +139,24 @@ struct Level {
   DBuf<int> sell_perm, sell_ptr, sell_col;
   DBuf<float> sell_val32, sell_invd32;
   DBuf<double> sell_val64, sell_invd64;
+};
+
+// activations of the stencil network on one lattice (learned.cu)
+struct NetScratch {
+  DBuf<float> feat, a1, z1, a2, z2, out3, dscale;
+  int NL = 0;
+  int alloc(int nl, int c0, int c1, int c2, int c3) {
+    if (nl == NL) return PMG_OK;
+    PMG_TRY(feat.alloc((size_t)c0 * nl));
+    PMG_TRY(a1.alloc((size_t)c1 * nl));
+    PMG_TRY(z1.alloc((size_t)c1 * nl));
+    PMG_TRY(a2.alloc((size_t)c2 * nl));
+    PMG_TRY(z2.alloc((size_t)c2 * nl));
+    PMG_TRY(out3.alloc((size_t)c3 * nl));
+    PMG_TRY(dscale.alloc(nl));
+    NL = nl;
+    return PMG_OK;
+  }
 };
 
 struct Handle {
@@ -168,9 +188,15 @@ struct Handle {
   int vgraph_prec = -1;
   unsigned long long vgraph_kernels = 0;
   bool use_graph = true;  // PMG_NO_GRAPH=1 launches the V-cycle kernels directly (profilers)
-  // learned smoother weights
-  DBuf<float> lw;
+  // learned smoother: BF16 weights used by the kernels, FP32 master copy, Adam state
+  DBuf<uint16_t> lw_bf16;
+  DBuf<float> lw_master, lw_grad, lw_m, lw_v;
   bool has_learned = false;
+  long adam_t = 0;
+  NetScratch net_scratch;
+  // learned-smoother guard: V-cycle graph with SSOR, active choice
+  cudaGraphExec_t vgraph_ssor = nullptr;
+  unsigned long long vgraph_ssor_kernels = 0;
   double *h_pinned = nullptr;
   size_t h_pinned_n = 0;
   // time-dependent state (tcd.cu): previous rhs, start vector preset, system assembled
@@ -221,5 +247,8 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
 
 // ------------------------------------------------------------- learned smoother (learned.cu)
 int learned_num_params();
+int learned_prepare(Handle &h);
+template <typename T>
+int learned_smooth(cudaStream_t s, const Level &L, const T *r, T *x, double omega);
 
 }  // namespace pmg

@@ -268,8 +268,17 @@ template <> struct Prec<float> {
   static const float *R(const Level &L) { return L.rval32.p; }
 };
 
+// one pre/post smoothing step: SSOR, or x += omega W (f - A x) with the learned stencil
 template <typename T>
-static int vcycle(Handle &h, int i) {
+static int smooth_step(Handle &h, Level &L, bool learned) {
+  using PT = Prec<T>;
+  if (!learned) return sell_ssor<T>(h.stream, L, PT::f(L), PT::x(L), h.prm.smooth_omega, h.num_sms);
+  PMG_TRY(sell_spmv<T>(h.stream, L, PT::x(L), PT::f(L), PT::d(L), 1, h.num_sms));
+  return learned_smooth<T>(h.stream, L, PT::d(L), PT::x(L), h.prm.smooth_omega);
+}
+
+template <typename T>
+static int vcycle(Handle &h, int i, bool learned) {
   cudaStream_t s = h.stream;
   Level &L = h.lv[i];
   using PT = Prec<T>;
@@ -281,20 +290,18 @@ static int vcycle(Handle &h, int i) {
       PMG_CUDA(cudaGetLastError());
     } else {
       int it = h.prm.coarse_maxit > 0 ? h.prm.coarse_maxit : 1;
-      for (int k = 0; k < it; k++) PMG_TRY(sell_ssor<T>(s, L, PT::f(L), PT::x(L), h.prm.smooth_omega, h.num_sms));
+      for (int k = 0; k < it; k++) PMG_TRY(smooth_step<T>(h, L, learned));
     }
     return PMG_OK;
   }
   Level &C = h.lv[i - 1];
-  for (int k = 0; k < h.prm.pre_smooth; k++)
-    PMG_TRY(sell_ssor<T>(s, L, PT::f(L), PT::x(L), h.prm.smooth_omega, h.num_sms));
+  for (int k = 0; k < h.prm.pre_smooth; k++) PMG_TRY(smooth_step<T>(h, L, learned));
   PMG_TRY(sell_spmv<T>(s, L, PT::x(L), PT::f(L), PT::d(L), 1, h.num_sms));
   PMG_TRY(restrict_defect<T>(s, L, C, PT::R(L), PT::d(L), PT::f(C)));
   PMG_TRY(zero<T>(s, PT::x(C), C.N));
-  PMG_TRY(vcycle<T>(h, i - 1));
+  PMG_TRY(vcycle<T>(h, i - 1, learned));
   PMG_TRY(prolongate_add<T>(s, L, PT::P(L), PT::x(C), PT::x(L), h.prm.gmg_damp));
-  for (int k = 0; k < h.prm.post_smooth; k++)
-    PMG_TRY(sell_ssor<T>(s, L, PT::f(L), PT::x(L), h.prm.smooth_omega, h.num_sms));
+  for (int k = 0; k < h.prm.post_smooth; k++) PMG_TRY(smooth_step<T>(h, L, learned));
   return PMG_OK;
 }
 
@@ -346,52 +353,63 @@ static int prepare_levels(Handle &h) {
   }
   // the outer Krylov method multiplies with the FP64 finest matrix
   PMG_TRY(sell_values<double>(h, h.lv.back()));
+  if (h.prm.smoother == PMG_SMOOTHER_LEARNED) PMG_TRY(learned_prepare(h));
   if (h.prm.coarse_smoother == PMG_COARSE_DIRECT && !h.coarse_ready) PMG_TRY(coarse_factor(h));
+  return PMG_OK;
+}
+
+static int capture_one(Handle &h, bool learned, cudaGraphExec_t &exec, unsigned long long &kernels) {
+  if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+  cudaGraph_t g;
+  const unsigned long long before = launches_so_far();
+  PMG_CUDA(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal));
+  int top = (int)h.lv.size() - 1;
+  int rc = h.prm.precision == PMG_PREC_FP32 ? vcycle<float>(h, top, learned) : vcycle<double>(h, top, learned);
+  cudaError_t e = cudaStreamEndCapture(h.stream, &g);
+  if (rc != PMG_OK) return rc;
+  PMG_CUDA(e);
+  PMG_CUDA(cudaGraphInstantiate(&exec, g, 0));
+  cudaGraphDestroy(g);
+  // kernels recorded during capture run at each replay, not now
+  kernels = launches_so_far() - before;
+  count_launches(0ULL - kernels);
   return PMG_OK;
 }
 
 static int capture_vcycle(Handle &h) {
   if (!h.use_graph) return PMG_OK;
+  const bool learned = h.prm.smoother == PMG_SMOOTHER_LEARNED;
   if (h.vgraph && h.vgraph_prec == h.prm.precision) return PMG_OK;
-  if (h.vgraph) { cudaGraphExecDestroy(h.vgraph); h.vgraph = nullptr; }
-  cudaGraph_t g;
-  const unsigned long long before = launches_so_far();
-  PMG_CUDA(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal));
-  int top = (int)h.lv.size() - 1;
-  int rc = h.prm.precision == PMG_PREC_FP32 ? vcycle<float>(h, top) : vcycle<double>(h, top);
-  cudaError_t e = cudaStreamEndCapture(h.stream, &g);
-  if (rc != PMG_OK) return rc;
-  PMG_CUDA(e);
-  PMG_CUDA(cudaGraphInstantiate(&h.vgraph, g, 0));
-  cudaGraphDestroy(g);
-  // kernels recorded during capture run at each replay, not now
-  h.vgraph_kernels = launches_so_far() - before;
-  count_launches(0ULL - h.vgraph_kernels);
+  PMG_TRY(capture_one(h, learned, h.vgraph, h.vgraph_kernels));
+  if (learned) PMG_TRY(capture_one(h, false, h.vgraph_ssor, h.vgraph_ssor_kernels));
   h.vgraph_prec = h.prm.precision;
   return PMG_OK;
 }
 
 // z = MG(v): one V-cycle with zero start (MultiGridScaIte.C:89-130)
-static int precondition(Handle &h, const double *v, double *z) {
+static int precondition(Handle &h, const double *v, double *z, bool learned) {
   Level &F = h.lv.back();
+  cudaGraphExec_t graph = learned ? h.vgraph : (h.prm.smoother == PMG_SMOOTHER_LEARNED ? h.vgraph_ssor : h.vgraph);
+  const unsigned long long nk = learned ? h.vgraph_kernels
+                                        : (h.prm.smoother == PMG_SMOOTHER_LEARNED ? h.vgraph_ssor_kernels : h.vgraph_kernels);
   int nb = (F.N + 255) / 256;
   const int top = (int)h.lv.size() - 1;
   if (h.prm.precision == PMG_PREC_FP32) {
     k_prec_in32<<<nb, 256, 0, h.stream>>>(F.Na, F.N, v, F.f32.p, F.x32.p); count_launches(1);
     if (h.use_graph) {
-      PMG_CUDA(cudaGraphLaunch(h.vgraph, h.stream));
-      count_launches(h.vgraph_kernels);
+      PMG_CUDA(cudaGraphLaunch(graph, h.stream));
+      count_launches(nk);
     } else {
-      PMG_TRY(vcycle<float>(h, top));
+      PMG_TRY(vcycle<float>(h, top, learned));
     }
     k_prec_out32<<<nb, 256, 0, h.stream>>>(F.N, F.x32.p, z); count_launches(1);
   } else {
     k_prec_in64<<<nb, 256, 0, h.stream>>>(F.Na, F.N, v, F.f64.p, F.x64.p); count_launches(1);
     if (h.use_graph) {
-      PMG_CUDA(cudaGraphLaunch(h.vgraph, h.stream));
-      count_launches(h.vgraph_kernels);
+      PMG_CUDA(cudaGraphLaunch(graph, h.stream));
+      count_launches(nk);
     } else {
-      PMG_TRY(vcycle<double>(h, top));
+      PMG_TRY(vcycle<double>(h, top, learned));
     }
     PMG_CUDA(cudaMemcpyAsync(z, F.x64.p, sizeof(double) * F.N, cudaMemcpyDeviceToDevice, h.stream));
   }
@@ -460,9 +478,16 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
     return PMG_OK;
   };
 
+  // learned smoother guard: 0 = calibrating with SSOR, 1 = learned, 2 = SSOR took over
+  const bool learned = h.prm.smoother == PMG_SMOOTHER_LEARNED;
+  const int kCalib = 2;
+  int guard_phase = learned ? 0 : 2, learned_start = 0;
+  double rho_plain = 0.0;
+  std::vector<double> res_hist;
   double beta;
   PMG_TRY(residual(V, beta));
   const double res0 = beta;
+  res_hist.push_back(beta);
   double r0 = beta, res = beta;
   int j = 1, status = PMG_ERR_NOT_CONVERGED, iters = 0;
   const double red = h.prm.lin_red, rmin = h.prm.lin_res_min;
@@ -477,7 +502,7 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
     bool done = false;
     for (i = 0; i < m && j <= maxit; i++, j++) {
       double *vi = V + (size_t)i * N, *zi = Z + (size_t)i * N;
-      PMG_TRY(precondition(h, vi, zi));
+      PMG_TRY(precondition(h, vi, zi, guard_phase == 1));
       PMG_TRY(sell_spmv<double>(s, F, zi, nullptr, w, 0, h.num_sms));
       double *Hc = Hd + (size_t)i * (m + 1);
       for (int k = 0; k <= i; k++) {
@@ -506,6 +531,17 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
       }
       res = fabs(sv[i + 1]);
       iters = j;
+      res_hist.push_back(res);
+      if (guard_phase == 0 && learned && j == kCalib) {
+        // per-cycle contraction of the plain SSOR V-cycle over the first cycles
+        rho_plain = pow(res / res_hist[0], 1.0 / kCalib);
+        guard_phase = 1;
+        learned_start = j;
+      } else if (guard_phase == 1 && j - learned_start >= 2) {
+        const int nl = j - learned_start;
+        const double rho_l = pow(res / res_hist[learned_start], 1.0 / nl);
+        if (rho_l > rho_plain) guard_phase = 2;  // the plain SSOR smoother takes over
+      }
       if (!std::isfinite(res)) { status = PMG_ERR_NONFINITE; set_error("solve: non-finite residual estimate"); done = true; i++; break; }
       double ref = h.prm.reference_restart_rule ? r0 : res0;
       if (res < rmin || res < red * ref) { status = PMG_OK; done = true; i++; break; }
@@ -545,10 +581,20 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
     st->res_final = res_final;
     st->rel_res = res0 > 0 ? res_final / res0 : 0.0;
     st->mean_contraction = (iters > 0 && res0 > 0 && res_final > 0) ? pow(res_final / res0, 1.0 / iters) : 0.0;
-    st->smoother_used = h.prm.smoother;
+    st->smoother_used = (learned && guard_phase == 1) ? PMG_SMOOTHER_LEARNED : PMG_SMOOTHER_SSOR;
     st->seconds = h.t_solve;
   }
   return status;
 }
 
 }  // namespace pmg
+
+extern "C" int pmg_vcycle(pmg_handle hh, const double *v_dev, double *z_dev) {
+  pmg::Handle *h = reinterpret_cast<pmg::Handle *>(hh);
+  if (!h || !v_dev || !z_dev) return PMG_ERR_ARG;
+  PMG_TRY(pmg::prepare_levels(*h));
+  PMG_TRY(pmg::capture_vcycle(*h));
+  PMG_TRY(pmg::precondition(*h, v_dev, z_dev, h->prm.smoother == PMG_SMOOTHER_LEARNED));
+  PMG_CUDA(cudaStreamSynchronize(h->stream));
+  return PMG_OK;
+}

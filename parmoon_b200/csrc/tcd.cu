@@ -129,6 +129,7 @@ extern "C" int pmg_tcd_system(pmg_handle hh, double tau, const double theta[4], 
       count_launches(1);
     }
     L.sell_val_fresh32 = L.sell_val_fresh64 = false;
+    L.lw_fresh = false;
   }
   PMG_CUDA(cudaGetLastError());
   h->coarse_ready = false;
@@ -148,6 +149,7 @@ extern "C" int pmg_tcd_restore(pmg_handle hh) {
   for (auto &L : h->lv) {
     PMG_CUDA(cudaMemcpyAsync(L.A.p, L.Astash.p, sizeof(double) * L.nnz, cudaMemcpyDeviceToDevice, h->stream));
     L.sell_val_fresh32 = L.sell_val_fresh64 = false;
+    L.lw_fresh = false;
   }
   PMG_CUDA(cudaStreamSynchronize(h->stream));
   h->coarse_ready = false;

@@ -1,0 +1,138 @@
+"""Training driver of the learned stencil smoother (config: Q1 CD3D with SUPG,
+eps = 1e-3, convection b = curl of a seeded 8-mode Fourier vector potential
+scaled so that max|b| lies in [1, 100]).
+
+Residual / error pairs come from the plain GMG itself: starting from a random
+error e_0 (zero on Dirichlet nodes) the plain V-cycle's error propagation
+e_{k+1} = e_k - MG(A e_k) is run on the device and every (e_k, r_k = A e_k)
+is a sample.  The network is trained on the device by the library's own
+forward / backward / Adam kernels (pmg_learned_train_step); torch only holds
+device buffers.
+"""
+import numpy as np
+
+import parmoon_b200 as P
+
+EPS, N_MODES = 1e-3, 8
+
+
+def curl_modes(seed, bmax=None):
+    """8 Fourier modes of the vector potential, amplitudes scaled so max|b| = bmax."""
+    rng = np.random.default_rng(seed)
+    m = np.zeros((N_MODES, 8))
+    m[:, 0:3] = rng.integers(-2, 3, size=(N_MODES, 3))
+    m[m[:, 0:3].sum(axis=1) == 0, 0] = 1
+    m[:, 3] = rng.normal(size=N_MODES) / np.sqrt(N_MODES)
+    m[:, 4] = rng.uniform(0, 2 * np.pi, N_MODES)
+    m[:, 5:8] = rng.normal(size=(N_MODES, 3))
+    if bmax is None:
+        bmax = float(np.exp(rng.uniform(0.0, np.log(100.0))))
+    # max |curl psi| sampled on a grid, used to scale to bmax
+    g = np.linspace(0, 1, 17)
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    bx = np.zeros_like(X); by = np.zeros_like(X); bz = np.zeros_like(X)
+    for M in m:
+        arg = 2 * np.pi * (M[0] * X + M[1] * Y + M[2] * Z) + M[4]
+        s = -M[3] * np.sin(arg) * 2 * np.pi
+        gx, gy, gz = s * M[0], s * M[1], s * M[2]
+        bx += gy * M[7] - gz * M[6]
+        by += gz * M[5] - gx * M[7]
+        bz += gx * M[6] - gy * M[5]
+    peak = float(np.sqrt(bx ** 2 + by ** 2 + bz ** 2).max())
+    return m, bmax / max(peak, 1e-12)
+
+
+def init_weights(seed=0, omega=0.7):
+    """He-initialised hidden layers; the output starts as damped Jacobi (W = omega / a_ii)."""
+    rng = np.random.default_rng(seed)
+    sizes = [(32, 27), (32, 32), (27, 32)]
+    parts = []
+    for li, (co, ci) in enumerate(sizes):
+        fan_in = ci * 27
+        scale = np.sqrt(2.0 / fan_in) if li < 2 else 1e-3
+        parts.append((rng.standard_normal(co * ci * 27) * scale).astype(np.float32))
+        b = np.zeros(co, dtype=np.float32)
+        if li == 2:
+            b[13] = omega
+        parts.append(b)
+    return np.concatenate(parts)
+
+
+def make_problem(seed, n, levels, precision=P.PREC_FP32, weights=None, smoother=P.SMOOTHER_SSOR):
+    """One CD3D SUPG problem on Q1 n^3 cells: (handle, hierarchy)."""
+    modes, scale = curl_modes(seed)
+    lv = P.struct_hierarchy(P.Q1_HEX, n, levels)
+    h = P.Handle(levels, P.default_params(precision=precision, smoother=smoother))
+    h.set_coefficients(P.coeff(kind=P.COEF_CURL_FOURIER, eps=EPS, b=(scale, 0, 0), f=1.0, modes=modes))
+    P.load_hierarchy(h, lv)
+    for l, L in enumerate(lv):
+        h.set_lattice(l, L["n"] + 1, L["dof_lat"])
+    h.assemble(-1, P.FORM_SUPG, copy_out=False)
+    if weights is not None:
+        h.set_learned_weights(weights)
+    return h, lv
+
+
+def generate_pairs(h, lv, n_start, n_steps, seed):
+    """(E, R) torch tensors (n_start * n_steps x N, FP64, cuda) from the plain GMG error propagation."""
+    import torch
+    F = lv[-1]
+    N, Na = F["N"], F["active_bound"]
+    rng = np.random.default_rng(seed)
+    E, R = [], []
+    for _ in range(n_start):
+        e = rng.standard_normal(N)
+        e[Na:] = 0.0
+        for _k in range(n_steps):
+            r = h.matvec(len(lv) - 1, e)
+            r[Na:] = 0.0
+            E.append(e.copy()); R.append(r.copy())
+            rd = torch.from_numpy(r).cuda()
+            zd = torch.empty_like(rd)
+            h.vcycle(rd.data_ptr(), zd.data_ptr())
+            torch.cuda.synchronize()
+            e = e - zd.cpu().numpy()
+            e[Na:] = 0.0
+            e /= max(np.linalg.norm(e), 1e-300)
+    return torch.from_numpy(np.stack(E)).cuda(), torch.from_numpy(np.stack(R)).cuda()
+
+
+def train(problems, weights, steps, lr=1e-3, batch=4, seed=0, log_every=0):
+    """Adam on the device over (handle, E, R) problems; returns (weights, loss history)."""
+    rng = np.random.default_rng(seed)
+    for h, _, _, _ in problems:
+        h.set_learned_weights(weights)
+    hist = []
+    cur = weights
+    for it in range(steps):
+        pi = rng.integers(len(problems))
+        h, lv, E, R = problems[pi]
+        h.set_learned_weights(cur)
+        idx = rng.integers(E.shape[0] - batch + 1)
+        loss, _ = h.learned_train_step(len(lv) - 1, E[idx].data_ptr(), R[idx].data_ptr(), batch, lr)
+        cur = h.get_learned_weights()
+        hist.append(loss)
+        if log_every and it % log_every == 0:
+            print(f"step {it} loss {loss:.4f}")
+    return cur, hist
+
+
+if __name__ == "__main__":
+    import argparse
+    import os
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--problems", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--out", default=os.path.join(os.path.dirname(__file__), "weights", "stencil_net_q1.f32"))
+    a = ap.parse_args()
+    w0 = init_weights(0)
+    probs = []
+    for s in range(a.problems):
+        h, lv = make_problem(1000 + s, a.n, 4)
+        E, R = generate_pairs(h, lv, 2, 4, s)
+        probs.append((h, lv, E, R))
+    w, hist = train(probs, w0, a.steps, log_every=50)
+    os.makedirs(os.path.dirname(a.out), exist_ok=True)
+    w.astype(np.float32).tofile(a.out)
+    print("loss first/last", hist[0], np.mean(hist[-20:]))
