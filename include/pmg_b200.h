@@ -103,6 +103,7 @@ typedef struct pmg_params {
     int    reference_restart_rule; /* 1: FGMRES restart resets r0 like FgmresIte.C:546-566; 0: always relative to the first r0 */
     int    problem_linear;     /* INTERNAL_PROBLEM_LINEAR: 1 -> Q1 Gauss2 / Q2 Gauss3 / P1 Keast4 / P2 Keast11,
                                   0 -> Q1 Gauss3 / Q2 Gauss4 / P1 Keast11 (FEDatabase3D.C:1203-1309) */
+    int    learned_steps;      /* learned-smoother steps per pre/post phase (0: pre_smooth / post_smooth) */
 } pmg_params;
 
 typedef struct pmg_solve_stats {

@@ -199,7 +199,8 @@ int pmg_set_params(pmg_handle hh, const pmg_params *p) {
   bool graph_shape = p->precision != h->prm.precision || p->pre_smooth != h->prm.pre_smooth ||
                      p->post_smooth != h->prm.post_smooth || p->coarse_smoother != h->prm.coarse_smoother ||
                      p->smooth_omega != h->prm.smooth_omega || p->gmg_damp != h->prm.gmg_damp ||
-                     p->coarse_maxit != h->prm.coarse_maxit || p->smoother != h->prm.smoother;
+                     p->coarse_maxit != h->prm.coarse_maxit || p->smoother != h->prm.smoother ||
+                     p->learned_steps != h->prm.learned_steps;
   h->prm = *p;
   if (graph_shape) invalidate_graphs(h);
   return PMG_OK;

@@ -295,13 +295,15 @@ static int vcycle(Handle &h, int i, bool learned) {
     return PMG_OK;
   }
   Level &C = h.lv[i - 1];
-  for (int k = 0; k < h.prm.pre_smooth; k++) PMG_TRY(smooth_step<T>(h, L, learned));
+  const int pre = (learned && h.prm.learned_steps > 0) ? h.prm.learned_steps : h.prm.pre_smooth;
+  const int post = (learned && h.prm.learned_steps > 0) ? h.prm.learned_steps : h.prm.post_smooth;
+  for (int k = 0; k < pre; k++) PMG_TRY(smooth_step<T>(h, L, learned));
   PMG_TRY(sell_spmv<T>(s, L, PT::x(L), PT::f(L), PT::d(L), 1, h.num_sms));
   PMG_TRY(restrict_defect<T>(s, L, C, PT::R(L), PT::d(L), PT::f(C)));
   PMG_TRY(zero<T>(s, PT::x(C), C.N));
   PMG_TRY(vcycle<T>(h, i - 1, learned));
   PMG_TRY(prolongate_add<T>(s, L, PT::P(L), PT::x(C), PT::x(L), h.prm.gmg_damp));
-  for (int k = 0; k < h.prm.post_smooth; k++) PMG_TRY(smooth_step<T>(h, L, learned));
+  for (int k = 0; k < post; k++) PMG_TRY(smooth_step<T>(h, L, learned));
   return PMG_OK;
 }
 

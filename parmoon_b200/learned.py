@@ -117,22 +117,62 @@ def train(problems, weights, steps, lr=1e-3, batch=4, seed=0, log_every=0):
     return cur, hist
 
 
+def evaluate(weights, seeds, n=128, levels=5, learned_steps=(2, 4)):
+    """Time to |r|/|r0| <= 1e-10 on held-out problems: plain FP64 GMG (SSOR), FP32 SSOR
+    V-cycle and FP32 learned-smoother V-cycle (with its SSOR guard), all in FP64 FGMRES."""
+    rows = []
+    for s in seeds:
+        h, lv = make_problem(s, n, levels, precision=P.PREC_FP64, weights=weights)
+        out = {"seed": int(s), "n_dofs": int(lv[-1]["N"])}
+        variants = [("fp64_ssor", dict(precision=P.PREC_FP64)), ("fp32_ssor", dict(precision=P.PREC_FP32))]
+        for k in learned_steps:
+            variants.append((f"fp32_learned_{k}", dict(precision=P.PREC_FP32, smoother=P.SMOOTHER_LEARNED,
+                                                       learned_steps=k)))
+        for name, prm in variants:
+            h.set_params(P.default_params(**prm))
+            h.solve()  # warm-up (graph capture, SELL copies)
+            _, st, rc = h.solve()
+            out[name] = {"seconds": st.seconds, "iterations": st.iterations, "rel_res": st.rel_res,
+                         "status": rc, "smoother_used": st.smoother_used}
+        rows.append(out)
+        h.close()
+    return rows
+
+
 if __name__ == "__main__":
     import argparse
+    import json
     import os
     ap = argparse.ArgumentParser()
+    ap.add_argument("mode", choices=["train", "eval"])
     ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--levels", type=int, default=4)
     ap.add_argument("--problems", type=int, default=8)
     ap.add_argument("--steps", type=int, default=400)
-    ap.add_argument("--out", default=os.path.join(os.path.dirname(__file__), "weights", "stencil_net_q1.f32"))
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
+                                                      "stencil_net_q1.f32"))
+    ap.add_argument("--seeds", default="5000,5001,5002,5003")
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--learned-steps", default="2,4")
     a = ap.parse_args()
-    w0 = init_weights(0)
-    probs = []
-    for s in range(a.problems):
-        h, lv = make_problem(1000 + s, a.n, 4)
-        E, R = generate_pairs(h, lv, 2, 4, s)
-        probs.append((h, lv, E, R))
-    w, hist = train(probs, w0, a.steps, log_every=50)
-    os.makedirs(os.path.dirname(a.out), exist_ok=True)
-    w.astype(np.float32).tofile(a.out)
-    print("loss first/last", hist[0], np.mean(hist[-20:]))
+    if a.mode == "train":
+        w0 = init_weights(0)
+        probs = []
+        for s in range(a.problems):
+            h, lv = make_problem(1000 + s, a.n, a.levels)
+            E, R = generate_pairs(h, lv, 2, 4, s)
+            probs.append((h, lv, E, R))
+        w, hist = train(probs, w0, a.steps, lr=a.lr, log_every=50)
+        os.makedirs(os.path.dirname(a.weights), exist_ok=True)
+        w.astype(np.float32).tofile(a.weights)
+        res = {"loss_first": hist[0], "loss_last20": float(np.mean(hist[-20:])), "steps": a.steps,
+               "problems": a.problems, "n": a.n}
+    else:
+        w = np.fromfile(a.weights, dtype=np.float32)
+        res = {"rows": evaluate(w, [int(x) for x in a.seeds.split(",")], n=a.n, levels=a.levels,
+                                learned_steps=[int(x) for x in a.learned_steps.split(",")])}
+    print(json.dumps(res))
+    if a.out:
+        with open(a.out, "w") as f:
+            json.dump(res, f)
