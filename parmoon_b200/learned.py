@@ -12,34 +12,9 @@ device buffers.
 import numpy as np
 
 import parmoon_b200 as P
+from parmoon_b200.configs import curl_modes
 
-EPS, N_MODES = 1e-3, 8
-
-
-def curl_modes(seed, bmax=None):
-    """8 Fourier modes of the vector potential, amplitudes scaled so max|b| = bmax."""
-    rng = np.random.default_rng(seed)
-    m = np.zeros((N_MODES, 8))
-    m[:, 0:3] = rng.integers(-2, 3, size=(N_MODES, 3))
-    m[m[:, 0:3].sum(axis=1) == 0, 0] = 1
-    m[:, 3] = rng.normal(size=N_MODES) / np.sqrt(N_MODES)
-    m[:, 4] = rng.uniform(0, 2 * np.pi, N_MODES)
-    m[:, 5:8] = rng.normal(size=(N_MODES, 3))
-    if bmax is None:
-        bmax = float(np.exp(rng.uniform(0.0, np.log(100.0))))
-    # max |curl psi| sampled on a grid, used to scale to bmax
-    g = np.linspace(0, 1, 17)
-    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
-    bx = np.zeros_like(X); by = np.zeros_like(X); bz = np.zeros_like(X)
-    for M in m:
-        arg = 2 * np.pi * (M[0] * X + M[1] * Y + M[2] * Z) + M[4]
-        s = -M[3] * np.sin(arg) * 2 * np.pi
-        gx, gy, gz = s * M[0], s * M[1], s * M[2]
-        bx += gy * M[7] - gz * M[6]
-        by += gz * M[5] - gx * M[7]
-        bz += gx * M[6] - gy * M[5]
-    peak = float(np.sqrt(bx ** 2 + by ** 2 + bz ** 2).max())
-    return m, bmax / max(peak, 1e-12)
+EPS = 1e-3
 
 
 def init_weights(seed=0, omega=0.7):
