@@ -58,6 +58,7 @@ extern "C" {
 #define PMG_COEF_CURL_FOURIER 3  /* b = curl psi, psi = sum of Fourier modes (scaled) ; eps, c, f constant */
 #define PMG_COEF_ROTATING     4  /* b = (-(y-.5), x-.5, 0.2 sin(2 pi t)) ; eps, c, f constant */
 #define PMG_COEF_AMC          5  /* amc.h: eps=1, f=(3 pi^2 - 0.1) e^{-0.1 t} sin(pi x) cos(pi y) cos(pi z) */
+#define PMG_COEF_TABLE        6  /* values per cell and quadrature point from pmg_set_coefficient_table */
 
 typedef struct pmg_coeff_desc {
     int    kind;          /* PMG_COEF_* */
@@ -133,7 +134,7 @@ int pmg_set_params(pmg_handle h, const pmg_params *p);
 /* TFESpace3D (src/FE/FESpace3D.C:81-239): element->dof map of one level in the
  * reference's GlobalNumbers + BeginIndex form flattened to n_cells x n_loc,
  * plus each cell's vertex coordinates in the cell's own vertex order
- * (8 vertices for hexahedra, 4 for tetrahedra; n_cells x n_vert x 3).
+ * in 8 vertex slots per cell (tetrahedra use the first 4; n_cells x 8 x 3).
  * Affine maps only (HexaAffin, TetraAffin): parallelepipeds / tetrahedra.
  * brick != 0 declares every hexahedron axis-aligned (needed for SUPG on hexes,
  * whose convection-direction mesh size uses the physical trilinear interpolant). */
@@ -165,6 +166,20 @@ int pmg_set_dirichlet_values(pmg_handle h, int level, const double *values);
 
 /* CoeffFct3D stand-in (include/General/Constants.h:148-149). */
 int pmg_set_coefficients(pmg_handle h, const pmg_coeff_desc *c);
+
+/* Tabulated coefficients, for a host CoeffFct3D callback the device cannot
+ * call (TDiscreteForm3D::GetLocalForms calls it at the cell's quadrature points,
+ * src/FE/DiscreteForm3D.C:264, after GetOrig maps them, AssembleMat3D.C:461-466).
+ * pmg_quad_points returns, for the rule pmg_assemble uses with the current
+ * params (INTERNAL_PROBLEM_LINEAR), the number of points per cell and, when
+ * xyz is non-NULL, their physical coordinates: n_cells x nq x 3 in the
+ * caller's cell order of pmg_set_level_mesh, mapped as the reference maps them
+ * (HexaAffin / TetraAffin).  The caller evaluates its callback there and
+ * passes n_cells x nq x 6 values c0..c5 (eps, b1, b2, b3, c, f) to
+ * pmg_set_coefficient_table; the level's assembly reads them when the
+ * coefficient kind is PMG_COEF_TABLE (|b| is formed on the device). */
+int pmg_quad_points(pmg_handle h, int level, int *nq, double *xyz);
+int pmg_set_coefficient_table(pmg_handle h, int level, const double *values);
 
 /* ------------------------------------------------------------ assembly */
 /* TAssembleMat3D::Reset + Assemble3D (src/System/AssembleMat3D.C:261-535,

@@ -38,6 +38,16 @@ int pmg_struct_csr(int n_cells, int nloc, const int *elem_dof, int n_dofs, int a
 int pmg_struct_prolongation(int elem_type, int nc, const int *lat_c, int n_coarse, const int *lat_f, int n_fine,
                             int *p_row_ptr, int *p_col, double *p_val);
 
+/* Prolongation between nested levels of any mesh: the coarse basis of the
+ * coarse cell f_dof_cell[r] (a cell containing fine dof r, e.g. the parent of a
+ * fine cell holding it) evaluated at fine dof r's position.  Coarse cells in the
+ * pmg_set_level_mesh layout (8 vertex slots).  p_col == NULL: counts only.
+ * Replaces GetProlongationMatrix3D + Prolongate (FEDatabase3D.C:1656-1815,
+ * MGComponents3D.C:208-488) for conforming nested spaces. */
+int pmg_nested_prolongation(int elem_type, int n_coarse_cells, const int *c_elem_dof, const double *c_cell_vert,
+                            int n_coarse, int n_fine, const double *f_dof_xyz, const int *f_dof_cell,
+                            int *p_row_ptr, int *p_col, double *p_val);
+
 /* Lattice colouring for the multicolour SSOR: (i mod m, j mod m, k mod m),
  * m = degree + 1; no two coupled dofs share a colour. */
 int pmg_struct_row_colors(int elem_type, int n, int n_dofs, const int *dof_lat, int *colors, int *n_colors);

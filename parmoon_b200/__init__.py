@@ -22,7 +22,7 @@ ERR = {-1: "ARG", -2: "CUDA", -3: "STATE", -4: "NOT_CONVERGED", -5: "DIVERGED", 
        -7: "NONFINITE", -8: "SINGULAR", -9: "UNSUPPORTED"}
 Q1_HEX, Q2_HEX, P1_TET, P2_TET = 1, 2, 11, 12
 FORM_GALERKIN, FORM_SUPG, FORM_MASS, FORM_MASS_SUPG, FORM_STIFF_SUPG = 1, 2, 3, 4, 5
-COEF_CONST, COEF_SINE_RHS, COEF_LOGNORMAL, COEF_CURL_FOURIER, COEF_ROTATING, COEF_AMC = range(6)
+COEF_CONST, COEF_SINE_RHS, COEF_LOGNORMAL, COEF_CURL_FOURIER, COEF_ROTATING, COEF_AMC, COEF_TABLE = range(7)
 SMOOTHER_JACOBI, SMOOTHER_SSOR, SMOOTHER_LEARNED = 1, 3, 30
 COARSE_SSOR, COARSE_DIRECT = 3, 17
 PREC_FP64, PREC_FP32 = 0, 1
@@ -115,6 +115,7 @@ class Handle:
         _check(lib().pmg_create(ctypes.byref(self.h), _i(n_levels), ctypes.byref(self.params)))
         self.n_levels = n_levels
         self.sizes = [None] * n_levels
+        self._ncells = [0] * n_levels
 
     def close(self):
         if self.h:
@@ -145,6 +146,7 @@ class Handle:
             raise ValueError("cell_vert must hold 8 vertex slots x 3 coordinates per cell")
         _check(lib().pmg_set_level_mesh(self.h, _i(level), _i(elem_type), _i(n_cells), _ptr(elem_dof),
                                         _ptr(cell_vert), _i(int(brick))))
+        self._ncells[level] = n_cells
 
     def set_row_colors(self, level, colors, n_colors):
         colors = _c_i32(colors)
@@ -162,6 +164,20 @@ class Handle:
     def set_coefficients(self, desc):
         self._coef = desc
         _check(lib().pmg_set_coefficients(self.h, ctypes.byref(desc)))
+
+    def quad_points(self, level):
+        """Physical quadrature points of one level's assembly rule: [n_cells, nq, 3]."""
+        nq = ctypes.c_int(0)
+        _check(lib().pmg_quad_points(self.h, _i(level), ctypes.byref(nq), None))
+        nc = self._ncells[level]
+        xyz = np.empty((nc, nq.value, 3))
+        _check(lib().pmg_quad_points(self.h, _i(level), ctypes.byref(nq), _ptr(xyz)))
+        return xyz
+
+    def set_coefficient_table(self, level, values):
+        """values [n_cells, nq, 6]: eps, b1, b2, b3, c, f at each quadrature point (PMG_COEF_TABLE)."""
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        _check(lib().pmg_set_coefficient_table(self.h, _i(level), _ptr(v)))
 
     def assemble(self, level, form, copy_out=True):
         """Assemble one level (level=-1: all); returns (entries, rhs) host copies if copy_out."""
@@ -321,6 +337,23 @@ def struct_prolongation(elem, nc, lat_c, lat_f):
     val = np.empty(int(rp[-1]), dtype=np.float64)
     _check(lib().pmg_struct_prolongation(_i(elem), _i(nc), _ptr(lat_c), _i(lat_c.size), _ptr(lat_f), _i(lat_f.size),
                                          _ptr(rp), _ptr(col), _ptr(val)))
+    return rp, col, val
+
+
+def nested_prolongation(elem, c_elem_dof, c_cell_vert, n_coarse, f_dof_xyz, f_dof_cell):
+    """Interpolation from a coarse level onto the dofs of a nested fine level of any mesh:
+    f_dof_cell[r] names a coarse cell containing fine dof r.  Returns CSR (rp, col, val)."""
+    ed, cv = _c_i32(c_elem_dof), _c_f64(c_cell_vert)
+    xyz, fc = _c_f64(f_dof_xyz), _c_i32(f_dof_cell)
+    nf = fc.size
+    nloc = {Q1_HEX: 8, Q2_HEX: 27, P1_TET: 4, P2_TET: 10}[elem]
+    ncc = ed.size // nloc
+    rp = np.empty(nf + 1, dtype=np.int32)
+    args = (_i(elem), _i(ncc), _ptr(ed), _ptr(cv), _i(n_coarse), _i(nf), _ptr(xyz), _ptr(fc))
+    _check(lib().pmg_nested_prolongation(*args, _ptr(rp), None, None))
+    col = np.empty(int(rp[-1]), dtype=np.int32)
+    val = np.empty(int(rp[-1]), dtype=np.float64)
+    _check(lib().pmg_nested_prolongation(*args, _ptr(rp), _ptr(col), _ptr(val)))
     return rp, col, val
 
 

@@ -75,6 +75,20 @@ __device__ __forceinline__ void coeff_eval(const CoefDev &C, double x, double y,
   c[6] = sqrt(c[1] * c[1] + c[2] * c[2] + c[3] * c[3]);
 }
 
+// coefficients at quadrature point q of element e: analytic kinds, or the
+// host-evaluated table (PMG_COEF_TABLE, 6 values per point)
+__device__ __forceinline__ void coeff_at(const CoefDev &C, const double *ctab, int nq, int e, int q, double x,
+                                         double y, double z, double *c) {
+  if (C.kind == PMG_COEF_TABLE) {
+    const double *v = ctab + ((size_t)e * nq + q) * 6;
+#pragma unroll
+    for (int k = 0; k < 6; k++) c[k] = v[k];
+    c[6] = sqrt(c[1] * c[1] + c[2] * c[2] + c[3] * c[3]);
+  } else {
+    coeff_eval(C, x, y, z, c);
+  }
+}
+
 // SDFEM_TYPE 2 (src/FE/ConvDiff.C:591-611)
 __device__ __forceinline__ double sdfem_delta(double h, double eps, double b1, double b2, double b3, int poly,
                                               double delta0) {
@@ -175,6 +189,7 @@ struct AsmArgs {
   int form, poly, brick;
   double delta0;
   CoefDev coef;
+  const double *ctab;  // n x NQ x 6 (PMG_COEF_TABLE), already offset to the colour
   const double *utab;  // NQ x NLOC x 4
   const double *qtab;  // NQ x 4 : weight, xi, eta, zeta
   int *flags;
@@ -250,7 +265,7 @@ __global__ void __launch_bounds__(ASM_WARPS * 32) k_assemble(AsmArgs a) {
         double Y = x0[1] + J[3] * sQ[1] + J[4] * sQ[2] + J[5] * sQ[3];
         double Z = x0[2] + J[6] * sQ[1] + J[7] * sQ[2] + J[8] * sQ[3];
         double c[7];
-        coeff_eval(a.coef, X, Y, Z, c);
+        coeff_at(a.coef, a.ctab, NQ, e, 0, X, Y, Z, c);
         hconv = hk_convection(HEX, a.brick != 0, cv, Ji, c[1], c[2], c[3]);
       }
       for (int q = t; q < NQ; q += NLOC) {
@@ -259,7 +274,7 @@ __global__ void __launch_bounds__(ASM_WARPS * 32) k_assemble(AsmArgs a) {
         double Y = x0[1] + J[3] * xi + J[4] * eta + J[5] * zeta;
         double Z = x0[2] + J[6] * xi + J[7] * eta + J[8] * zeta;
         double c[7];
-        coeff_eval(a.coef, X, Y, Z, c);
+        coeff_at(a.coef, a.ctab, NQ, e, q, X, Y, Z, c);
         const double mult = sQ[q * 4] * adet;
         double delta = supg ? sdfem_delta(hconv, c[0], c[1], c[2], c[3], a.poly, a.delta0) : 0.0;
         double bh[3];  // b in reference gradients: b . (Ji^T g^) = (Ji b) . g^
@@ -446,6 +461,7 @@ static int launch_assemble(Handle &h, Level &L, AsmArgs a) {
     b.elem_dof = ed0 + (size_t)beg * NLOC;
     b.cell_vert = cv0 + (size_t)beg * ET<E>::NV * 3;
     b.slot = sl0 + (size_t)beg * NLOC * NLOC;
+    b.ctab = a.ctab ? a.ctab + (size_t)beg * NQ * 6 : nullptr;
     int blocks = (n + per_block - 1) / per_block;
     int cap = h.num_sms * 8;
     if (blocks > cap) blocks = cap;
@@ -478,6 +494,10 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
     return PMG_ERR_UNSUPPORTED;
   }
   PMG_TRY(get_tables(L.elem, rule, T));
+  if (h.coeff.kind == PMG_COEF_TABLE && (!L.ctab.p || L.ctab_nq != T->nq)) {
+    set_error("assemble: PMG_COEF_TABLE needs pmg_set_coefficient_table for this level and quadrature rule");
+    return PMG_ERR_STATE;
+  }
   PMG_CUDA(cudaMemsetAsync(target, 0, sizeof(double) * L.nnz, h.stream));
   if (rhs_target && zero_rhs) PMG_CUDA(cudaMemsetAsync(rhs_target, 0, sizeof(double) * L.N, h.stream));
   PMG_CUDA(cudaMemsetAsync(h.d_flags.p, 0, sizeof(int) * 4, h.stream));
@@ -500,6 +520,7 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
   a.coef.t = h.coeff.t;
   a.coef.n_modes = h.coeff.n_modes;
   a.coef.modes = h.d_modes.p;
+  a.ctab = h.coeff.kind == PMG_COEF_TABLE ? L.ctab.p : nullptr;
   a.utab = T->utab.p;
   a.qtab = T->qtab.p;
   a.flags = h.d_flags.p;
@@ -533,3 +554,81 @@ int set_dirichlet_rows(Handle &h, Level &L, double *target, double *rhs_target) 
 }
 
 }  // namespace pmg
+
+using namespace pmg;
+
+// quadrature points of one level in the caller's cell order, mapped like the
+// kernel maps them (HexaAffin: vertices 0, 1, 3, 4; TetraAffin: 0, 1, 2, 3)
+extern "C" int pmg_quad_points(pmg_handle hh, int level, int *nq, double *xyz) {
+  Handle *h = reinterpret_cast<Handle *>(hh);
+  if (!h || level < 0 || level >= (int)h->lv.size() || !nq) {
+    set_error("pmg_quad_points: bad arguments");
+    return PMG_ERR_ARG;
+  }
+  Level &L = h->lv[level];
+  if (!L.has_mesh) {
+    set_error("pmg_quad_points: call pmg_set_level_mesh first");
+    return PMG_ERR_STATE;
+  }
+  const int rule = rule_for(L.elem, h->prm.problem_linear);
+  if (rule < 0) {
+    set_error("pmg_quad_points: the degree-6 tetrahedral rule is not built");
+    return PMG_ERR_UNSUPPORTED;
+  }
+  QuadRule q = make_rule(rule);
+  *nq = q.n;
+  if (!xyz) return PMG_OK;
+  const int nv = L.nvert;
+  std::vector<double> cv((size_t)L.n_cells * nv * 3);
+  PMG_CUDA(cudaMemcpyAsync(cv.data(), L.cell_vert.p, sizeof(double) * cv.size(), cudaMemcpyDeviceToHost, h->stream));
+  PMG_CUDA(cudaStreamSynchronize(h->stream));
+  const bool hex = nv == 8;
+  for (int k = 0; k < L.n_cells; k++) {
+    const double *v = &cv[(size_t)k * nv * 3];
+    double J[9], x0[3];
+    for (int d = 0; d < 3; d++) {
+      if (hex) {
+        J[d * 3 + 0] = (v[3 + d] - v[d]) * 0.5;
+        J[d * 3 + 1] = (v[9 + d] - v[d]) * 0.5;
+        J[d * 3 + 2] = (v[12 + d] - v[d]) * 0.5;
+        x0[d] = (v[3 + d] + v[9 + d] + v[12 + d] - v[d]) * 0.5;
+      } else {
+        J[d * 3 + 0] = v[3 + d] - v[d];
+        J[d * 3 + 1] = v[6 + d] - v[d];
+        J[d * 3 + 2] = v[9 + d] - v[d];
+        x0[d] = v[d];
+      }
+    }
+    double *o = xyz + (size_t)L.cell_order[k] * q.n * 3;
+    for (int p = 0; p < q.n; p++)
+      for (int d = 0; d < 3; d++)
+        o[p * 3 + d] = x0[d] + J[d * 3 + 0] * q.x[p] + J[d * 3 + 1] * q.y[p] + J[d * 3 + 2] * q.z[p];
+  }
+  return PMG_OK;
+}
+
+extern "C" int pmg_set_coefficient_table(pmg_handle hh, int level, const double *values) {
+  Handle *h = reinterpret_cast<Handle *>(hh);
+  if (!h || level < 0 || level >= (int)h->lv.size() || !values) {
+    set_error("pmg_set_coefficient_table: bad arguments");
+    return PMG_ERR_ARG;
+  }
+  Level &L = h->lv[level];
+  int nq = 0;
+  PMG_TRY(pmg_quad_points(hh, level, &nq, nullptr));
+  const size_t per = (size_t)nq * 6;
+  std::vector<double> t((size_t)L.n_cells * per);
+  for (int k = 0; k < L.n_cells; k++) {
+    const double *src = values + (size_t)L.cell_order[k] * per;
+    for (size_t j = 0; j < per; j++)
+      if (!std::isfinite(src[j])) {
+        set_error("pmg_set_coefficient_table: non-finite value");
+        return PMG_ERR_NONFINITE;
+      }
+    std::copy(src, src + per, &t[(size_t)k * per]);
+  }
+  PMG_TRY(L.ctab.upload(t.data(), t.size(), h->stream));
+  PMG_CUDA(cudaStreamSynchronize(h->stream));
+  L.ctab_nq = nq;
+  return PMG_OK;
+}

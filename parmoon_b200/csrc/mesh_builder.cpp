@@ -294,6 +294,76 @@ int pmg_struct_prolongation(int e, int nc, const int *lat_c, int Nc, const int *
   return PMG_OK;
 }
 
+// Interpolation from a coarse level onto the dof nodes of a nested fine
+// level, for any mesh the reference refines (GetProlongationMatrix3D composes
+// the same values from the reference-element tables, FEDatabase3D.C:1656-1815):
+// row r holds the coarse basis functions of the coarse cell f_dof_cell[r]
+// evaluated at the fine node.  For conforming nested spaces the value does not
+// depend on which containing coarse cell is named.
+int pmg_nested_prolongation(int e, int n_coarse_cells, const int *c_elem_dof, const double *c_cell_vert, int Nc,
+                            int Nf, const double *f_dof_xyz, const int *f_dof_cell, int *prp, int *pcol,
+                            double *pval) {
+  if (!valid_elem(e) || n_coarse_cells < 1 || !c_elem_dof || !c_cell_vert || !f_dof_xyz || !f_dof_cell || !prp)
+    return PMG_ERR_ARG;
+  const int nl = nloc_of(e);
+  const bool hex = is_hex(e);
+  prp[0] = 0;
+  for (int r = 0; r < Nf; r++) {
+    const int c = f_dof_cell[r];
+    if (c < 0 || c >= n_coarse_cells) return PMG_ERR_ARG;
+    const double *v = c_cell_vert + (size_t)c * 24;
+    double J[9], x0[3];
+    for (int d = 0; d < 3; d++) {
+      if (hex) {
+        J[d * 3 + 0] = (v[3 + d] - v[d]) * 0.5;
+        J[d * 3 + 1] = (v[9 + d] - v[d]) * 0.5;
+        J[d * 3 + 2] = (v[12 + d] - v[d]) * 0.5;
+        x0[d] = (v[3 + d] + v[9 + d] + v[12 + d] - v[d]) * 0.5;
+      } else {
+        J[d * 3 + 0] = v[3 + d] - v[d];
+        J[d * 3 + 1] = v[6 + d] - v[d];
+        J[d * 3 + 2] = v[9 + d] - v[d];
+        x0[d] = v[d];
+      }
+    }
+    const double det = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
+                       J[2] * (J[3] * J[7] - J[4] * J[6]);
+    if (!(std::fabs(det) > 0)) return PMG_ERR_ARG;
+    double Ji[9];
+    Ji[0] = (J[4] * J[8] - J[5] * J[7]) / det; Ji[1] = (J[2] * J[7] - J[1] * J[8]) / det;
+    Ji[2] = (J[1] * J[5] - J[2] * J[4]) / det; Ji[3] = (J[5] * J[6] - J[3] * J[8]) / det;
+    Ji[4] = (J[0] * J[8] - J[2] * J[6]) / det; Ji[5] = (J[2] * J[3] - J[0] * J[5]) / det;
+    Ji[6] = (J[3] * J[7] - J[4] * J[6]) / det; Ji[7] = (J[1] * J[6] - J[0] * J[7]) / det;
+    Ji[8] = (J[0] * J[4] - J[1] * J[3]) / det;
+    const double dx[3] = {f_dof_xyz[3 * (size_t)r] - x0[0], f_dof_xyz[3 * (size_t)r + 1] - x0[1],
+                          f_dof_xyz[3 * (size_t)r + 2] - x0[2]};
+    double ref[3];
+    for (int d = 0; d < 3; d++) ref[d] = Ji[d * 3] * dx[0] + Ji[d * 3 + 1] * dx[1] + Ji[d * 3 + 2] * dx[2];
+    double tab[27 * 4];
+    pmg::basis_eval(e, ref[0], ref[1], ref[2], tab);
+    int cols[27], m = 0;
+    double vals[27];
+    for (int l = 0; l < nl; l++) {
+      const double w = tab[l * 4 + 3];
+      if (std::fabs(w) < 1e-12) continue;
+      const int col = c_elem_dof[(size_t)c * nl + l];
+      if (col < 0 || col >= Nc) return PMG_ERR_ARG;
+      cols[m] = col; vals[m] = w; m++;
+    }
+    for (int x = 1; x < m; x++) {
+      int cc = cols[x]; double vv = vals[x]; int y = x - 1;
+      while (y >= 0 && cols[y] > cc) { cols[y + 1] = cols[y]; vals[y + 1] = vals[y]; y--; }
+      cols[y + 1] = cc; vals[y + 1] = vv;
+    }
+    if (pcol) {
+      std::memcpy(pcol + prp[r], cols, sizeof(int) * m);
+      std::memcpy(pval + prp[r], vals, sizeof(double) * m);
+    }
+    prp[r + 1] = prp[r] + m;
+  }
+  return PMG_OK;
+}
+
 int pmg_struct_row_colors(int e, int n, int N, const int *lat, int *colors, int *n_colors) {
   if (!valid_elem(e) || !lat || !colors || !n_colors) return PMG_ERR_ARG;
   const int p = degree_of(e), n1 = p * n + 1, m = p + 1;

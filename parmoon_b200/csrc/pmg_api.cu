@@ -243,6 +243,9 @@ int pmg_set_level_mesh(pmg_handle hh, int level, int elem_type, int n_cells, con
   L.n_cells = n_cells;
   L.brick = brick;
   L.ecolor_ptr = ptr;
+  L.cell_order = order;
+  L.ctab.release();
+  L.ctab_nq = 0;
   PMG_TRY(L.elem_dof.upload(ed.data(), ed.size(), h->stream));
   PMG_TRY(L.cell_vert.upload(cv.data(), cv.size(), h->stream));
   L.slot.release();
@@ -384,7 +387,7 @@ int pmg_set_dirichlet_values(pmg_handle hh, int level, const double *values) {
 int pmg_set_coefficients(pmg_handle hh, const pmg_coeff_desc *c) {
   Handle *h = H(hh);
   if (!h || !c) return PMG_ERR_ARG;
-  if (c->kind < PMG_COEF_CONST || c->kind > PMG_COEF_AMC) { set_error("unknown coefficient kind"); return PMG_ERR_ARG; }
+  if (c->kind < PMG_COEF_CONST || c->kind > PMG_COEF_TABLE) { set_error("unknown coefficient kind"); return PMG_ERR_ARG; }
   double vals[7] = {c->eps, c->b[0], c->b[1], c->b[2], c->c, c->f, c->t};
   for (double v : vals)
     if (!std::isfinite(v)) { set_error("pmg_set_coefficients: non-finite coefficient"); return PMG_ERR_NONFINITE; }

@@ -111,6 +111,10 @@ struct Level {
   DBuf<double> cell_vert;   // n_cells x nvert x 3
   DBuf<int> slot;           // n_cells x nloc x nloc
   std::vector<int> ecolor_ptr;  // element colour classes [ecolor_ptr[c], ecolor_ptr[c+1])
+  std::vector<int> cell_order;  // colour-sorted position -> caller's cell index
+  // tabulated coefficients (PMG_COEF_TABLE): n_cells x ctab_nq x 6, colour order
+  DBuf<double> ctab;
+  int ctab_nq = 0;
   // multicolour SSOR row lists (active rows only), grouped by colour
   DBuf<int> row_list;
   std::vector<int> rcolor_ptr;

@@ -103,3 +103,56 @@ def test_struct_builder_pattern_equals_reference_up_to_numbering(name, elem, p):
     ref_edges = set(zip(np.repeat(perm, np.diff(rp)).tolist(), perm[kc].tolist()))
     my_edges = set(zip(np.repeat(np.arange(L["N"]), np.diff(L["rowptr"])).tolist(), L["kcol"].tolist()))
     assert ref_edges == my_edges
+
+
+def locate_cells(elem, cell_vert, pts):
+    """Index of a cell of the (affine) mesh containing each point, by inverting every cell's map."""
+    v = np.asarray(cell_vert).reshape(-1, 8, 3)
+    if elem in (1, 2):
+        J = np.stack([(v[:, 1] - v[:, 0]) / 2, (v[:, 3] - v[:, 0]) / 2, (v[:, 4] - v[:, 0]) / 2], axis=2)
+        x0 = (v[:, 1] + v[:, 3] + v[:, 4] - v[:, 0]) / 2
+    else:
+        J = np.stack([v[:, 1] - v[:, 0], v[:, 2] - v[:, 0], v[:, 3] - v[:, 0]], axis=2)
+        x0 = v[:, 0]
+    Ji = np.linalg.inv(J)
+    ref = np.einsum("cij,pcj->pci", Ji, pts[:, None, :] - x0[None])  # [points, cells, 3]
+    tol = 1e-10
+    if elem in (1, 2):
+        inside = np.all(np.abs(ref) <= 1 + tol, axis=2)
+    else:
+        inside = np.all(ref >= -tol, axis=2) & (ref.sum(axis=2) <= 1 + tol)
+    assert inside.any(axis=1).all()
+    return inside.argmax(axis=1).astype(np.int32)
+
+
+@pytest.mark.parametrize("name,elem", [("q1_laplace", 1), ("q2_supg", 2), ("p1tet_laplace", 11), ("p2tet_supg", 12)])
+def test_nested_prolongation_matches_reference_prolongate(name, elem):
+    """Prolongate and DefectRestriction of the reference (MGComponents3D.C:208-488, 732-1014)
+    on its own refined meshes, tetrahedra included, equal P and P^T from pmg_nested_prolongation."""
+    import parmoon_b200 as P
+    g = golden(name)
+    nl = sum(1 for k in g.files if k.endswith("_rowptr"))
+    for l in range(1, nl):
+        c, f = f"L{l-1}_", f"L{l}_"
+        xyz = g[f + "dof_xyz"].reshape(-1, 3)
+        owner = locate_cells(elem, g[c + "cell_vert"], xyz)
+        rp, col, val = P.nested_prolongation(elem, g[c + "elem_dof"], g[c + "cell_vert"], int(g[c + "N"]), xyz, owner)
+        ci = g[f"T{l}_coarse_in"]
+        pf = np.array([np.dot(val[rp[i]:rp[i + 1]], ci[col[rp[i]:rp[i + 1]]]) for i in range(xyz.shape[0])])
+        assert np.max(np.abs(pf - g[f"T{l}_prolongated"])) < 1e-13
+        d = g[f"T{l}_fine_in"]
+        r = np.zeros(ci.size)
+        np.add.at(r, col, val * np.repeat(d, np.diff(rp)))
+        assert np.max(np.abs(r - g[f"T{l}_restricted"])) < 1e-13
+
+
+def test_nested_prolongation_equals_lattice_interpolation():
+    """On the structured hierarchy the nested builder reproduces pmg_struct_prolongation."""
+    import parmoon_b200 as P
+    for elem in (1, 2, 11, 12):
+        C, F = P.struct_level(elem, 2), P.struct_level(elem, 4)
+        owner = locate_cells(elem, C["cell_vert"], F["dof_xyz"])
+        rp, col, val = P.nested_prolongation(elem, C["elem_dof"], C["cell_vert"], C["N"], F["dof_xyz"], owner)
+        srp, scol, sval = P.struct_prolongation(elem, 2, C["dof_lat"], F["dof_lat"])
+        assert np.array_equal(rp, srp) and np.array_equal(col, scol)
+        assert np.max(np.abs(val - sval)) < 1e-14
