@@ -106,3 +106,12 @@ void dgetrs_(char *trans, int *n, int *nrhs, double *a, int *lda, int *ipiv, dou
   }
 }
 }
+
+// Tecplot binary writer (TOutput3D::WriteBinaryPlt): report failure, as the
+// writer does when the library cannot open its file
+int TECINI112(...) { return -1; }
+int TECZNE112(...) { return -1; }
+int TECDAT112(...) { return -1; }
+int TECNOD112(...) { return -1; }
+int TECEND112(...) { return -1; }
+int TECEND(...) { return -1; }

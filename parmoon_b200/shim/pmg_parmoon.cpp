@@ -67,6 +67,8 @@ TPmgSystemCD3D::~TPmgSystemCD3D() {
 
 // patterns, meshes, Dirichlet values and transfers of every level
 void TPmgSystemCD3D::setup(BoundValueFunct3D *BoundValue) {
+  BoundValues = BoundValue;
+  dirichlet.assign(N_Levels, DirichletNodes());
   std::vector<std::vector<int>> ed_lv(N_Levels);
   std::vector<std::vector<double>> cv_lv(N_Levels);
   for (int i = 0; i < N_Levels && status == PMG_OK; i++) {
@@ -107,7 +109,7 @@ void TPmgSystemCD3D::setup(BoundValueFunct3D *BoundValue) {
     check(pmg_set_level_mesh(h, i, elem, nc, ed.data(), cv.data(), brick ? 1 : 0), "pmg_set_level_mesh");
     // Dirichlet values: BoundValue(Bd_ID, node) at the dof nodes of every boundary
     // face, Bd_ID the face's boundary component (AssembleMat3D.C:1020-1081)
-    std::vector<double> X(N), Y(N), Z(N), dv(N - Na);
+    std::vector<double> X(N), Y(N), Z(N);
     std::vector<int> bd_id(N - Na, 0);
     sp->GetDOFPosition(X.data(), Y.data(), Z.data());
     for (int c = 0; c < nc; c++) {
@@ -125,8 +127,14 @@ void TPmgSystemCD3D::setup(BoundValueFunct3D *BoundValue) {
         }
       }
     }
-    for (int d = Na; d < N; d++) BoundValue(bd_id[d - Na], X[d], Y[d], Z[d], dv[d - Na]);
-    if (N > Na) check(pmg_set_dirichlet_values(h, i, dv.data()), "pmg_set_dirichlet_values");
+    DirichletNodes &dn = dirichlet[i];
+    dn.id = bd_id;
+    dn.xyz.resize((size_t)3 * (N - Na));
+    for (int d = Na; d < N; d++) {
+      dn.xyz[3 * (size_t)(d - Na)] = X[d];
+      dn.xyz[3 * (size_t)(d - Na) + 1] = Y[d];
+      dn.xyz[3 * (size_t)(d - Na) + 2] = Z[d];
+    }
     if (i == 0 || status != PMG_OK) continue;
     // prolongation from level i-1: the coarse basis of each fine cell's parent
     // evaluated at the fine dofs (Prolongate, MGComponents3D.C:208-488)
@@ -162,6 +170,20 @@ void TPmgSystemCD3D::setup(BoundValueFunct3D *BoundValue) {
   }
 }
 
+// BoundValue at every level's Dirichlet nodes, re-evaluated before every
+// assembly as Assemble3D does (time-dependent boundary data included)
+void TPmgSystemCD3D::update_dirichlet() {
+  for (int i = 0; i < N_Levels && status == PMG_OK; i++) {
+    const DirichletNodes &dn = dirichlet[i];
+    const size_t nd = dn.id.size();
+    if (nd == 0) continue;
+    std::vector<double> dv(nd);
+    for (size_t d = 0; d < nd; d++)
+      BoundValues(dn.id[d], dn.xyz[3 * d], dn.xyz[3 * d + 1], dn.xyz[3 * d + 2], dv[d]);
+    check(pmg_set_dirichlet_values(h, i, dv.data()), "pmg_set_dirichlet_values");
+  }
+}
+
 void TPmgSystemCD3D::Init(CoeffFct3D *BilinearCoeffs, BoundCondFunct3D *, BoundValueFunct3D *BoundValue,
                           TAuxParam3D *) {
   if (status != PMG_OK) return;
@@ -176,7 +198,11 @@ void TPmgSystemCD3D::Init(CoeffFct3D *, BoundCondFunct3D *, BoundValueFunct3D *B
                           const pmg_coeff_desc &device_coeffs) {
   if (status != PMG_OK) return;
   Coeffs = nullptr;
-  check(pmg_set_coefficients(h, &device_coeffs), "pmg_set_coefficients");
+  dev_coeffs = device_coeffs;
+  if (device_coeffs.modes && device_coeffs.n_modes > 0)
+    dev_modes.assign(device_coeffs.modes, device_coeffs.modes + 8 * (size_t)device_coeffs.n_modes);
+  dev_coeffs.modes = dev_modes.empty() ? nullptr : dev_modes.data();
+  check(pmg_set_coefficients(h, &dev_coeffs), "pmg_set_coefficients");
   setup(BoundValue);
 }
 
@@ -211,17 +237,88 @@ void TPmgSystemCD3D::tabulate_coefficients() {
   }
 }
 
-void TPmgSystemCD3D::Assemble() {
+// assemble one form on every level; rhs of every level and the Dirichlet part
+// of every level's solution back to the host arrays (SystemCD3D.C:340-365)
+void TPmgSystemCD3D::assemble_form(int form) {
   if (status != PMG_OK) return;
-  if (Coeffs) tabulate_coefficients();
+  update_dirichlet();
+  if (Coeffs) {
+    tabulate_coefficients();
+  } else {
+    // built-in fields read the time from the descriptor
+    dev_coeffs.t = TDatabase::TimeDB->CURRENTTIME;
+    check(pmg_set_coefficients(h, &dev_coeffs), "pmg_set_coefficients");
+  }
   if (status != PMG_OK) return;
-  check(pmg_assemble(h, -1, Disctype == SDFEM ? PMG_FORM_SUPG : PMG_FORM_GALERKIN, nullptr, nullptr), "pmg_assemble");
+  check(pmg_assemble(h, -1, form, nullptr, nullptr), "pmg_assemble");
   for (int i = 0; i < N_Levels && status == PMG_OK; i++) {
     const int N = FeSpaces[i]->GetN_DegreesOfFreedom(), Na = FeSpaces[i]->GetActiveBound();
     check(pmg_get_rhs(h, i, RhsArray[i]), "pmg_get_rhs");
     // set rhs for Dirichlet nodes (SystemCD3D.C:361)
     std::memcpy(SolArray[i] + Na, RhsArray[i] + Na, (size_t)(N - Na) * sizeof(double));
   }
+}
+
+void TPmgSystemCD3D::Assemble() { assemble_form(Disctype == SDFEM ? PMG_FORM_SUPG : PMG_FORM_GALERKIN); }
+
+// TSystemTCD3D::AssembleMRhs (SystemTCD3D.C:208-232): M and f(t) on every level
+void TPmgSystemCD3D::AssembleMRhs() { assemble_form(Disctype == SDFEM ? PMG_FORM_MASS_SUPG : PMG_FORM_MASS); }
+
+// TSystemTCD3D::AssembleARhs (SystemTCD3D.C:235-257): A and f(t) on every level
+void TPmgSystemCD3D::AssembleARhs() {
+  if (syst_assembled) {
+    check(PMG_ERR_STATE, "AssembleARhs: the system matrix is assembled; call RestoreMassMat first");
+    return;
+  }
+  assemble_form(Disctype == SDFEM ? PMG_FORM_SUPG : PMG_FORM_GALERKIN);
+}
+
+// TSystemTCD3D::AssembleSystMat (SystemTCD3D.C:260-326); rhs is the finest
+// level's f(t_new) of the last AssembleARhs, which the device holds
+void TPmgSystemCD3D::AssembleSystMat(double *oldrhs, double *oldsol, double *rhs, double *sol) {
+  if (status != PMG_OK) return;
+  const int F = N_Levels - 1;
+  const int N = FeSpaces[F]->GetN_DegreesOfFreedom(), Na = FeSpaces[F]->GetActiveBound();
+  const double tau = TDatabase::TimeDB->CURRENTTIMESTEPLENGTH;
+  const double theta[4] = {TDatabase::TimeDB->THETA1, TDatabase::TimeDB->THETA2, TDatabase::TimeDB->THETA3,
+                           TDatabase::TimeDB->THETA4};
+  B.resize(N);
+  check(pmg_tcd_system(h, tau, theta, oldrhs, oldsol, B.data()), "pmg_tcd_system");
+  if (status != PMG_OK) return;
+  // Dirichlet values into the start vector (SystemTCD3D.C:297-298)
+  std::memcpy(sol + Na, rhs + Na, (size_t)(N - Na) * sizeof(double));
+  syst_assembled = true;
+}
+
+// TSystemTCD3D::RestoreMassMat (SystemTCD3D.C:328-347)
+void TPmgSystemCD3D::RestoreMassMat() {
+  if (status != PMG_OK) return;
+  check(pmg_tcd_restore(h), "pmg_tcd_restore");
+  syst_assembled = false;
+}
+
+// TSystemTCD3D::Solve (SystemTCD3D.C:349-420): sol is the start vector, B the rhs
+void TPmgSystemCD3D::Solve(double *sol) {
+  if (status != PMG_OK) return;
+  if (!syst_assembled) {
+    check(PMG_ERR_STATE, "Solve: call AssembleSystMat first");
+    return;
+  }
+  Solve(sol, nullptr);
+}
+
+// TSystemTCD3D::GetResidual (SystemTCD3D.C:423-460): |B - (M + tau theta1 A) sol|
+double TPmgSystemCD3D::GetResidual(double *sol) {
+  if (status != PMG_OK) return 0.0;
+  if (!syst_assembled) {
+    check(PMG_ERR_STATE, "GetResidual: assemble the system matrix first");
+    return 0.0;
+  }
+  const int F = N_Levels - 1;
+  std::vector<double> r(B.size());
+  double norm = 0.0;
+  check(pmg_defect(h, F, sol, B.data(), r.data(), &norm), "pmg_defect");
+  return norm;
 }
 
 void TPmgSystemCD3D::Solve(double *sol, double *rhs) {

@@ -19,6 +19,9 @@
 // CoeffFct3D works unchanged; the overload taking a pmg_coeff_desc lets the
 // device evaluate a built-in field instead (no host work per assembly).
 // DISCTYPE GALERKIN (1) and SDFEM/SUPG (2) are built; SOLVER must be GMG (1).
+// The time-dependent surface of TSystemTCD3D is here as well; the reference's
+// class names are provided by SystemCD3D_pmg.C / SystemTCD3D_pmg.C, which a
+// program links instead of src/System/SystemCD3D.C / SystemTCD3D.C.
 //
 // Build inside a ParMooN tree (the reference headers on the include path,
 // -D__3D__) and link libpmg_b200.so.
@@ -49,9 +52,20 @@ class TPmgSystemCD3D {
   // TSystemCD3D::Solve (SystemCD3D.C:368-420), SOLVER = GMG with FGMRES
   void Solve(double *sol, double *rhs);
 
+  // TSystemTCD3D surface (include/System/SystemTCD3D.h, SystemTCD3D.C:208-460):
+  // mass and stiffness assembly at TDatabase::TimeDB->CURRENTTIME, the theta-
+  // scheme system with THETA1..4 and CURRENTTIMESTEPLENGTH, and its solve
+  void AssembleMRhs();
+  void AssembleARhs();
+  void AssembleSystMat(double *oldrhs, double *oldsol, double *rhs, double *sol);
+  void RestoreMassMat();
+  void Solve(double *sol);
+  double GetResidual(double *sol);
+
   // device matrices into the TSquareMatrix3D objects, for code that reads GetEntries()
   void CopyMatricesToHost();
   TSquareMatrix3D **GetAMatrix() { return sqmatrixA.data(); }
+  TSquareStructure3D **GetStructures() { return sqstructure.data(); }
 
   // PMG_OK, or the PMG_ERR_* code of the first failed device call (the
   // reference exits; a library caller decides)
@@ -61,9 +75,19 @@ class TPmgSystemCD3D {
 
  private:
   int N_Levels, Disctype, status = PMG_OK;
+  bool syst_assembled = false;
+  std::vector<double> B;  // theta-scheme rhs of the last AssembleSystMat
   TFESpace3D **FeSpaces;
   double **SolArray, **RhsArray;
   CoeffFct3D *Coeffs = nullptr;
+  BoundValueFunct3D *BoundValues = nullptr;
+  pmg_coeff_desc dev_coeffs{};
+  std::vector<double> dev_modes;
+  struct DirichletNodes {
+    std::vector<int> id;       // boundary component of each Dirichlet dof
+    std::vector<double> xyz;   // its node
+  };
+  std::vector<DirichletNodes> dirichlet;
   std::vector<TSquareStructure3D *> sqstructure;
   std::vector<TSquareMatrix3D *> sqmatrixA;
   pmg_handle h = nullptr;
@@ -71,4 +95,13 @@ class TPmgSystemCD3D {
   void check(int rc, const char *what);
   void setup(BoundValueFunct3D *BoundValue);
   void tabulate_coefficients();
+  void assemble_form(int form);
+  void update_dirichlet();
 };
+
+// the device system behind a TSystemCD3D / TSystemTCD3D of the link-time
+// replacements (SystemCD3D_pmg.C); NULL for any other object
+class TSystemCD3D;
+TPmgSystemCD3D *PmgDeviceSystem(const TSystemCD3D *s);
+// reference-style failure: print the library's message and exit(4711)
+void PmgRequireOk(TPmgSystemCD3D *d, const char *where);
