@@ -279,7 +279,7 @@ def bench_ours(args, rank, world, dist):
             "fp64_gmg": {"solve_s": fp64_s, "iterations": fp64[0][1], "rel_res": fp64[0][2], "status": fp64[0][3]},
             "fp32_solve_s": statistics.mean(s.seconds for s in stats),
             "wall_s_per_step": t_wall / args.steps,
-            "roofline": {"bound": "hbm", "kernel": "k_gs_color<32,float> (FP32 SSOR step, finest level)",
+            "roofline": {"bound": "hbm", "kernel": "k_sell_gs<float,K> (FP32 multicolour SSOR step on SELL-32, finest level)",
                          "achieved": ssor["gbs"], "peak": hbm, "unit": "GB/s", "frac": ssor["gbs"] / hbm,
                          "traffic": None, "peak_kind": peak_kind, "bytes_per_launch": ssor["bytes"],
                          "launch_s": ssor["seconds"]},
@@ -296,6 +296,33 @@ def bench_ours(args, rank, world, dist):
     h.close()
 
 
+KERNELS = {"spmv64": 0, "spmv32": 1, "ssor64": 2, "ssor32": 3, "assemble": 4}
+
+
+def profile_kernel(name):
+    """Time one kernel family on the finest level only (the command the ncu
+    captures run: the first matching launches are the finest level's)."""
+    import ctypes
+    import parmoon_b200 as P
+    lib = P.lib()
+    levels = P.struct_hierarchy(P.Q2_HEX, N_CELLS, N_LEVELS)
+    h = P.Handle(N_LEVELS, P.default_params(precision=P.PREC_FP32))
+    h.set_coefficients(P.coeff(kind=P.COEF_CONST, eps=EPS, b=B, f=F))
+    P.load_hierarchy(h, levels, dirichlet=dirichlet)
+    fine = N_LEVELS - 1
+    if name != "assemble":
+        h.assemble(fine, P.FORM_SUPG, copy_out=False)
+    sec, by, fl = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    P._check(lib.pmg_time_kernel(h.h, KERNELS[name], fine, P.FORM_SUPG, 3, ctypes.byref(sec), ctypes.byref(by),
+                                 ctypes.byref(fl)))
+    hbm, kind = peaks()
+    print(json.dumps({"kernel": name, "n_cells": N_CELLS, "levels": N_LEVELS, "n_dofs": levels[-1]["N"],
+                      "nnz": int(levels[-1]["rowptr"][-1]), "seconds": sec.value, "bytes": by.value,
+                      "flops": fl.value, "gbs": by.value / sec.value / 1e9, "hbm_frac": by.value / sec.value / 1e9 / hbm,
+                      "peak_kind": kind}))
+    h.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -305,10 +332,15 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--n-cells", type=int, default=64, help="cells per direction (64 = the benchmarked workload)")
     ap.add_argument("--levels", type=int, default=5)
+    ap.add_argument("--profile-kernel", choices=sorted(KERNELS), default=None,
+                    help="time one kernel on the finest level only (the profiling command)")
     args = ap.parse_args()
     global N_CELLS, N_LEVELS, N_FULL
     N_CELLS, N_LEVELS = args.n_cells, args.levels
     N_FULL = (2 * N_CELLS + 1) ** 3
+    if args.profile_kernel:
+        profile_kernel(args.profile_kernel)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None
