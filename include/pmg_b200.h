@@ -105,6 +105,8 @@ typedef struct pmg_params {
     int    problem_linear;     /* INTERNAL_PROBLEM_LINEAR: 1 -> Q1 Gauss2 / Q2 Gauss3 / P1 Keast4 / P2 Keast11,
                                   0 -> Q1 Gauss3 / Q2 Gauss4 / P1 Keast11 (FEDatabase3D.C:1203-1309) */
     int    learned_steps;      /* learned-smoother steps per pre/post phase (0: pre_smooth / post_smooth) */
+    int    assembly_kernel;    /* 0: automatic (cells with space-constant eps, b, c use the reference-matrix
+                                  kernel), 1: per-quadrature-point kernel for every coefficient kind */
 } pmg_params;
 
 typedef struct pmg_solve_stats {

@@ -35,7 +35,8 @@ class Params(ctypes.Structure):
                 ("coarse_maxit", _i), ("coarse_red", _d), ("smooth_omega", _d), ("gmg_damp", _d),
                 ("lin_red", _d), ("lin_res_min", _d), ("lin_maxit", _i), ("restart", _i), ("div_factor", _d),
                 ("precision", _i), ("sdfem_type", _i), ("poly_degree", _i), ("delta0", _d),
-                ("reference_restart_rule", _i), ("problem_linear", _i), ("learned_steps", _i)]
+                ("reference_restart_rule", _i), ("problem_linear", _i), ("learned_steps", _i),
+                ("assembly_kernel", _i)]
 
 
 class CoeffDesc(ctypes.Structure):

@@ -195,8 +195,79 @@ struct AsmArgs {
   int *flags;
 };
 
+// affine map of a cell (HexaAffin on vertices 0, 1, 3, 4 over [-1,1]^3;
+// TetraAffin on vertices 0..3 over the unit simplex): x = x0 + J xi, its
+// inverse Ji, |det J| and K = Ji Ji^T (diffusion in reference gradients)
+template <bool HEX>
+__device__ __forceinline__ void cell_map(const double *cv, double *J, double *x0, double *Ji, double &adet,
+                                         double *K) {
+  if (HEX) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      J[d * 3 + 0] = (cv[3 + d] - cv[d]) * 0.5;
+      J[d * 3 + 1] = (cv[9 + d] - cv[d]) * 0.5;
+      J[d * 3 + 2] = (cv[12 + d] - cv[d]) * 0.5;
+      x0[d] = (cv[3 + d] + cv[9 + d] + cv[12 + d] - cv[d]) * 0.5;
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      J[d * 3 + 0] = cv[3 + d] - cv[d];
+      J[d * 3 + 1] = cv[6 + d] - cv[d];
+      J[d * 3 + 2] = cv[9 + d] - cv[d];
+      x0[d] = cv[d];
+    }
+  }
+  double det = J[0] * J[4] * J[8] + J[1] * J[5] * J[6] + J[2] * J[3] * J[7] - J[2] * J[4] * J[6] -
+               J[1] * J[3] * J[8] - J[0] * J[5] * J[7];
+  double rd = 1.0 / det;
+  Ji[0] = (J[4] * J[8] - J[5] * J[7]) * rd;
+  Ji[1] = (J[2] * J[7] - J[1] * J[8]) * rd;
+  Ji[2] = (J[1] * J[5] - J[2] * J[4]) * rd;
+  Ji[3] = (J[5] * J[6] - J[3] * J[8]) * rd;
+  Ji[4] = (J[0] * J[8] - J[2] * J[6]) * rd;
+  Ji[5] = (J[2] * J[3] - J[0] * J[5]) * rd;
+  Ji[6] = (J[3] * J[7] - J[4] * J[6]) * rd;
+  Ji[7] = (J[1] * J[6] - J[0] * J[7]) * rd;
+  Ji[8] = (J[0] * J[4] - J[1] * J[3]) * rd;
+  adet = fabs(det);
+#pragma unroll
+  for (int p = 0; p < 3; p++)
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+      K[p * 3 + q] = Ji[p * 3 + 0] * Ji[q * 3 + 0] + Ji[p * 3 + 1] * Ji[q * 3 + 1] + Ji[p * 3 + 2] * Ji[q * 3 + 2];
+}
+
+// the 4x4 matrix D of one form at one point, in reference gradients:
+// A_ij = sum_q w_q |det J| sum_{a,b} u_ia(q) D_ab u_jb(q), u = (d/dxi, d/deta,
+// d/dzeta, value) of the test (i) and trial (j) basis functions
+// (BilinearAssemble / _SD, ConvDiff3D.C:87-214; MatrixMRhsAssemble(_SUPG),
+// TCD3D.C:37-266).  bh = Ji b.
+__device__ __forceinline__ void form_matrix(int form, bool supg, const double *c, const double *K,
+                                            const double *bh, double delta, double *D) {
+#pragma unroll
+  for (int k = 0; k < 16; k++) D[k] = 0.0;
+  if (form == PMG_FORM_MASS || form == PMG_FORM_MASS_SUPG) {
+    D[15] = 1.0;
+    if (form == PMG_FORM_MASS_SUPG)
+#pragma unroll
+      for (int p = 0; p < 3; p++) D[p * 4 + 3] = delta * bh[p];
+  } else {
+#pragma unroll
+    for (int p = 0; p < 3; p++)
+#pragma unroll
+      for (int r = 0; r < 3; r++) D[p * 4 + r] = c[0] * K[p * 3 + r] + (supg ? delta * bh[p] * bh[r] : 0.0);
+#pragma unroll
+    for (int r = 0; r < 3; r++) D[12 + r] = bh[r];
+    D[15] = c[4];
+    if (supg)
+#pragma unroll
+      for (int p = 0; p < 3; p++) D[p * 4 + 3] = delta * c[4] * bh[p];
+  }
+}
+
 template <int E, int NQ>
-__global__ void __launch_bounds__(ASM_WARPS * 32) k_assemble(AsmArgs a) {
+__global__ void __launch_bounds__(ASM_WARPS * 32, 2) k_assemble(AsmArgs a) {
   constexpr int NLOC = ET<E>::NLOC, NV = ET<E>::NV, GPW = 32 / NLOC;
   constexpr bool HEX = ET<E>::HEX;
   constexpr int GS = NQ * 20;  // per-element scratch: D_q (16) + F_q (4)
@@ -219,44 +290,8 @@ __global__ void __launch_bounds__(ASM_WARPS * 32) k_assemble(AsmArgs a) {
     const bool valid = lane_used && e < a.n_elems;
     if (valid) {
       const double *cv = a.cell_vert + (size_t)e * NV * 3;
-      double J[9], x0[3];
-      if (HEX) {
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-          J[d * 3 + 0] = (cv[3 + d] - cv[d]) * 0.5;
-          J[d * 3 + 1] = (cv[9 + d] - cv[d]) * 0.5;
-          J[d * 3 + 2] = (cv[12 + d] - cv[d]) * 0.5;
-          x0[d] = (cv[3 + d] + cv[9 + d] + cv[12 + d] - cv[d]) * 0.5;
-        }
-      } else {
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-          J[d * 3 + 0] = cv[3 + d] - cv[d];
-          J[d * 3 + 1] = cv[6 + d] - cv[d];
-          J[d * 3 + 2] = cv[9 + d] - cv[d];
-          x0[d] = cv[d];
-        }
-      }
-      double det = J[0] * J[4] * J[8] + J[1] * J[5] * J[6] + J[2] * J[3] * J[7] - J[2] * J[4] * J[6] -
-                   J[1] * J[3] * J[8] - J[0] * J[5] * J[7];
-      double rd = 1.0 / det, Ji[9];
-      Ji[0] = (J[4] * J[8] - J[5] * J[7]) * rd;
-      Ji[1] = (J[2] * J[7] - J[1] * J[8]) * rd;
-      Ji[2] = (J[1] * J[5] - J[2] * J[4]) * rd;
-      Ji[3] = (J[5] * J[6] - J[3] * J[8]) * rd;
-      Ji[4] = (J[0] * J[8] - J[2] * J[6]) * rd;
-      Ji[5] = (J[2] * J[3] - J[0] * J[5]) * rd;
-      Ji[6] = (J[3] * J[7] - J[4] * J[6]) * rd;
-      Ji[7] = (J[1] * J[6] - J[0] * J[7]) * rd;
-      Ji[8] = (J[0] * J[4] - J[1] * J[3]) * rd;
-      const double adet = fabs(det);
-      // K = Ji Ji^T (diffusion in reference gradients)
-      double K[9];
-#pragma unroll
-      for (int p = 0; p < 3; p++)
-#pragma unroll
-        for (int q = 0; q < 3; q++)
-          K[p * 3 + q] = Ji[p * 3 + 0] * Ji[q * 3 + 0] + Ji[p * 3 + 1] * Ji[q * 3 + 1] + Ji[p * 3 + 2] * Ji[q * 3 + 2];
+      double J[9], x0[3], Ji[9], K[9], adet;
+      cell_map<HEX>(cv, J, x0, Ji, adet, K);
       double hconv = 0;
       if (supg) {
         // the reference caches the convection-direction size from the first
@@ -281,25 +316,7 @@ __global__ void __launch_bounds__(ASM_WARPS * 32) k_assemble(AsmArgs a) {
 #pragma unroll
         for (int p = 0; p < 3; p++) bh[p] = Ji[p * 3 + 0] * c[1] + Ji[p * 3 + 1] * c[2] + Ji[p * 3 + 2] * c[3];
         double D[16];
-#pragma unroll
-        for (int k = 0; k < 16; k++) D[k] = 0.0;
-        if (a.form == PMG_FORM_MASS || a.form == PMG_FORM_MASS_SUPG) {
-          D[15] = 1.0;
-          if (a.form == PMG_FORM_MASS_SUPG)
-#pragma unroll
-            for (int p = 0; p < 3; p++) D[p * 4 + 3] = delta * bh[p];
-        } else {
-#pragma unroll
-          for (int p = 0; p < 3; p++)
-#pragma unroll
-            for (int r = 0; r < 3; r++) D[p * 4 + r] = c[0] * K[p * 3 + r] + (supg ? delta * bh[p] * bh[r] : 0.0);
-#pragma unroll
-          for (int r = 0; r < 3; r++) D[12 + r] = bh[r];
-          D[15] = c[4];
-          if (supg)
-#pragma unroll
-            for (int p = 0; p < 3; p++) D[p * 4 + 3] = delta * c[4] * bh[p];
-        }
+        form_matrix(a.form, supg, c, K, bh, delta, D);
         double *Gq = G + q * 20;
 #pragma unroll
         for (int k = 0; k < 16; k++) Gq[k] = D[k] * mult;
@@ -359,6 +376,134 @@ __global__ void __launch_bounds__(ASM_WARPS * 32) k_assemble(AsmArgs a) {
   }
 }
 
+// ------------------------------------------------- constant-coefficient kernel
+// When eps, b and c do not vary in space (PMG_COEF_CONST, SINE_RHS, AMC) and
+// the cell map is affine, D is the same at every quadrature point of a cell,
+// so the local matrix is a 16-term combination of reference matrices:
+//   A_ij = |det J| sum_{a,b} D_ab S_ab[i][j],  S_ab[i][j] = sum_q w_q u_ia(q) u_jb(q)
+// (S from the element's basis and quadrature rule, computed once on the host).
+// That is n_loc^2 x 16 FMA per cell instead of n_q x n_loc^2 x 4, which moves
+// the Q2 kernel from FP64-bound to HBM-bound (slot map + entry read-modify-
+// write).  The result equals the per-point sum up to rounding order.
+// A warp takes P cells at a time; S sits in shared memory ([ab][i*n_loc+j],
+// conflict-free across lanes) and each value read serves P cells.
+constexpr int ASMC_WARPS = 8, ASMC_P = 2;
+
+template <int E, int NQ>
+__global__ void __launch_bounds__(ASMC_WARPS * 32, 2) k_assemble_cc(AsmArgs a, const double *__restrict__ stab) {
+  constexpr int NLOC = ET<E>::NLOC, NV = ET<E>::NV, NN = NLOC * NLOC, P = ASMC_P;
+  constexpr bool HEX = ET<E>::HEX;
+  constexpr int WE = 33 + NQ;  // per-cell scratch: D|det| (16), bh (3), delta, J (9), x0 (3), |det|, w_q |det| f(x_q) (NQ)
+  extern __shared__ double sm[];
+  double *sS = sm;
+  double *sW = sS + 16 * NN;
+  for (int k = threadIdx.x; k < 16 * NN; k += blockDim.x) sS[k] = stab[k];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double *W = sW + warp * P * WE;
+  const bool supg = (a.form == PMG_FORM_SUPG || a.form == PMG_FORM_MASS_SUPG || a.form == PMG_FORM_STIFF_SUPG);
+
+  for (int base = (blockIdx.x * ASMC_WARPS + warp) * P; base < a.n_elems; base += gridDim.x * ASMC_WARPS * P) {
+    // cell set-up: lane p handles cell base + p
+    if (lane < P && base + lane < a.n_elems) {
+      const int e = base + lane;
+      const double *cv = a.cell_vert + (size_t)e * NV * 3;
+      double J[9], x0[3], Ji[9], K[9], adet;
+      cell_map<HEX>(cv, J, x0, Ji, adet, K);
+      const double *q0 = a.qtab;
+      double c[7];
+      coeff_eval(a.coef, x0[0] + J[0] * q0[1] + J[1] * q0[2] + J[2] * q0[3],
+                 x0[1] + J[3] * q0[1] + J[4] * q0[2] + J[5] * q0[3], x0[2] + J[6] * q0[1] + J[7] * q0[2] + J[8] * q0[3],
+                 c);
+      double hconv = supg ? hk_convection(HEX, a.brick != 0, cv, Ji, c[1], c[2], c[3]) : 0.0;
+      double delta = supg ? sdfem_delta(hconv, c[0], c[1], c[2], c[3], a.poly, a.delta0) : 0.0;
+      double bh[3];
+#pragma unroll
+      for (int p = 0; p < 3; p++) bh[p] = Ji[p * 3 + 0] * c[1] + Ji[p * 3 + 1] * c[2] + Ji[p * 3 + 2] * c[3];
+      double D[16];
+      form_matrix(a.form, supg, c, K, bh, delta, D);
+      double *w = W + lane * WE;
+#pragma unroll
+      for (int k = 0; k < 16; k++) w[k] = D[k] * adet;
+      w[16] = bh[0]; w[17] = bh[1]; w[18] = bh[2];
+      w[19] = supg ? delta : 0.0;
+#pragma unroll
+      for (int k = 0; k < 9; k++) w[20 + k] = J[k];
+      w[29] = x0[0]; w[30] = x0[1]; w[31] = x0[2];
+      w[32] = adet;
+    }
+    __syncwarp();
+    // w_q |det J| f(x_q) at every quadrature point of every cell
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+      double *w = W + p * WE;
+      const double adet = w[32];
+      if (base + p < a.n_elems)
+        for (int q = lane; q < NQ; q += 32) {
+          const double *qq = a.qtab + q * 4;
+          const double X = w[29] + w[20] * qq[1] + w[21] * qq[2] + w[22] * qq[3];
+          const double Y = w[30] + w[23] * qq[1] + w[24] * qq[2] + w[25] * qq[3];
+          const double Z = w[31] + w[26] * qq[1] + w[27] * qq[2] + w[28] * qq[3];
+          double c[7];
+          coeff_eval(a.coef, X, Y, Z, c);
+          w[33 + q] = qq[0] * adet * c[5];
+        }
+      __syncwarp();
+    }
+    double Dr[P][16];
+#pragma unroll
+    for (int p = 0; p < P; p++)
+#pragma unroll
+      for (int k = 0; k < 16; k++) Dr[p][k] = W[p * WE + k];
+    int bad = 0;
+    for (int m = lane; m < NN; m += 32) {
+      double acc[P];
+#pragma unroll
+      for (int p = 0; p < P; p++) acc[p] = 0.0;
+#pragma unroll
+      for (int ab = 0; ab < 16; ab++) {
+        const double sv = sS[ab * NN + m];
+#pragma unroll
+        for (int p = 0; p < P; p++) acc[p] += Dr[p][ab] * sv;
+      }
+      const int i = m / NLOC, j = m - i * NLOC;
+#pragma unroll
+      for (int p = 0; p < P; p++) {
+        const int e = base + p;
+        if (e >= a.n_elems) break;
+        const int di = __ldg(a.elem_dof + (size_t)e * NLOC + i);
+        const int sl = __ldg(a.slot + (size_t)e * NN + m);
+        if (di < a.Na) {
+          if (sl >= 0) a.entries[sl] += acc[p];
+          else bad = 1;
+        } else if (i == j && sl >= 0) {
+          a.entries[sl] = 1.0;  // Dirichlet row: unit diagonal (AssembleMat3D.C:840-848)
+        }
+      }
+    }
+    // rhs: f_i = sum_q w_q |det J| f(x_q) (u_i3(q) + delta bh . u_i(q))
+    if (a.rhs)
+#pragma unroll
+      for (int p = 0; p < P; p++) {
+        const int e = base + p;
+        if (e >= a.n_elems) break;
+        const double *w = W + p * WE;
+        for (int i = lane; i < NLOC; i += 32) {
+          const int di = __ldg(a.elem_dof + (size_t)e * NLOC + i);
+          if (di >= a.Na) continue;
+          double r = 0.0;
+          for (int q = 0; q < NQ; q++) {
+            const double *u = a.utab + ((size_t)q * NLOC + i) * 4;
+            r += w[33 + q] * (__ldg(u + 3) + w[19] * (w[16] * __ldg(u) + w[17] * __ldg(u + 1) + w[18] * __ldg(u + 2)));
+          }
+          a.rhs[di] += r;
+        }
+      }
+    if (bad) atomicOr(a.flags, 1);
+    __syncwarp();
+  }
+}
+
 // ----------------------------------------------------------------- slot map
 // slot[e][i][j] = position of column dof_j in the sorted CSR row dof_i
 // (-1 where the row is a Dirichlet row and j != i, or the pair is missing).
@@ -405,6 +550,7 @@ int build_slot_map(Handle &h, Level &L) {
 struct TableCache {
   int elem = -1, rule = -1;
   DBuf<double> utab, qtab;
+  DBuf<double> stab;  // 16 x n_loc^2: S_ab[i][j] = sum_q w_q u_ia(q) u_jb(q)
   int nq = 0;
 };
 static TableCache g_tab[4];
@@ -431,8 +577,19 @@ static int get_tables(int elem, int rule, TableCache *&out) {
       basis_eval(elem, q.x[k], q.y[k], q.z[k], &u[(size_t)k * nl * 4]);
       qt[k * 4] = q.w[k]; qt[k * 4 + 1] = q.x[k]; qt[k * 4 + 2] = q.y[k]; qt[k * 4 + 3] = q.z[k];
     }
+    const size_t nn = (size_t)nl * nl;
+    std::vector<double> st(16 * nn, 0.0);
+    for (int ab = 0; ab < 16; ab++)
+      for (int i = 0; i < nl; i++)
+        for (int j = 0; j < nl; j++) {
+          double acc = 0.0;
+          for (int k = 0; k < q.n; k++)
+            acc += q.w[k] * u[((size_t)k * nl + i) * 4 + ab / 4] * u[((size_t)k * nl + j) * 4 + ab % 4];
+          st[ab * nn + (size_t)i * nl + j] = acc;
+        }
     PMG_TRY(T.utab.upload(u.data(), u.size(), 0));
     PMG_TRY(T.qtab.upload(qt.data(), qt.size(), 0));
+    PMG_TRY(T.stab.upload(st.data(), st.size(), 0));
     PMG_CUDA(cudaDeviceSynchronize());
     T.elem = elem; T.rule = rule; T.nq = q.n;
   }
@@ -469,6 +626,40 @@ static int launch_assemble(Handle &h, Level &L, AsmArgs a) {
     PMG_CUDA(cudaGetLastError());
   }
   return PMG_OK;
+}
+
+template <int E, int NQ>
+static int launch_assemble_cc(Handle &h, Level &L, AsmArgs a, const double *stab) {
+  constexpr int NLOC = ET<E>::NLOC;
+  const size_t smem = sizeof(double) * (16 * (size_t)NLOC * NLOC + (size_t)ASMC_WARPS * ASMC_P * (33 + NQ));
+  static bool attr_set = false;
+  if (!attr_set) {
+    PMG_CUDA(cudaFuncSetAttribute(k_assemble_cc<E, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PMG_CUDA(cudaFuncSetAttribute(k_assemble_cc<E, NQ>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    attr_set = true;
+  }
+  const int per_block = ASMC_WARPS * ASMC_P;
+  const int *ed0 = a.elem_dof;
+  const double *cv0 = a.cell_vert;
+  const int *sl0 = a.slot;
+  for (size_t c = 0; c + 1 < L.ecolor_ptr.size(); c++) {
+    int beg = L.ecolor_ptr[c], n = L.ecolor_ptr[c + 1] - beg;
+    if (n <= 0) continue;
+    AsmArgs b = a;
+    b.n_elems = n;
+    b.elem_dof = ed0 + (size_t)beg * NLOC;
+    b.cell_vert = cv0 + (size_t)beg * ET<E>::NV * 3;
+    b.slot = sl0 + (size_t)beg * NLOC * NLOC;
+    int blocks = std::min((n + per_block - 1) / per_block, h.num_sms * 2);
+    k_assemble_cc<E, NQ><<<blocks, ASMC_WARPS * 32, smem, h.stream>>>(b, stab); count_launches(1);
+    PMG_CUDA(cudaGetLastError());
+  }
+  return PMG_OK;
+}
+
+// coefficient kinds whose eps, b and c are constant in space
+static bool constant_matrix_coefficients(int kind) {
+  return kind == PMG_COEF_CONST || kind == PMG_COEF_SINE_RHS || kind == PMG_COEF_AMC;
 }
 
 // Assemble one level into `target` (A or M) and rhs_target (may be NULL).
@@ -524,6 +715,19 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
   a.utab = T->utab.p;
   a.qtab = T->qtab.p;
   a.flags = h.d_flags.p;
+  if (constant_matrix_coefficients(h.coeff.kind) && h.prm.assembly_kernel != 1) {
+    const double *st = T->stab.p;
+    switch (L.elem * 1000 + T->nq) {
+      case PMG_ELEM_Q1_HEX * 1000 + 8: return launch_assemble_cc<PMG_ELEM_Q1_HEX, 8>(h, L, a, st);
+      case PMG_ELEM_Q1_HEX * 1000 + 27: return launch_assemble_cc<PMG_ELEM_Q1_HEX, 27>(h, L, a, st);
+      case PMG_ELEM_Q2_HEX * 1000 + 27: return launch_assemble_cc<PMG_ELEM_Q2_HEX, 27>(h, L, a, st);
+      case PMG_ELEM_Q2_HEX * 1000 + 64: return launch_assemble_cc<PMG_ELEM_Q2_HEX, 64>(h, L, a, st);
+      case PMG_ELEM_P1_TET * 1000 + 4: return launch_assemble_cc<PMG_ELEM_P1_TET, 4>(h, L, a, st);
+      case PMG_ELEM_P1_TET * 1000 + 11: return launch_assemble_cc<PMG_ELEM_P1_TET, 11>(h, L, a, st);
+      case PMG_ELEM_P2_TET * 1000 + 11: return launch_assemble_cc<PMG_ELEM_P2_TET, 11>(h, L, a, st);
+      default: break;
+    }
+  }
   switch (L.elem * 1000 + T->nq) {
     case PMG_ELEM_Q1_HEX * 1000 + 8: PMG_TRY((launch_assemble<PMG_ELEM_Q1_HEX, 8>(h, L, a))); break;
     case PMG_ELEM_Q1_HEX * 1000 + 27: PMG_TRY((launch_assemble<PMG_ELEM_Q1_HEX, 27>(h, L, a))); break;

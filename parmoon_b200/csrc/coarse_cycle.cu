@@ -1,0 +1,319 @@
+// The coarse end of the V-cycle in one launch: one thread-block cluster
+// (16 CTAs x 32 warps on one GPC) runs TMultiGrid3D::Cycle
+// (src/FE/MultiGrid3D.C:449-695) for every level from `top` down to the
+// coarsest and back up -- pre-smoothing, defect, restriction, the coarsest
+// solve, prolongation, post-smoothing -- with a cluster barrier wherever the
+// level-by-level path would start a new kernel.
+//
+// Why: below ~40k rows a colour sweep is a few microseconds of work, so the
+// colour-by-colour launches of the fine levels (2 x 27 per Q2 SSOR step) are
+// pure launch latency there: levels 1-2 of the 64^3 Q2 hierarchy took longer
+// than the 2.1M-row finest level.  A cluster barrier costs a fraction of a
+// launch, and the coarse levels' matrices (a few MB) stay in L2.
+//
+// Memory: the vectors of a level are read with ld.global.cg and written with
+// st.global.cg (L2, never a stale L1 line of another SM), the matrices with
+// the read-only path; barrier.cluster.arrive.release / wait.acquire orders the
+// writes of one CTA before the reads of the others.  The arithmetic is the
+// level-by-level path's: the same SELL-32 slices, colour order, omega,
+// damping and coarsest solve, so both give the same iterates up to the order
+// of the partial sums inside a row.
+#include "pmg_internal.h"
+#include <cooperative_groups.h>
+#include <cstdlib>
+
+namespace cg = cooperative_groups;
+
+namespace pmg {
+
+constexpr int CC_MAX_LEVELS = 8, CC_MAX_GROUPS = 64, CC_WARPS = 32;
+constexpr int CC_MAX_ROWS = 65536;  // levels up to this size go into the cluster launch
+
+template <typename T>
+struct CcLevel {
+  int N, Na, ncolors;
+  int group[CC_MAX_GROUPS];  // slice range of colour c: [group[c], group[c+1]); group[ncolors+1] = all slices
+  const int *perm, *sptr, *col;
+  const T *val, *invd;
+  // transfer between this level and the one below (this level is the fine side)
+  const int *prp, *pcol, *rrp, *rcol;
+  const T *pval, *rval;
+  T *x, *f, *d;
+};
+
+template <typename T>
+struct CcArgs {
+  int nlev;  // levels 0 .. nlev-1; the cycle enters at nlev-1
+  CcLevel<T> lv[CC_MAX_LEVELS];
+  const double *inv;  // coarsest dense inverse (direct coarse solve) or NULL
+  int n0, coarse_it, pre, post;
+  T omega, damp;
+};
+
+template <typename T>
+struct CcCtx {
+  cg::cluster_group cl;
+  int warp, lane, gw, tw, rank, nblocks;
+  T (*part)[32];
+  __device__ void sync() { cl.sync(); }
+};
+
+// one pass over the slices [s0, s1): Gauss-Seidel update of x (GS) or d = f - A x
+template <typename T, bool GS>
+__device__ void cc_slices(CcCtx<T> &c, const CcLevel<T> &L, int s0, int s1, T omega) {
+  const int nsl = s1 - s0;
+  if (nsl <= 0) return;
+  int K = c.tw / nsl;  // warps per slice: as many as the cluster offers, up to 16
+  K = K >= 16 ? 16 : K >= 8 ? 8 : K >= 4 ? 4 : K >= 2 ? 2 : 1;
+  const int spc = CC_WARPS / K;  // slices per CTA per round
+  const int per_round = spc * c.nblocks;
+  const int rounds = (nsl + per_round - 1) / per_round;
+  const int k = c.warp % K;
+  constexpr int CC_PF = sizeof(T) == 4 ? 16 : 8;  // column steps loaded ahead (64 registers per thread)
+  for (int r = 0; r < rounds; r++) {
+    const int sl = s0 + r * per_round + c.rank * spc + c.warp / K;
+    T sum = 0;
+    if (sl < s1) {
+      const int off = __ldg(L.sptr + sl), lmax = (__ldg(L.sptr + sl + 1) - off) >> 5;
+      const int *cp = L.col + off + c.lane;
+      const T *vp = L.val + off + c.lane;
+      // all loads of the first CC_PF column steps first, then the x gathers:
+      // two L2 round trips per pass instead of one per unrolled group
+      int ci[CC_PF];
+      T cv[CC_PF];
+#pragma unroll
+      for (int u = 0; u < CC_PF; u++) {
+        const int j = k + u * K;
+        ci[u] = j < lmax ? __ldg(cp + 32 * j) : -1;
+        cv[u] = j < lmax ? __ldg(vp + 32 * j) : (T)0;
+      }
+#pragma unroll
+      for (int u = 0; u < CC_PF; u++)
+        if (ci[u] >= 0) sum += cv[u] * __ldcg(L.x + ci[u]);
+      for (int j = k + CC_PF * K; j < lmax; j += K) sum += __ldg(vp + 32 * j) * __ldcg(L.x + __ldg(cp + 32 * j));
+    }
+    c.part[c.warp][c.lane] = sum;
+    __syncthreads();
+    if (k == 0 && sl < s1) {
+      for (int kk = 1; kk < K; kk++) sum += c.part[c.warp + kk][c.lane];
+      const int row = __ldg(L.perm + sl * 32 + c.lane);
+      if (row >= 0) {
+        const T fr = __ldcg(L.f + row);
+        if (GS) __stcg(L.x + row, __ldcg(L.x + row) + omega * (fr - sum) * __ldg(L.invd + sl * 32 + c.lane));
+        else __stcg(L.d + row, fr - sum);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// SSOR step of TMGLevel3D::SSOR in colour order: Dirichlet rows from f, forward, backward
+template <typename T>
+__device__ void cc_ssor(CcCtx<T> &c, const CcLevel<T> &L, T omega) {
+  for (int i = L.Na + c.gw * 32 + c.lane; i < L.N; i += c.tw * 32) __stcg(L.x + i, __ldcg(L.f + i));
+  c.sync();
+  for (int cc = 0; cc < L.ncolors; cc++) {
+    cc_slices<T, true>(c, L, L.group[cc], L.group[cc + 1], omega);
+    c.sync();
+  }
+  for (int cc = L.ncolors - 1; cc >= 0; cc--) {
+    cc_slices<T, true>(c, L, L.group[cc], L.group[cc + 1], omega);
+    c.sync();
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(CC_WARPS * 32, 1) k_coarse_cycle(const __grid_constant__ CcArgs<T> a) {
+  __shared__ T part[CC_WARPS][32];
+  CcCtx<T> c{cg::this_cluster()};
+  c.warp = threadIdx.x >> 5;
+  c.lane = threadIdx.x & 31;
+  c.rank = (int)c.cl.block_rank();
+  c.nblocks = (int)c.cl.num_blocks();
+  c.gw = c.rank * CC_WARPS + c.warp;
+  c.tw = c.nblocks * CC_WARPS;
+  c.part = part;
+  pdl_wait();
+  pdl_trigger();
+  // down: smooth, defect, restrict
+  for (int l = a.nlev - 1; l >= 1; l--) {
+    const CcLevel<T> &L = a.lv[l];
+    const CcLevel<T> &C = a.lv[l - 1];
+    for (int s = 0; s < a.pre; s++) cc_ssor(c, L, a.omega);
+    cc_slices<T, false>(c, L, 0, L.group[L.ncolors + 1], a.omega);
+    c.sync();
+    // restriction, 8 lanes per coarse row (R = P^T rows hold up to 125 entries)
+    for (int base = c.gw * 4; base < C.N; base += c.tw * 4) {
+      const int row = base + (c.lane >> 3), l8 = c.lane & 7;
+      T v = 0;
+      if (row < C.Na) {
+        const int beg = __ldg(L.rrp + row), end = __ldg(L.rrp + row + 1);
+#pragma unroll 4
+        for (int q = beg + l8; q < end; q += 8) v += __ldg(L.rval + q) * __ldcg(L.d + __ldg(L.rcol + q));
+      }
+      v += __shfl_xor_sync(0xffffffffu, v, 4);
+      v += __shfl_xor_sync(0xffffffffu, v, 2);
+      v += __shfl_xor_sync(0xffffffffu, v, 1);
+      if (l8 == 0 && row < C.N) {
+        __stcg(C.f + row, v);
+        __stcg(C.x + row, (T)0);
+      }
+    }
+    c.sync();
+  }
+  // coarsest level: dense inverse (SolveExact) or SSOR steps
+  const CcLevel<T> &Z = a.lv[0];
+  if (a.inv) {
+    for (int row = c.gw; row < a.n0; row += c.tw) {
+      double s = 0;
+      const double *ir = a.inv + (size_t)row * a.n0;
+      for (int j = c.lane; j < a.n0; j += 32) s += __ldg(ir + j) * (double)__ldcg(Z.f + j);
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (c.lane == 0) __stcg(Z.x + row, (T)s);
+    }
+    c.sync();
+  } else {
+    for (int s = 0; s < a.coarse_it; s++) cc_ssor(c, Z, a.omega);
+  }
+  // up: prolongate, smooth
+  for (int l = 1; l < a.nlev; l++) {
+    const CcLevel<T> &L = a.lv[l];
+    const CcLevel<T> &C = a.lv[l - 1];
+    // prolongation, one fine row per lane (P rows hold at most 27 entries)
+    for (int row = c.gw * 32 + c.lane; row < L.Na; row += c.tw * 32) {
+      const int beg = __ldg(L.prp + row), end = __ldg(L.prp + row + 1);
+      T v = 0;
+#pragma unroll 4
+      for (int q = beg; q < end; q++) v += __ldg(L.pval + q) * __ldcg(C.x + __ldg(L.pcol + q));
+      __stcg(L.x + row, __ldcg(L.x + row) + a.damp * v);
+    }
+    c.sync();
+    for (int s = 0; s < a.post; s++) cc_ssor(c, L, a.omega);
+  }
+}
+
+template <typename T> static const T *lv_val(const Level &L);
+template <> const float *lv_val<float>(const Level &L) { return L.sell_val32.p; }
+template <> const double *lv_val<double>(const Level &L) { return L.sell_val64.p; }
+template <typename T> static const T *lv_invd(const Level &L);
+template <> const float *lv_invd<float>(const Level &L) { return L.sell_invd32.p; }
+template <> const double *lv_invd<double>(const Level &L) { return L.sell_invd64.p; }
+template <typename T> static T *lv_vec(Level &L, int which);
+template <> float *lv_vec<float>(Level &L, int w) { return w == 0 ? L.x32.p : w == 1 ? L.f32.p : L.d32.p; }
+template <> double *lv_vec<double>(Level &L, int w) { return w == 0 ? L.x64.p : w == 1 ? L.f64.p : L.d64.p; }
+template <typename T> static const T *lv_p(const Level &L, bool r);
+template <> const float *lv_p<float>(const Level &L, bool r) { return r ? L.rval32.p : L.pval32.p; }
+template <> const double *lv_p<double>(const Level &L, bool r) { return r ? L.rval.p : L.pval.p; }
+
+template <typename T>
+static int cluster_ctas() {
+  static int ctas = 0;
+  if (ctas) return ctas;
+  const void *kernel = (const void *)k_coarse_cycle<T>;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  for (int want : {16, 8, 4}) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(want);
+    cfg.blockDim = dim3(CC_WARPS * 32);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = want;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, kernel, &cfg) == cudaSuccess && n > 0) {
+      ctas = want;
+      break;
+    }
+  }
+  cudaGetLastError();
+  return ctas;
+}
+
+// the highest level that, with every level below it, fits the cluster launch
+// (0: none -- the level-by-level path runs)
+int coarse_cycle_top(const Handle &h) {
+  static int off = -1;
+  if (off < 0) {
+    // opt-in: on the 64^3 Q2 hierarchy this launch measured slower than the
+    // PDL-chained colour launches (a colour pass still waits for two
+    // dependent L2 round trips and a cluster barrier)
+    const char *e = getenv("PMG_COARSE_CLUSTER");
+    off = (e && e[0] == '1') ? 0 : 1;
+  }
+  if (off) return 0;
+  int top = 0;
+  for (int i = 0; i < (int)h.lv.size() - 1 && i < CC_MAX_LEVELS; i++) {
+    const Level &L = h.lv[i];
+    if (L.N > CC_MAX_ROWS || (int)L.sell_group.size() > CC_MAX_GROUPS) break;
+    top = i;
+  }
+  // the launch shape is queried here, outside any stream capture
+  if (top >= 1 && (!cluster_ctas<float>() || !cluster_ctas<double>())) return 0;
+  return top;
+}
+
+template <typename T>
+int coarse_cycle(Handle &h, int top) {
+  if (top < 1 || top >= CC_MAX_LEVELS) {
+    set_error("coarse_cycle: level out of range");
+    return PMG_ERR_ARG;
+  }
+  CcArgs<T> a{};
+  a.nlev = top + 1;
+  for (int i = 0; i <= top; i++) {
+    Level &L = h.lv[i];
+    CcLevel<T> &d = a.lv[i];
+    d.N = L.N;
+    d.Na = L.Na;
+    d.ncolors = (int)L.sell_group.size() - 2;
+    for (size_t g = 0; g < L.sell_group.size(); g++) d.group[g] = L.sell_group[g];
+    d.perm = L.sell_perm.p;
+    d.sptr = L.sell_ptr.p;
+    d.col = L.sell_col.p;
+    d.val = lv_val<T>(L);
+    d.invd = lv_invd<T>(L);
+    if (i > 0) {
+      d.prp = L.prp.p; d.pcol = L.pcol.p; d.pval = lv_p<T>(L, false);
+      d.rrp = L.rrp.p; d.rcol = L.rcol.p; d.rval = lv_p<T>(L, true);
+    }
+    d.x = lv_vec<T>(L, 0);
+    d.f = lv_vec<T>(L, 1);
+    d.d = lv_vec<T>(L, 2);
+  }
+  const bool direct = h.prm.coarse_smoother == PMG_COARSE_DIRECT;
+  a.inv = direct ? h.coarse_inv.p : nullptr;
+  a.n0 = h.lv[0].N;
+  a.coarse_it = h.prm.coarse_maxit > 0 ? h.prm.coarse_maxit : 1;
+  a.pre = h.prm.pre_smooth;
+  a.post = h.prm.post_smooth;
+  a.omega = (T)h.prm.smooth_omega;
+  a.damp = (T)h.prm.gmg_damp;
+  const int ctas = cluster_ctas<T>();
+  if (!ctas) {
+    set_error("coarse_cycle: no thread-block cluster of 4 or more CTAs can be scheduled");
+    return PMG_ERR_UNSUPPORTED;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ctas);
+  cfg.blockDim = dim3(CC_WARPS * 32);
+  cfg.stream = h.stream;
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = ctas;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 2;
+  PMG_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_cycle<T>, a));
+  count_launches(1);
+  return PMG_OK;
+}
+template int coarse_cycle<float>(Handle &, int);
+template int coarse_cycle<double>(Handle &, int);
+
+}  // namespace pmg

@@ -36,7 +36,7 @@ static bool tracing() {
 }
 #define PMG_TRACE_AT(tag) do { if (tracing()) { fprintf(stderr, "[pmg] %s:%d %s\n", __func__, __LINE__, tag); fflush(stderr); } } while (0)
 
-static void invalidate_graphs(Handle *h) {
+void invalidate_graphs(Handle *h) {
   if (h->vgraph) { cudaGraphExecDestroy(h->vgraph); h->vgraph = nullptr; }
   if (h->vgraph_ssor) { cudaGraphExecDestroy(h->vgraph_ssor); h->vgraph_ssor = nullptr; }
 }
@@ -196,6 +196,7 @@ int pmg_set_params(pmg_handle hh, const pmg_params *p) {
   Handle *h = H(hh);
   if (!h || !p) return PMG_ERR_ARG;
   if (p->restart < 1 || p->restart > 60) { set_error("restart must be in [1,60]"); return PMG_ERR_ARG; }
+  if (p->assembly_kernel != 0 && p->assembly_kernel != 1) { set_error("assembly_kernel must be 0 or 1"); return PMG_ERR_ARG; }
   bool graph_shape = p->precision != h->prm.precision || p->pre_smooth != h->prm.pre_smooth ||
                      p->post_smooth != h->prm.post_smooth || p->coarse_smoother != h->prm.coarse_smoother ||
                      p->smooth_omega != h->prm.smooth_omega || p->gmg_damp != h->prm.gmg_damp ||

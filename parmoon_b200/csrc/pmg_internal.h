@@ -174,7 +174,7 @@ struct Handle {
   int num_sms = 148;
   // coarsest-level dense inverse (FP64)
   DBuf<double> coarse_lu, coarse_inv;
-  DBuf<int> coarse_piv;
+  DBuf<int> coarse_piv, coarse_perm;
   bool coarse_ready = false;
   // FGMRES workspace
   int krylov_n = 0, krylov_restart = 0;
@@ -192,6 +192,7 @@ struct Handle {
   int vgraph_prec = -1;
   unsigned long long vgraph_kernels = 0;
   bool use_graph = true;  // PMG_NO_GRAPH=1 launches the V-cycle kernels directly (profilers)
+  int cc_top = 0;         // levels 0..cc_top run as one cluster launch (0: none)
   // learned smoother: BF16 weights used by the kernels, FP32 master copy, Adam state
   DBuf<uint16_t> lw_bf16;
   DBuf<float> lw_master, lw_grad, lw_m, lw_v;
@@ -254,5 +255,13 @@ int learned_num_params();
 int learned_prepare(Handle &h);
 template <typename T>
 int learned_smooth(cudaStream_t s, const Level &L, const T *r, T *x, double omega);
+
+// drop the captured V-cycle graphs (their shape changed)
+void invalidate_graphs(Handle *h);
+
+// the coarse end of the V-cycle in one thread-block-cluster launch (coarse_cycle.cu)
+int coarse_cycle_top(const Handle &h);
+template <typename T>
+int coarse_cycle(Handle &h, int top);
 
 }  // namespace pmg

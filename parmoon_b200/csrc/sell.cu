@@ -179,23 +179,47 @@ __global__ void __launch_bounds__(32 * K) k_sell_mv(int s0, int s1, const int *_
   }
 }
 
-// Gauss-Seidel update of the rows of one colour (slices [s0, s1))
+// Gauss-Seidel update of the rows of one colour (slices [s0, s1)).
+// The first GS_PF column steps of a warp's slice are loaded before
+// pdl_wait(): the predecessor in the stream (the previous colour, a transfer
+// or a defect) writes vectors only, never the matrix, so the colour's matrix
+// streams in while the predecessor drains, and only the x gathers wait.
+constexpr int GS_PF = 16;
+
 template <typename T, int K>
 __global__ void __launch_bounds__(32 * K) k_sell_gs(int s0, int s1, const int *__restrict__ perm,
                                                     const int *__restrict__ sptr, const int *__restrict__ col,
                                                     const T *__restrict__ val, const T *__restrict__ invd,
                                                     const T *__restrict__ f, T *x, T omega) {
   __shared__ T part[K][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int s = s0 + blockIdx.x;
+  int off = 0, lmax = 0;
+  int ci[GS_PF];
+  T cv[GS_PF];
+  auto prefetch = [&](int sl) {
+    off = __ldg(sptr + sl);
+    lmax = (__ldg(sptr + sl + 1) - off) >> 5;
+#pragma unroll
+    for (int u = 0; u < GS_PF; u++) {
+      const int j = w + u * K;
+      const bool in = j < lmax;
+      ci[u] = in ? __ldg(col + off + 32 * j + lane) : 0;
+      cv[u] = in ? __ldg(val + off + 32 * j + lane) : (T)0;
+    }
+  };
+  if (s < s1) prefetch(s);
   pdl_wait();
   pdl_trigger();
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int s = s0 + blockIdx.x; s < s1; s += gridDim.x) {
-    const int off = __ldg(sptr + s), lmax = (__ldg(sptr + s + 1) - off) >> 5;
+  for (; s < s1; s += gridDim.x) {
+    T sum = 0;
+#pragma unroll
+    for (int u = 0; u < GS_PF; u++)
+      if (w + u * K < lmax) sum += cv[u] * x[ci[u]];
     const int *c = col + off + lane;
     const T *v = val + off + lane;
-    T sum = 0;
-#pragma unroll 8
-    for (int j = w; j < lmax; j += K) sum += __ldg(v + 32 * j) * x[__ldg(c + 32 * j)];
+#pragma unroll 4
+    for (int j = w + GS_PF * K; j < lmax; j += K) sum += __ldg(v + 32 * j) * x[__ldg(c + 32 * j)];
     part[w][lane] = sum;
     __syncthreads();
     if (w == 0) {
@@ -205,6 +229,7 @@ __global__ void __launch_bounds__(32 * K) k_sell_gs(int s0, int s1, const int *_
       if (r >= 0) x[r] += omega * (__ldg(f + r) - sum) * __ldg(invd + s * 32 + lane);
     }
     __syncthreads();
+    if (s + gridDim.x < s1) prefetch(s + gridDim.x);
   }
 }
 

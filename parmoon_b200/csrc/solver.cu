@@ -30,25 +30,23 @@ int level_invdiag(cudaStream_t s, Level &L, int *flags);
 //   k_lu_swap    applies the panel's row interchanges to the other columns
 //   k_lu_trsm    U12 = L11^{-1} A12 (one thread per column)
 //   k_lu_gemm    A22 -= L21 U12 (32 x 32 output tiles)
-// then the inverse is formed column tile by column tile (k_lu_inverse):
-// P e_c, forward substitution with L, back substitution with U, the
-// right-hand sides kept in shared memory.
+// then the inverse is formed by block rows (k_lu_inv_step, below).
 constexpr int LU_NB = 32;
-constexpr int LU_MAX_N = 864;  // panel (n x 32 doubles) must fit in 227 KB of shared memory
+constexpr int LU_MAX_N = 832;  // panel (n x 33 doubles) must fit in 227 KB of shared memory
 
 __global__ void __launch_bounds__(1024) k_lu_panel(int n, int k0, int nb, double *A, int *piv, int *flags) {
-  extern __shared__ double S[];  // m x nb, row-major
+  extern __shared__ double S[];  // m x nb, row-major with stride nb + 1 (column reads hit distinct banks)
   __shared__ double sval[32];
   __shared__ int sidx[32];
   __shared__ int spiv;
-  const int m = n - k0, tid = threadIdx.x, nt = blockDim.x;
-  for (int t = tid; t < m * nb; t += nt) S[t] = A[(size_t)(k0 + t / nb) * n + k0 + t % nb];
+  const int m = n - k0, tid = threadIdx.x, nt = blockDim.x, ld = nb + 1;
+  for (int t = tid; t < m * nb; t += nt) S[(t / nb) * ld + t % nb] = A[(size_t)(k0 + t / nb) * n + k0 + t % nb];
   __syncthreads();
   for (int j = 0; j < nb; j++) {
     double best = -1.0;
     int bi = j;
     for (int i = j + tid; i < m; i += nt) {
-      double v = fabs(S[i * nb + j]);
+      double v = fabs(S[i * ld + j]);
       if (v > best) { best = v; bi = i; }
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -70,24 +68,24 @@ __global__ void __launch_bounds__(1024) k_lu_panel(int n, int k0, int nb, double
     __syncthreads();
     const int p = spiv;
     if (p != j && tid < nb) {
-      double t = S[j * nb + tid];
-      S[j * nb + tid] = S[p * nb + tid];
-      S[p * nb + tid] = t;
+      double t = S[j * ld + tid];
+      S[j * ld + tid] = S[p * ld + tid];
+      S[p * ld + tid] = t;
     }
     __syncthreads();
-    const double d = S[j * nb + j];
+    const double d = S[j * ld + j];
     const double inv = d != 0.0 ? 1.0 / d : 0.0;
-    for (int i = j + 1 + tid; i < m; i += nt) S[i * nb + j] *= inv;
+    for (int i = j + 1 + tid; i < m; i += nt) S[i * ld + j] *= inv;
     __syncthreads();
     const int w = nb - j - 1;
     if (w > 0)
       for (int t = tid; t < (m - j - 1) * w; t += nt) {
         const int i = j + 1 + t / w, c = j + 1 + t % w;
-        S[i * nb + c] -= S[i * nb + j] * S[j * nb + c];
+        S[i * ld + c] -= S[i * ld + j] * S[j * ld + c];
       }
     __syncthreads();
   }
-  for (int t = tid; t < m * nb; t += nt) A[(size_t)(k0 + t / nb) * n + k0 + t % nb] = S[t];
+  for (int t = tid; t < m * nb; t += nt) A[(size_t)(k0 + t / nb) * n + k0 + t % nb] = S[(t / nb) * ld + t % nb];
 }
 
 // row interchanges of panel k0 on the columns outside the panel
@@ -146,37 +144,77 @@ __global__ void __launch_bounds__(256) k_lu_gemm(int n, int k0, int nb, double *
   }
 }
 
-// 16 columns of the inverse per block: y = P e_c, L y' = y, U x = y'
-constexpr int INV_COLS = 16;
-__global__ void __launch_bounds__(32 * INV_COLS) k_lu_inverse(int n, const double *__restrict__ LU,
-                                                              const int *__restrict__ piv, double *Inv) {
-  extern __shared__ double Y[];  // n x INV_COLS
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int c = blockIdx.x * INV_COLS + w;
-  for (int i = lane; i < n; i += 32) Y[i * INV_COLS + w] = (i == c) ? 1.0 : 0.0;
-  __syncwarp();
-  if (lane == 0)
+// Inverse from the factors, X = U^{-1} L^{-1} P, by block rows of LU_NB:
+// X starts as the permuted identity; a block-row step updates
+// X_i -= sum_j LU_ij X_j over the block rows already final (j < i for L, j > i
+// for U) and then solves with the diagonal block (unit lower / upper).  Each
+// block of 32 threads x 8 owns 32 right-hand-side columns, so a step is a
+// small GEMM plus a 32-step triangular solve, and the 2 n / LU_NB steps are
+// the only sequential chain (instead of 2 n dependent dot products).
+__global__ void k_lu_perm_identity(int n, const int *__restrict__ piv, int *perm) {
+  // perm[i] = original row that the interchanges bring to position i
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (int i = 0; i < n; i++) perm[i] = i;
     for (int k = 0; k < n; k++) {
       const int p = piv[k];
-      if (p != k) { double t = Y[k * INV_COLS + w]; Y[k * INV_COLS + w] = Y[p * INV_COLS + w]; Y[p * INV_COLS + w] = t; }
+      if (p != k) { int t = perm[k]; perm[k] = perm[p]; perm[p] = t; }
     }
-  __syncwarp();
-  for (int i = 1; i < n; i++) {
-    double s = 0.0;
-    for (int j = lane; j < i; j += 32) s += LU[(size_t)i * n + j] * Y[j * INV_COLS + w];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) Y[i * INV_COLS + w] -= s;
-    __syncwarp();
   }
-  for (int i = n - 1; i >= 0; i--) {
-    double s = 0.0;
-    for (int j = i + 1 + lane; j < n; j += 32) s += LU[(size_t)i * n + j] * Y[j * INV_COLS + w];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) Y[i * INV_COLS + w] = (Y[i * INV_COLS + w] - s) / LU[(size_t)i * n + i];
-    __syncwarp();
+}
+__global__ void k_lu_fill_perm(int n, const int *__restrict__ perm, double *X) {
+  const int i = blockIdx.x;
+  if (i >= n) return;
+  const int pc = perm[i];
+  for (int c = threadIdx.x; c < n; c += blockDim.x) X[(size_t)i * n + c] = (c == pc) ? 1.0 : 0.0;
+}
+
+template <bool LOWER>
+__global__ void __launch_bounds__(256) k_lu_inv_step(int n, int ib, const double *__restrict__ LU, double *X) {
+  __shared__ double B[LU_NB][LU_NB + 1], T[LU_NB][LU_NB + 1], Xs[LU_NB][LU_NB + 1];
+  const int r0 = ib * LU_NB, nr = min(LU_NB, n - r0);
+  const int c0 = blockIdx.x * LU_NB;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 columns x 8 row groups
+  const int c = c0 + tx;
+  for (int r = ty; r < LU_NB; r += 8) B[r][tx] = (r < nr && c < n) ? X[(size_t)(r0 + r) * n + c] : 0.0;
+  const int nblk = (n + LU_NB - 1) / LU_NB;
+  const int jb0 = LOWER ? 0 : ib + 1, jb1 = LOWER ? ib : nblk;
+  for (int jb = jb0; jb < jb1; jb++) {
+    const int q0 = jb * LU_NB, nq = min(LU_NB, n - q0);
+    __syncthreads();
+    for (int r = ty; r < LU_NB; r += 8) {
+      T[r][tx] = (r < nr && tx < nq) ? LU[(size_t)(r0 + r) * n + q0 + tx] : 0.0;
+      Xs[r][tx] = (r < nq && c < n) ? X[(size_t)(q0 + r) * n + c] : 0.0;
+    }
+    __syncthreads();
+    for (int r = ty; r < LU_NB; r += 8) {
+      double s = 0.0;
+#pragma unroll 8
+      for (int k = 0; k < LU_NB; k++) s += T[r][k] * Xs[k][tx];
+      B[r][tx] -= s;
+    }
   }
-  if (c < n)
-    for (int i = lane; i < n; i += 32) Inv[(size_t)i * n + c] = Y[i * INV_COLS + w];
+  __syncthreads();
+  // diagonal block
+  for (int r = ty; r < LU_NB; r += 8) T[r][tx] = (r < nr && tx < nr) ? LU[(size_t)(r0 + r) * n + r0 + tx] : 0.0;
+  __syncthreads();
+  if (ty == 0) {
+    if (LOWER) {
+      for (int r = 1; r < nr; r++) {
+        double s = B[r][tx];
+        for (int k = 0; k < r; k++) s -= T[r][k] * B[k][tx];
+        B[r][tx] = s;
+      }
+    } else {
+      for (int r = nr - 1; r >= 0; r--) {
+        double s = B[r][tx];
+        for (int k = r + 1; k < nr; k++) s -= T[r][k] * B[k][tx];
+        B[r][tx] = s / T[r][r];
+      }
+    }
+  }
+  __syncthreads();
+  for (int r = ty; r < nr; r += 8)
+    if (c < n) X[(size_t)(r0 + r) * n + c] = B[r][tx];
 }
 
 __global__ void k_csr_to_dense(int n, const int *__restrict__ rp, const int *__restrict__ kc, const double *__restrict__ a,
@@ -205,7 +243,7 @@ int coarse_factor(Handle &h) {
   Level &L = h.lv[0];
   const int n = L.N;
   if (n > LU_MAX_N) {
-    set_error("coarsest level too large for the dense direct solve (n > 864); use the SSOR coarse smoother");
+    set_error("coarsest level too large for the dense direct solve (n > 832); use the SSOR coarse smoother");
     return PMG_ERR_UNSUPPORTED;
   }
   PMG_TRY(h.coarse_lu.alloc((size_t)n * n));
@@ -215,13 +253,12 @@ int coarse_factor(Handle &h) {
   k_csr_to_dense<<<n, 256, 0, h.stream>>>(n, L.rowptr.p, L.kcol.p, L.A.p, h.coarse_lu.p); count_launches(1);
   static bool attr = false;
   if (!attr) {
-    PMG_CUDA(cudaFuncSetAttribute(k_lu_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, LU_MAX_N * LU_NB * 8));
-    PMG_CUDA(cudaFuncSetAttribute(k_lu_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, LU_MAX_N * INV_COLS * 8));
+    PMG_CUDA(cudaFuncSetAttribute(k_lu_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, LU_MAX_N * (LU_NB + 1) * 8));
     attr = true;
   }
   for (int k0 = 0; k0 < n; k0 += LU_NB) {
     const int nb = std::min(LU_NB, n - k0);
-    k_lu_panel<<<1, 1024, (size_t)(n - k0) * nb * 8, h.stream>>>(n, k0, nb, h.coarse_lu.p, h.coarse_piv.p, h.d_flags.p);
+    k_lu_panel<<<1, 1024, (size_t)(n - k0) * (nb + 1) * 8, h.stream>>>(n, k0, nb, h.coarse_lu.p, h.coarse_piv.p, h.d_flags.p);
     k_lu_swap<<<(n + 255) / 256, 256, 0, h.stream>>>(n, k0, nb, h.coarse_lu.p, h.coarse_piv.p);
     count_launches(2);
     const int rest = n - k0 - nb;
@@ -232,9 +269,19 @@ int coarse_factor(Handle &h) {
       count_launches(2);
     }
   }
-  k_lu_inverse<<<(n + INV_COLS - 1) / INV_COLS, 32 * INV_COLS, (size_t)n * INV_COLS * 8, h.stream>>>(
-      n, h.coarse_lu.p, h.coarse_piv.p, h.coarse_inv.p);
-  count_launches(1);
+  PMG_TRY(h.coarse_perm.alloc(n));
+  k_lu_perm_identity<<<1, 32, 0, h.stream>>>(n, h.coarse_piv.p, h.coarse_perm.p);
+  k_lu_fill_perm<<<n, 256, 0, h.stream>>>(n, h.coarse_perm.p, h.coarse_inv.p);
+  count_launches(2);
+  const int nblk = (n + LU_NB - 1) / LU_NB;
+  for (int ib = 0; ib < nblk; ib++) {
+    k_lu_inv_step<true><<<nblk, 256, 0, h.stream>>>(n, ib, h.coarse_lu.p, h.coarse_inv.p);
+    count_launches(1);
+  }
+  for (int ib = nblk - 1; ib >= 0; ib--) {
+    k_lu_inv_step<false><<<nblk, 256, 0, h.stream>>>(n, ib, h.coarse_lu.p, h.coarse_inv.p);
+    count_launches(1);
+  }
   PMG_CUDA(cudaGetLastError());
   int flags[4];
   PMG_CUDA(cudaMemcpyAsync(flags, h.d_flags.p, sizeof(flags), cudaMemcpyDeviceToHost, h.stream));
@@ -282,6 +329,7 @@ static int vcycle(Handle &h, int i, bool learned) {
   cudaStream_t s = h.stream;
   Level &L = h.lv[i];
   using PT = Prec<T>;
+  if (!learned && i >= 1 && i == h.cc_top) return coarse_cycle<T>(h, i);
   if (i == 0) {
     if (h.prm.coarse_smoother == PMG_COARSE_DIRECT) {
       PMG_CUDA(launch_pdl(k_dense_apply<T>, dim3((L.N * 32 + 255) / 256), dim3(256), 0, s, L.N,
@@ -357,6 +405,11 @@ static int prepare_levels(Handle &h) {
   PMG_TRY(sell_values<double>(h, h.lv.back()));
   if (h.prm.smoother == PMG_SMOOTHER_LEARNED) PMG_TRY(learned_prepare(h));
   if (h.prm.coarse_smoother == PMG_COARSE_DIRECT && !h.coarse_ready) PMG_TRY(coarse_factor(h));
+  const int cc = coarse_cycle_top(h);
+  if (cc != h.cc_top) {
+    h.cc_top = cc;
+    invalidate_graphs(&h);
+  }
   return PMG_OK;
 }
 

@@ -1,0 +1,55 @@
+"""The coarse end of the V-cycle as one thread-block-cluster launch gives the
+same solve as the level-by-level launches: same
+FGMRES iteration count (+-1) and solutions within 1e-8 relative (both stop at
+|r| <= 1e-10 |r0|; the two paths differ only in the order of partial sums
+inside a row).  The cluster launch is opt-in (PMG_COARSE_CLUSTER=1); each
+configuration runs in its own process because the switch is read once per
+process."""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+SCRIPT = r"""
+import json, sys, numpy as np
+sys.path.insert(0, {root!r})
+import parmoon_b200 as P
+elem, n, nl, prec, coarse = {args}
+levels = P.struct_hierarchy(elem, n, nl)
+h = P.Handle(nl, P.default_params(precision=prec, coarse_smoother=coarse))
+h.set_coefficients(P.coeff(kind=P.COEF_CONST, eps=1e-3, b=(1.0, 0.5, 0.25), f=1.0))
+P.load_hierarchy(h, levels, dirichlet=lambda x, y, z: (abs(x) < 1e-12).astype(float))
+h.assemble(-1, P.FORM_SUPG, copy_out=False)
+_, st, rc = h.solve()
+x = h.get_solution()
+np.save({out!r}, x)
+print(json.dumps(dict(rc=rc, its=st.iterations, rel=st.rel_res)))
+"""
+
+
+def run(tmp_path, tag, args, cluster):
+    out = str(tmp_path / f"{tag}.npy")
+    env = dict(os.environ)
+    env["PMG_COARSE_CLUSTER"] = "1" if cluster else "0"
+    p = subprocess.run([sys.executable, "-c", SCRIPT.format(root=ROOT, args=args, out=out)], env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-3000:]
+    return json.loads(p.stdout.strip().splitlines()[-1]), np.load(out)
+
+
+@pytest.mark.parametrize("elem,n,nl,prec,coarse", [(2, 16, 3, 1, 17), (1, 32, 4, 1, 17), (1, 32, 4, 0, 17),
+                                                   (2, 16, 3, 0, 3)])
+def test_cluster_coarse_cycle_matches_level_launches(tmp_path, elem, n, nl, prec, coarse):
+    args = (elem, n, nl, prec, coarse)
+    a, xa = run(tmp_path, "cluster", args, True)
+    b, xb = run(tmp_path, "levels", args, False)
+    assert a["rc"] == 0 and b["rc"] == 0 and a["rel"] <= 1e-10 and b["rel"] <= 1e-10
+    assert abs(a["its"] - b["its"]) <= 1, (a, b)
+    assert np.linalg.norm(xa - xb) <= 1e-8 * np.linalg.norm(xb)
