@@ -102,6 +102,18 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def max_over_ranks(value, dist, device=None):
+    """The largest of the ranks' values (the job's time is its slowest rank's);
+    the value itself without a process group."""
+    if dist is None or not dist.is_initialized():
+        return value
+    import torch
+    dev = device or ("cuda" if dist.get_backend() == "nccl" else "cpu")
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dirichlet(x, y, z):
     return (np.abs(x) < 1e-12).astype(float)
 
@@ -208,12 +220,7 @@ def bench_ours(args, rank, world, dist):
     cnt1 = ctypes.c_ulonglong()
     lib.pmg_launch_count(ctypes.byref(cnt1))
     sync()
-    step_time = statistics.mean(times)
-    if dist is not None:
-        import torch
-        tt = torch.tensor([step_time], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        step_time = float(tt.item())
+    step_time = max_over_ranks(statistics.mean(times), dist)
 
     # finest-level assembly throughput (one Assemble() of the finest level)
     asm_fine = []

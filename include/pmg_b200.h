@@ -278,6 +278,9 @@ int pmg_learned_stencil(pmg_handle h, int level, float *W_out);
  * W r)|^2 / |r|^2; lr > 0 applies an Adam step on the device. */
 int pmg_learned_train_step(pmg_handle h, int level, int n_samples, const double *e_dev, const double *r_dev, float lr,
                            double *loss_out, float *grad_out);
+/* One Adam step from a host gradient (e.g. the mean of the ranks' gradients
+ * of pmg_learned_train_step with lr = 0, for data-parallel training). */
+int pmg_learned_apply_gradient(pmg_handle h, const float *grad, float lr);
 /* One V-cycle z = MG(v) (the preconditioner) on device vectors of the
  * finest level (TMultiGridScaIte::Iterate with zero start). */
 int pmg_vcycle(pmg_handle h, const double *v_dev, double *z_dev);

@@ -286,6 +286,11 @@ class Handle:
                                             ctypes.c_float(lr), ctypes.byref(loss), _ptr(g)))
         return loss.value, g
 
+    def learned_apply_gradient(self, grad, lr):
+        """Adam step from a host gradient (data-parallel training applies the ranks' mean)."""
+        g = np.ascontiguousarray(grad, dtype=np.float32)
+        _check(lib().pmg_learned_apply_gradient(self.h, _ptr(g), ctypes.c_float(lr)))
+
     def vcycle(self, v_ptr, z_ptr):
         """z = MG(v) on device vectors of the finest level."""
         _check(lib().pmg_vcycle(self.h, _p(v_ptr), _p(z_ptr)))

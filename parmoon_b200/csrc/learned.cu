@@ -350,6 +350,23 @@ __global__ void k_adam(int n, float *__restrict__ p, const float *__restrict__ g
 
 using namespace pmg;
 
+// Adam on the FP32 master weights (BF16 copy refreshed) from a host gradient
+static int adam_step(pmg::Handle *h, const float *g, float lr) {
+  using namespace pmg;
+  cudaStream_t s = h->stream;
+  PMG_CUDA(cudaMemcpyAsync(h->lw_grad.p, g, sizeof(float) * NET_NPARAM, cudaMemcpyHostToDevice, s));
+  h->adam_t++;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.0f - powf(b1, (float)h->adam_t), c2 = 1.0f - powf(b2, (float)h->adam_t);
+  k_adam<<<(NET_NPARAM + 255) / 256, 256, 0, s>>>(NET_NPARAM, h->lw_master.p, h->lw_grad.p, h->lw_m.p, h->lw_v.p, lr,
+                                                   b1, b2, 1e-8f, c1, c2, reinterpret_cast<__nv_bfloat16 *>(h->lw_bf16.p));
+  count_launches(1);
+  PMG_CUDA(cudaGetLastError());
+  PMG_CUDA(cudaStreamSynchronize(s));
+  for (auto &Lv : h->lv) Lv.lw_fresh = false;
+  return PMG_OK;
+}
+
 extern "C" {
 
 int pmg_learned_num_params(int *n) {
@@ -502,18 +519,33 @@ int pmg_learned_train_step(pmg_handle hh, int level, int n_samples, const double
   PMG_CUDA(cudaMemcpy(g.data(), gw, sizeof(float) * NET_NPARAM, cudaMemcpyDeviceToHost));
   for (auto &x : g) x /= (float)n_samples;
   if (grad_out) std::copy(g.begin(), g.end(), grad_out);
-  if (lr > 0) {
-    PMG_CUDA(cudaMemcpy(gw, g.data(), sizeof(float) * NET_NPARAM, cudaMemcpyHostToDevice));
-    h->adam_t++;
-    const float b1 = 0.9f, b2 = 0.999f;
-    const float c1 = 1.0f - powf(b1, (float)h->adam_t), c2 = 1.0f - powf(b2, (float)h->adam_t);
-    k_adam<<<(NET_NPARAM + 255) / 256, 256, 0, s>>>(NET_NPARAM, h->lw_master.p, gw, h->lw_m.p, h->lw_v.p, lr, b1, b2,
-                                                     1e-8f, c1, c2, reinterpret_cast<__nv_bfloat16 *>(h->lw_bf16.p));
-    count_launches(1);
-    PMG_CUDA(cudaStreamSynchronize(s));
-    for (auto &Lv : h->lv) Lv.lw_fresh = false;
-  }
+  if (lr > 0) PMG_TRY(adam_step(h, g.data(), lr));
   return PMG_OK;
+}
+
+int pmg_learned_apply_gradient(pmg_handle hh, const float *grad, float lr) {
+  Handle *h = reinterpret_cast<Handle *>(hh);
+  if (!h || !grad || !(lr > 0)) {
+    set_error("pmg_learned_apply_gradient: bad arguments");
+    return PMG_ERR_ARG;
+  }
+  if (!h->lw_master.p) {
+    set_error("pmg_learned_apply_gradient: set the weights first");
+    return PMG_ERR_STATE;
+  }
+  for (int k = 0; k < NET_NPARAM; k++)
+    if (!std::isfinite(grad[k])) {
+      set_error("pmg_learned_apply_gradient: non-finite gradient");
+      return PMG_ERR_NONFINITE;
+    }
+  PMG_TRY(h->lw_grad.alloc(NET_NPARAM));
+  PMG_TRY(h->lw_m.alloc(NET_NPARAM));
+  PMG_TRY(h->lw_v.alloc(NET_NPARAM));
+  if (h->adam_t == 0) {
+    PMG_CUDA(cudaMemsetAsync(h->lw_m.p, 0, sizeof(float) * NET_NPARAM, h->stream));
+    PMG_CUDA(cudaMemsetAsync(h->lw_v.p, 0, sizeof(float) * NET_NPARAM, h->stream));
+  }
+  return adam_step(h, grad, lr);
 }
 
 }  // extern "C"

@@ -92,6 +92,60 @@ def train(problems, weights, steps, lr=1e-3, batch=4, seed=0, log_every=0):
     return cur, hist
 
 
+def allreduce_mean(g, dist=None):
+    """Mean of a host array over the ranks of the default process group (identity without one).
+    Runs on the backend's device: CPU tensors under gloo, CUDA tensors under nccl."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return np.asarray(g, dtype=np.float32)
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.from_numpy(np.ascontiguousarray(g, dtype=np.float32)).to(dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return (t / dist.get_world_size()).cpu().numpy()
+
+
+def train_data_parallel(grad_fn, apply_fn, steps, dist=None):
+    """Data-parallel training: every rank computes the gradient on its own
+    problems (grad_fn(step) -> (loss, grad)), the gradients are averaged over
+    the ranks (one all-reduce of the 57k-float gradient per step) and every
+    rank applies the same update (apply_fn(mean_grad)), so the ranks' weights
+    stay identical.  Returns the ranks' mean loss per step."""
+    hist = []
+    for it in range(steps):
+        loss, g = grad_fn(it)
+        g = allreduce_mean(g, dist)
+        loss = float(allreduce_mean(np.array([loss], dtype=np.float32), dist)[0])
+        apply_fn(g)
+        hist.append(loss)
+    return hist
+
+
+def train_dp_device(problems, weights, steps, lr=1e-3, batch=4, seed=0, dist=None):
+    """train() spread over the ranks of `dist`: each rank holds its own problems
+    (handle, hierarchy, E, R) on its GPU; the mean gradient drives one Adam step
+    per rank (pmg_learned_apply_gradient)."""
+    rank = dist.get_rank() if dist is not None and dist.is_initialized() else 0
+    rng = np.random.default_rng(seed + 1000 * rank)
+    for h, _, _, _ in problems:
+        h.set_learned_weights(weights)
+    state = {"w": np.asarray(weights, dtype=np.float32)}
+
+    def grad_fn(it):
+        h, lv, E, R = problems[rng.integers(len(problems))]
+        h.set_learned_weights(state["w"])
+        idx = rng.integers(E.shape[0] - batch + 1)
+        return h.learned_train_step(len(lv) - 1, E[idx].data_ptr(), R[idx].data_ptr(), batch, 0.0, want_grad=True)
+
+    h0 = problems[0][0]
+
+    def apply_fn(g):
+        h0.learned_apply_gradient(g, lr)
+        state["w"] = h0.get_learned_weights()
+
+    hist = train_data_parallel(grad_fn, apply_fn, steps, dist)
+    return state["w"], hist
+
+
 def evaluate(weights, seeds, n=128, levels=5, learned_steps=(2, 4)):
     """Time to |r|/|r0| <= 1e-10 on held-out problems: plain FP64 GMG (SSOR), FP32 SSOR
     V-cycle and FP32 learned-smoother V-cycle (with its SSOR guard), all in FP64 FGMRES."""

@@ -84,3 +84,21 @@ def test_training_gain_and_guarded_solve(pmg):
     for h, *_ in probs:
         h.close()
     hv.close()
+
+
+def test_data_parallel_step_equals_device_step(pmg):
+    """One rank of the data-parallel loop (gradient to the host, mean over
+    ranks, pmg_learned_apply_gradient) reproduces the fused device step
+    (pmg_learned_train_step with lr > 0) exactly."""
+    from parmoon_b200 import learned as PL
+    w0 = PL.init_weights(1)
+    h, lv = PL.make_problem(7, 8, 2)
+    E, R = PL.generate_pairs(h, lv, 2, 3, 1)
+    probs = [(h, lv, E, R)]
+    wa, ha = PL.train(probs, w0, 12, lr=2e-3, batch=2, seed=3)
+    h2, lv2 = PL.make_problem(7, 8, 2)
+    wb, hb = PL.train_dp_device([(h2, lv2, E, R)], w0, 12, lr=2e-3, batch=2, seed=3)
+    assert np.array_equal(wa, wb)
+    assert np.allclose(ha, hb, rtol=1e-6)
+    h.close()
+    h2.close()

@@ -1,0 +1,46 @@
+"""Host logic of the multi-process paths on CPU (gloo, world size 2): the
+gradient average of data-parallel training of the learned smoother, the
+identical updates it leads to on every rank, and the max-over-ranks timing of
+bench.py.  No GPU."""
+import os
+import socket
+
+import numpy as np
+import torch.multiprocessing as mp
+
+import dist_workers as W
+
+
+def free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def test_data_parallel_training_and_rank_max(tmp_path):
+    world = 2
+    mp.start_processes(W.dp_training, args=(world, free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    r = [np.load(os.path.join(tmp_path, f"rank{k}.npz")) for k in range(world)]
+    # every rank holds the same weights after training
+    assert np.array_equal(r[0]["w"], r[1]["w"])
+    # ... equal to one process that applies the mean of the ranks' gradients
+    probs = [W.quadratic_problem(k) for k in range(world)]
+    w = np.zeros(8, dtype=np.float32)
+    losses = []
+    for _ in range(25):
+        gs, ls = [], []
+        for A, y in probs:
+            res = A @ w - y
+            ls.append(0.5 * float(res @ res))
+            gs.append((A.T @ res).astype(np.float32))
+        g = np.mean(np.stack(gs), axis=0).astype(np.float32)
+        losses.append(np.mean(ls))
+        w = (w - 0.01 * g).astype(np.float32)
+    assert np.allclose(r[0]["w"], w, rtol=1e-5, atol=1e-6)
+    assert np.allclose(r[0]["hist"], losses, rtol=1e-5)
+    assert losses[-1] < losses[0]
+    assert np.allclose(r[0]["mean"], 1.5) and np.allclose(r[1]["mean"], 1.5)
+    assert float(r[0]["mx"]) == 1.5 and float(r[1]["mx"]) == 1.5
