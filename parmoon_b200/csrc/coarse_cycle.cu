@@ -1,23 +1,25 @@
 // The coarse end of the V-cycle in one launch: one thread-block cluster
-// (16 CTAs x 32 warps on one GPC) runs TMultiGrid3D::Cycle
+// (up to 16 CTAs x 32 warps on one GPC) runs TMultiGrid3D::Cycle
 // (src/FE/MultiGrid3D.C:449-695) for every level from `top` down to the
 // coarsest and back up -- pre-smoothing, defect, restriction, the coarsest
 // solve, prolongation, post-smoothing -- with a cluster barrier wherever the
-// level-by-level path would start a new kernel.
+// level-by-level path starts a new kernel.
 //
-// Why: below ~40k rows a colour sweep is a few microseconds of work, so the
-// colour-by-colour launches of the fine levels (2 x 27 per Q2 SSOR step) are
-// pure launch latency there: levels 1-2 of the 64^3 Q2 hierarchy took longer
-// than the 2.1M-row finest level.  A cluster barrier costs a fraction of a
-// launch, and the coarse levels' matrices (a few MB) stay in L2.
+// Why: below ~50k rows a colour sweep is a few microseconds of work, so the
+// colour-by-colour launches (2 x 27 per Q2 SSOR step) are launch and L2
+// latency: levels 1-2 of the 64^3 Q2 hierarchy cost about as much as the
+// 2.1M-row finest level.
 //
-// Memory: the vectors of a level are read with ld.global.cg and written with
-// st.global.cg (L2, never a stale L1 line of another SM), the matrices with
-// the read-only path; barrier.cluster.arrive.release / wait.acquire orders the
-// writes of one CTA before the reads of the others.  The arithmetic is the
-// level-by-level path's: the same SELL-32 slices, colour order, omega,
-// damping and coarsest solve, so both give the same iterates up to the order
-// of the partial sums inside a row.
+// Layout: every CTA keeps a full copy of the iterate x of each level of the
+// cycle in its shared memory (35,937 + 4,913 + 729 floats for the 64^3 Q2
+// hierarchy, 166 KB).  A colour pass gathers x from the local copy (no L2
+// round trip) and a row update is stored to all copies through distributed
+// shared memory; barrier.cluster.arrive.release / wait.acquire between passes
+// makes the stores visible.  Matrices, f, d and the transfers stay in global
+// memory (L2-resident at these sizes) and are loaded before the x gathers.
+// The arithmetic is the level-by-level path's -- the same SELL-32 slices,
+// colour order, omega, damping and coarsest solve -- up to the order of the
+// partial sums inside a row.
 #include "pmg_internal.h"
 #include <cooperative_groups.h>
 #include <cstdlib>
@@ -27,11 +29,11 @@ namespace cg = cooperative_groups;
 namespace pmg {
 
 constexpr int CC_MAX_LEVELS = 8, CC_MAX_GROUPS = 64, CC_WARPS = 32;
-constexpr int CC_MAX_ROWS = 65536;  // levels up to this size go into the cluster launch
+constexpr size_t CC_SMEM_X = 200 * 1024;  // budget for the replicated iterates
 
 template <typename T>
 struct CcLevel {
-  int N, Na, ncolors;
+  int N, Na, ncolors, xoff;  // xoff: offset of the level's x copy in shared memory
   int group[CC_MAX_GROUPS];  // slice range of colour c: [group[c], group[c+1]); group[ncolors+1] = all slices
   const int *perm, *sptr, *col;
   const T *val, *invd;
@@ -55,7 +57,12 @@ struct CcCtx {
   cg::cluster_group cl;
   int warp, lane, gw, tw, rank, nblocks;
   T (*part)[32];
+  T *xs;  // this CTA's shared memory holding the x copies
   __device__ void sync() { cl.sync(); }
+  // x_i := v in every CTA's copy
+  __device__ void bcast(int off, int i, T v) {
+    for (int b = 0; b < nblocks; b++) *cl.map_shared_rank(xs + off + i, b) = v;
+  }
 };
 
 // one pass over the slices [s0, s1): Gauss-Seidel update of x (GS) or d = f - A x
@@ -69,39 +76,42 @@ __device__ void cc_slices(CcCtx<T> &c, const CcLevel<T> &L, int s0, int s1, T om
   const int per_round = spc * c.nblocks;
   const int rounds = (nsl + per_round - 1) / per_round;
   const int k = c.warp % K;
-  constexpr int CC_PF = sizeof(T) == 4 ? 16 : 8;  // column steps loaded ahead (64 registers per thread)
+  constexpr int PF = sizeof(T) == 4 ? 16 : 8;  // column steps loaded ahead (64 registers per thread)
+  const T *x = c.xs + L.xoff;
   for (int r = 0; r < rounds; r++) {
     const int sl = s0 + r * per_round + c.rank * spc + c.warp / K;
-    T sum = 0;
+    T sum = 0, fr = 0, id = 0;
+    int row = -1;
     if (sl < s1) {
       const int off = __ldg(L.sptr + sl), lmax = (__ldg(L.sptr + sl + 1) - off) >> 5;
       const int *cp = L.col + off + c.lane;
       const T *vp = L.val + off + c.lane;
-      // all loads of the first CC_PF column steps first, then the x gathers:
-      // two L2 round trips per pass instead of one per unrolled group
-      int ci[CC_PF];
-      T cv[CC_PF];
+      int ci[PF];
+      T cv[PF];
 #pragma unroll
-      for (int u = 0; u < CC_PF; u++) {
+      for (int u = 0; u < PF; u++) {
         const int j = k + u * K;
         ci[u] = j < lmax ? __ldg(cp + 32 * j) : -1;
         cv[u] = j < lmax ? __ldg(vp + 32 * j) : (T)0;
       }
+      if (k == 0) {
+        row = __ldg(L.perm + sl * 32 + c.lane);
+        if (row >= 0) {
+          fr = __ldcg(L.f + row);
+          if (GS) id = __ldg(L.invd + sl * 32 + c.lane);
+        }
+      }
 #pragma unroll
-      for (int u = 0; u < CC_PF; u++)
-        if (ci[u] >= 0) sum += cv[u] * __ldcg(L.x + ci[u]);
-      for (int j = k + CC_PF * K; j < lmax; j += K) sum += __ldg(vp + 32 * j) * __ldcg(L.x + __ldg(cp + 32 * j));
+      for (int u = 0; u < PF; u++)
+        if (ci[u] >= 0) sum += cv[u] * x[ci[u]];
+      for (int j = k + PF * K; j < lmax; j += K) sum += __ldg(vp + 32 * j) * x[__ldg(cp + 32 * j)];
     }
     c.part[c.warp][c.lane] = sum;
     __syncthreads();
-    if (k == 0 && sl < s1) {
+    if (k == 0 && row >= 0) {
       for (int kk = 1; kk < K; kk++) sum += c.part[c.warp + kk][c.lane];
-      const int row = __ldg(L.perm + sl * 32 + c.lane);
-      if (row >= 0) {
-        const T fr = __ldcg(L.f + row);
-        if (GS) __stcg(L.x + row, __ldcg(L.x + row) + omega * (fr - sum) * __ldg(L.invd + sl * 32 + c.lane));
-        else __stcg(L.d + row, fr - sum);
-      }
+      if (GS) c.bcast(L.xoff, row, x[row] + omega * (fr - sum) * id);
+      else __stcg(L.d + row, fr - sum);
     }
     __syncthreads();
   }
@@ -110,8 +120,9 @@ __device__ void cc_slices(CcCtx<T> &c, const CcLevel<T> &L, int s0, int s1, T om
 // SSOR step of TMGLevel3D::SSOR in colour order: Dirichlet rows from f, forward, backward
 template <typename T>
 __device__ void cc_ssor(CcCtx<T> &c, const CcLevel<T> &L, T omega) {
-  for (int i = L.Na + c.gw * 32 + c.lane; i < L.N; i += c.tw * 32) __stcg(L.x + i, __ldcg(L.f + i));
-  c.sync();
+  // every CTA refreshes the Dirichlet rows of its own copy
+  for (int i = L.Na + threadIdx.x; i < L.N; i += blockDim.x) c.xs[L.xoff + i] = __ldcg(L.f + i);
+  __syncthreads();
   for (int cc = 0; cc < L.ncolors; cc++) {
     cc_slices<T, true>(c, L, L.group[cc], L.group[cc + 1], omega);
     c.sync();
@@ -125,6 +136,7 @@ __device__ void cc_ssor(CcCtx<T> &c, const CcLevel<T> &L, T omega) {
 template <typename T>
 __global__ void __launch_bounds__(CC_WARPS * 32, 1) k_coarse_cycle(const __grid_constant__ CcArgs<T> a) {
   __shared__ T part[CC_WARPS][32];
+  extern __shared__ __align__(16) unsigned char cc_dyn[];
   CcCtx<T> c{cg::this_cluster()};
   c.warp = threadIdx.x >> 5;
   c.lane = threadIdx.x & 31;
@@ -133,14 +145,21 @@ __global__ void __launch_bounds__(CC_WARPS * 32, 1) k_coarse_cycle(const __grid_
   c.gw = c.rank * CC_WARPS + c.warp;
   c.tw = c.nblocks * CC_WARPS;
   c.part = part;
+  c.xs = reinterpret_cast<T *>(cc_dyn);
+  const int top = a.nlev - 1;
+  // the entry level starts from x = 0 (the caller zeroed its global copy)
+  for (int i = threadIdx.x; i < a.lv[top].N; i += blockDim.x) c.xs[a.lv[top].xoff + i] = (T)0;
   pdl_wait();
   pdl_trigger();
+  c.sync();  // every copy initialised before any remote store
   // down: smooth, defect, restrict
-  for (int l = a.nlev - 1; l >= 1; l--) {
+  for (int l = top; l >= 1; l--) {
     const CcLevel<T> &L = a.lv[l];
     const CcLevel<T> &C = a.lv[l - 1];
     for (int s = 0; s < a.pre; s++) cc_ssor(c, L, a.omega);
     cc_slices<T, false>(c, L, 0, L.group[L.ncolors + 1], a.omega);
+    // each CTA zeroes its own copy of the coarse iterate
+    for (int i = threadIdx.x; i < C.N; i += blockDim.x) c.xs[C.xoff + i] = (T)0;
     c.sync();
     // restriction, 8 lanes per coarse row (R = P^T rows hold up to 125 entries)
     for (int base = c.gw * 4; base < C.N; base += c.tw * 4) {
@@ -154,10 +173,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, 1) k_coarse_cycle(const __grid_
       v += __shfl_xor_sync(0xffffffffu, v, 4);
       v += __shfl_xor_sync(0xffffffffu, v, 2);
       v += __shfl_xor_sync(0xffffffffu, v, 1);
-      if (l8 == 0 && row < C.N) {
-        __stcg(C.f + row, v);
-        __stcg(C.x + row, (T)0);
-      }
+      if (l8 == 0 && row < C.N) __stcg(C.f + row, v);
     }
     c.sync();
   }
@@ -169,27 +185,31 @@ __global__ void __launch_bounds__(CC_WARPS * 32, 1) k_coarse_cycle(const __grid_
       const double *ir = a.inv + (size_t)row * a.n0;
       for (int j = c.lane; j < a.n0; j += 32) s += __ldg(ir + j) * (double)__ldcg(Z.f + j);
       for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (c.lane == 0) __stcg(Z.x + row, (T)s);
+      if (c.lane == 0) c.bcast(Z.xoff, row, (T)s);
     }
     c.sync();
   } else {
     for (int s = 0; s < a.coarse_it; s++) cc_ssor(c, Z, a.omega);
   }
   // up: prolongate, smooth
-  for (int l = 1; l < a.nlev; l++) {
+  for (int l = 1; l <= top; l++) {
     const CcLevel<T> &L = a.lv[l];
     const CcLevel<T> &C = a.lv[l - 1];
     // prolongation, one fine row per lane (P rows hold at most 27 entries)
+    const T *xc = c.xs + C.xoff;
     for (int row = c.gw * 32 + c.lane; row < L.Na; row += c.tw * 32) {
       const int beg = __ldg(L.prp + row), end = __ldg(L.prp + row + 1);
       T v = 0;
 #pragma unroll 4
-      for (int q = beg; q < end; q++) v += __ldg(L.pval + q) * __ldcg(C.x + __ldg(L.pcol + q));
-      __stcg(L.x + row, __ldcg(L.x + row) + a.damp * v);
+      for (int q = beg; q < end; q++) v += __ldg(L.pval + q) * xc[__ldg(L.pcol + q)];
+      c.bcast(L.xoff, row, c.xs[L.xoff + row] + a.damp * v);
     }
     c.sync();
     for (int s = 0; s < a.post; s++) cc_ssor(c, L, a.omega);
   }
+  // the entry level's iterate back to global memory for the finer level
+  const CcLevel<T> &E = a.lv[top];
+  for (int i = c.rank * blockDim.x + threadIdx.x; i < E.N; i += c.nblocks * blockDim.x) __stcg(E.x + i, c.xs[E.xoff + i]);
 }
 
 template <typename T> static const T *lv_val(const Level &L);
@@ -211,10 +231,12 @@ static int cluster_ctas() {
   if (ctas) return ctas;
   const void *kernel = (const void *)k_coarse_cycle<T>;
   cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CC_SMEM_X);
   for (int want : {16, 8, 4}) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(want);
     cfg.blockDim = dim3(CC_WARPS * 32);
+    cfg.dynamicSmemBytes = CC_SMEM_X;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = want;
@@ -235,19 +257,23 @@ static int cluster_ctas() {
 // the highest level that, with every level below it, fits the cluster launch
 // (0: none -- the level-by-level path runs)
 int coarse_cycle_top(const Handle &h) {
-  static int off = -1;
-  if (off < 0) {
-    // opt-in: on the 64^3 Q2 hierarchy this launch measured slower than the
-    // PDL-chained colour launches (a colour pass still waits for two
-    // dependent L2 round trips and a cluster barrier)
+  static int on = -1;
+  if (on < 0) {
+    // opt-in (PMG_COARSE_CLUSTER=1): on the 64^3 Q2 hierarchy a colour pass
+    // of this launch (loads, gathers, broadcast stores, cluster barrier)
+    // measured ~7 us against ~4.4 us for a PDL-chained colour launch
     const char *e = getenv("PMG_COARSE_CLUSTER");
-    off = (e && e[0] == '1') ? 0 : 1;
+    on = (e && e[0] == '1') ? 1 : 0;
   }
-  if (off) return 0;
+  if (!on) return 0;
+  // levels from the coarsest up while their iterates fit the shared-memory budget
+  const size_t vb = h.prm.precision == PMG_PREC_FP32 ? sizeof(float) : sizeof(double);
+  size_t bytes = 0;
   int top = 0;
   for (int i = 0; i < (int)h.lv.size() - 1 && i < CC_MAX_LEVELS; i++) {
     const Level &L = h.lv[i];
-    if (L.N > CC_MAX_ROWS || (int)L.sell_group.size() > CC_MAX_GROUPS) break;
+    bytes += ((size_t)L.N * vb + 15) / 16 * 16;
+    if (bytes > CC_SMEM_X || (int)L.sell_group.size() > CC_MAX_GROUPS) break;
     top = i;
   }
   // the launch shape is queried here, outside any stream capture
@@ -263,11 +289,14 @@ int coarse_cycle(Handle &h, int top) {
   }
   CcArgs<T> a{};
   a.nlev = top + 1;
+  size_t smem = 0;
   for (int i = 0; i <= top; i++) {
     Level &L = h.lv[i];
     CcLevel<T> &d = a.lv[i];
     d.N = L.N;
     d.Na = L.Na;
+    d.xoff = (int)(smem / sizeof(T));
+    smem += ((size_t)L.N * sizeof(T) + 15) / 16 * 16;
     d.ncolors = (int)L.sell_group.size() - 2;
     for (size_t g = 0; g < L.sell_group.size(); g++) d.group[g] = L.sell_group[g];
     d.perm = L.sell_perm.p;
@@ -296,9 +325,14 @@ int coarse_cycle(Handle &h, int top) {
     set_error("coarse_cycle: no thread-block cluster of 4 or more CTAs can be scheduled");
     return PMG_ERR_UNSUPPORTED;
   }
+  if (smem > CC_SMEM_X) {
+    set_error("coarse_cycle: iterates exceed the shared-memory budget");
+    return PMG_ERR_ARG;
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(ctas);
   cfg.blockDim = dim3(CC_WARPS * 32);
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = h.stream;
   cudaLaunchAttribute at[2];
   at[0].id = cudaLaunchAttributeClusterDimension;
