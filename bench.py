@@ -259,7 +259,7 @@ def bench_ours(args, rank, world, dist):
     fp64 = []
     for _ in range(2):
         _, st64, rc64 = h.solve()
-        fp64.append((st64.seconds, st64.iterations, st64.rel_res, rc64))
+        fp64.append((st64.seconds, st64.iterations, st64.rel_res, rc64, st64.vcycle_seconds))
     fp64_s = min(x[0] for x in fp64)
 
     line = None
@@ -283,8 +283,11 @@ def bench_ours(args, rank, world, dist):
                        "parallelism": f"replicas x{world}"},
             "iterations": st.iterations, "rel_res_fp64": st.rel_res, "res0": st.res0,
             "assembly_mnnz_s": nnz_fine / t_asm_fine / 1e6, "assembly_fine_s": t_asm_fine,
-            "fp64_gmg": {"solve_s": fp64_s, "iterations": fp64[0][1], "rel_res": fp64[0][2], "status": fp64[0][3]},
+            "fp64_gmg": {"solve_s": fp64_s, "iterations": fp64[0][1], "rel_res": fp64[0][2], "status": fp64[0][3],
+                         "vcycle_s": fp64[0][4]},
             "fp32_solve_s": statistics.mean(s.seconds for s in stats),
+            "fp32_solve_setup_s": statistics.mean(s.setup_seconds for s in stats),
+            "fp32_vcycle_s": statistics.mean(s.vcycle_seconds for s in stats),
             "wall_s_per_step": t_wall / args.steps,
             "roofline": {"bound": "hbm", "kernel": "k_sell_gs<float,K> (FP32 multicolour SSOR step on SELL-32, finest level)",
                          "achieved": ssor["gbs"], "peak": hbm, "unit": "GB/s", "frac": ssor["gbs"] / hbm,
@@ -303,7 +306,7 @@ def bench_ours(args, rank, world, dist):
     h.close()
 
 
-KERNELS = {"spmv64": 0, "spmv32": 1, "ssor64": 2, "ssor32": 3, "assemble": 4}
+KERNELS = {"spmv64": 0, "spmv32": 1, "ssor64": 2, "ssor32": 3, "assemble": 4, "coarse_factor": 6}
 
 
 def profile_kernel(name):
@@ -316,15 +319,15 @@ def profile_kernel(name):
     h = P.Handle(N_LEVELS, P.default_params(precision=P.PREC_FP32))
     h.set_coefficients(P.coeff(kind=P.COEF_CONST, eps=EPS, b=B, f=F))
     P.load_hierarchy(h, levels, dirichlet=dirichlet)
-    fine = N_LEVELS - 1
+    fine = 0 if name == "coarse_factor" else N_LEVELS - 1
     if name != "assemble":
         h.assemble(fine, P.FORM_SUPG, copy_out=False)
     sec, by, fl = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
     P._check(lib.pmg_time_kernel(h.h, KERNELS[name], fine, P.FORM_SUPG, 3, ctypes.byref(sec), ctypes.byref(by),
                                  ctypes.byref(fl)))
     hbm, kind = peaks()
-    print(json.dumps({"kernel": name, "n_cells": N_CELLS, "levels": N_LEVELS, "n_dofs": levels[-1]["N"],
-                      "nnz": int(levels[-1]["rowptr"][-1]), "seconds": sec.value, "bytes": by.value,
+    print(json.dumps({"kernel": name, "n_cells": N_CELLS, "levels": N_LEVELS, "level": fine, "n_dofs": levels[fine]["N"],
+                      "nnz": int(levels[fine]["rowptr"][-1]), "seconds": sec.value, "bytes": by.value,
                       "flops": fl.value, "gbs": by.value / sec.value / 1e9, "hbm_frac": by.value / sec.value / 1e9 / hbm,
                       "peak_kind": kind}))
     h.close()

@@ -117,6 +117,8 @@ typedef struct pmg_solve_stats {
     double mean_contraction;   /* (res_final/res0)^(1/iterations) */
     int    smoother_used;      /* PMG_SMOOTHER_* actually used (learned may fall back) */
     double seconds;            /* device time of the solve (CUDA events) */
+    double setup_seconds;      /* of which per-solve set-up: SELL values, coarsest factorisation, graph capture */
+    double vcycle_seconds;     /* device time of the first preconditioner application (one V-cycle) */
 } pmg_solve_stats;
 
 typedef struct pmg_handle_s *pmg_handle;
@@ -304,6 +306,7 @@ int pmg_last_timings(pmg_handle h, double *assemble_s, double *solve_s, double *
 #define PMG_KERNEL_SSOR32    3
 #define PMG_KERNEL_ASSEMBLE  4
 #define PMG_KERNEL_CSR_SPMV64 5
+#define PMG_KERNEL_COARSE_FACTOR 6  /* LU + inverse of the coarsest level (level must be 0) */
 int pmg_time_kernel(pmg_handle h, int kernel, int level, int form, int reps,
                     double *seconds_per_launch, double *bytes_per_launch, double *flops_per_launch);
 

@@ -46,7 +46,7 @@ class CoeffDesc(ctypes.Structure):
 
 class SolveStats(ctypes.Structure):
     _fields_ = [("iterations", _i), ("res0", _d), ("res_final", _d), ("rel_res", _d), ("mean_contraction", _d),
-                ("smoother_used", _i), ("seconds", _d)]
+                ("smoother_used", _i), ("seconds", _d), ("setup_seconds", _d), ("vcycle_seconds", _d)]
 
 
 class PmgError(RuntimeError):

@@ -47,8 +47,11 @@ template <typename T>
 struct CcArgs {
   int nlev;  // levels 0 .. nlev-1; the cycle enters at nlev-1
   CcLevel<T> lv[CC_MAX_LEVELS];
-  const double *inv;  // coarsest dense inverse (direct coarse solve) or NULL
-  int n0, coarse_it, pre, post;
+  const double *inv;  // inverse of the coarsest level's active block (direct coarse solve) or NULL
+  int direct, n0, na0, coarse_it, pre, post;
+  const int *rp0, *kc0;  // coarsest CSR (FP64 values a0) for the Dirichlet columns of the rhs
+  const double *a0;
+  double *t0;            // reduced rhs f_a - A_ad f_d
   T omega, damp;
 };
 
@@ -179,11 +182,27 @@ __global__ void __launch_bounds__(CC_WARPS * 32, 1) k_coarse_cycle(const __grid_
   }
   // coarsest level: dense inverse (SolveExact) or SSOR steps
   const CcLevel<T> &Z = a.lv[0];
-  if (a.inv) {
+  if (a.direct) {
+    // x_d = f_d; t = f_a - A_ad f_d
     for (int row = c.gw; row < a.n0; row += c.tw) {
+      if (row >= a.na0) {
+        if (c.lane == 0) c.bcast(Z.xoff, row, __ldcg(Z.f + row));
+        continue;
+      }
       double s = 0;
-      const double *ir = a.inv + (size_t)row * a.n0;
-      for (int j = c.lane; j < a.n0; j += 32) s += __ldg(ir + j) * (double)__ldcg(Z.f + j);
+      for (int k = __ldg(a.rp0 + row) + c.lane; k < __ldg(a.rp0 + row + 1); k += 32) {
+        const int j = __ldg(a.kc0 + k);
+        if (j >= a.na0) s += __ldg(a.a0 + k) * (double)__ldcg(Z.f + j);
+      }
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (c.lane == 0) __stcg(a.t0 + row, (double)__ldcg(Z.f + row) - s);
+    }
+    c.sync();
+    // x_a = A_aa^{-1} t
+    for (int row = c.gw; row < a.na0; row += c.tw) {
+      double s = 0;
+      const double *ir = a.inv + (size_t)row * a.na0;
+      for (int j = c.lane; j < a.na0; j += 32) s += __ldg(ir + j) * __ldcg(a.t0 + j);
       for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
       if (c.lane == 0) c.bcast(Z.xoff, row, (T)s);
     }
@@ -313,8 +332,14 @@ int coarse_cycle(Handle &h, int top) {
     d.d = lv_vec<T>(L, 2);
   }
   const bool direct = h.prm.coarse_smoother == PMG_COARSE_DIRECT;
+  a.direct = direct ? 1 : 0;
   a.inv = direct ? h.coarse_inv.p : nullptr;
   a.n0 = h.lv[0].N;
+  a.na0 = h.lv[0].Na;
+  a.rp0 = h.lv[0].rowptr.p;
+  a.kc0 = h.lv[0].kcol.p;
+  a.a0 = h.lv[0].A.p;
+  a.t0 = h.coarse_t.p;
   a.coarse_it = h.prm.coarse_maxit > 0 ? h.prm.coarse_maxit : 1;
   a.pre = h.prm.pre_smooth;
   a.post = h.prm.post_smooth;

@@ -160,7 +160,7 @@ int pmg_create(pmg_handle *out, int n_levels, const pmg_params *p) {
     set_error("pmg_create: stream creation failed");
     return PMG_ERR_CUDA;
   }
-  for (int k = 0; k < 6; k++) cudaEventCreate(&h->ev[k]);
+  for (int k = 0; k < 10; k++) cudaEventCreate(&h->ev[k]);
   int rc = h->d_flags.alloc(4);
   if (rc == PMG_OK) rc = h->red_partial.alloc(1024);
   if (rc == PMG_OK) rc = h->red_counter.alloc(1);
@@ -184,7 +184,7 @@ int pmg_destroy(pmg_handle hh) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->vgraph) cudaGraphExecDestroy(h->vgraph);
   if (h->vgraph_ssor) cudaGraphExecDestroy(h->vgraph_ssor);
-  for (int k = 0; k < 6; k++) if (h->ev[k]) cudaEventDestroy(h->ev[k]);
+  for (int k = 0; k < 10; k++) if (h->ev[k]) cudaEventDestroy(h->ev[k]);
   if (h->h_H) cudaFreeHost(h->h_H);
   h->lv.clear();
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -644,6 +644,7 @@ int pmg_time_kernel(pmg_handle hh, int kernel, int level, int form, int reps, do
       case PMG_KERNEL_SSOR32: return sell_ssor<float>(s, L, y32.p, x32.p, 1.0, h->num_sms);
       case PMG_KERNEL_CSR_SPMV64: return spmv<double>(s, L, L.A.p, x64.p, y64.p);
       case PMG_KERNEL_ASSEMBLE: return assemble_level(*h, L, form, L.A.p, true, L.rhs.p);
+      case PMG_KERNEL_COARSE_FACTOR: return coarse_factor(*h);
       default: set_error("pmg_time_kernel: unknown kernel"); return PMG_ERR_ARG;
     }
   };
@@ -663,6 +664,11 @@ int pmg_time_kernel(pmg_handle hh, int kernel, int level, int form, int reps, do
     double spmv_b = 8 * nnz + 4 * (N + 1) + 8 * N;
     by = kernel == PMG_KERNEL_SPMV32 ? spmv_b : 2 * spmv_b + 8 * N;
     fl = kernel == PMG_KERNEL_SPMV32 ? 2 * nnz : 4 * nnz;
+  } else if (kernel == PMG_KERNEL_COARSE_FACTOR) {
+    if (level != 0) { set_error("pmg_time_kernel: the coarse factorisation is of level 0"); return PMG_ERR_ARG; }
+    // LU (2/3 n^3) and inverse (4/3 n^3) flops; the dense matrix is read and written
+    by = 2.0 * 8.0 * N * N;
+    fl = 2.0 * N * N * N;
   } else {
     // coloured scatter per element: n_loc^2 (4 slot + 8 read + 8 write) + n_loc (4 dof + 16 rhs) + vertices
     const double nl = L.nloc, nv = L.nvert;

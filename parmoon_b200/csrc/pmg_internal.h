@@ -173,7 +173,7 @@ struct Handle {
   int device = 0;
   int num_sms = 148;
   // coarsest-level dense inverse (FP64)
-  DBuf<double> coarse_lu, coarse_inv;
+  DBuf<double> coarse_lu, coarse_inv, coarse_t;  // active block: LU, inverse; reduced rhs
   DBuf<int> coarse_piv, coarse_perm;
   bool coarse_ready = false;
   // FGMRES workspace
@@ -185,7 +185,7 @@ struct Handle {
   // error flags written by kernels (slot lookups, non-finite values)
   DBuf<int> d_flags;
   // timing
-  cudaEvent_t ev[6];
+  cudaEvent_t ev[10];
   double t_assemble = 0, t_solve = 0, t_assemble_kernel = 0;
   // V-cycle graph
   cudaGraphExec_t vgraph = nullptr;

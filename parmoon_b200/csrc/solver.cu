@@ -30,7 +30,7 @@ int level_invdiag(cudaStream_t s, Level &L, int *flags);
 //   k_lu_swap    applies the panel's row interchanges to the other columns
 //   k_lu_trsm    U12 = L11^{-1} A12 (one thread per column)
 //   k_lu_gemm    A22 -= L21 U12 (32 x 32 output tiles)
-// then the inverse is formed by block rows (k_lu_inv_step, below).
+// then the inverse is formed in one launch (k_lu_inverse_slab, below).
 constexpr int LU_NB = 32;
 constexpr int LU_MAX_N = 832;  // panel (n x 33 doubles) must fit in 227 KB of shared memory
 
@@ -56,14 +56,19 @@ __global__ void __launch_bounds__(1024) k_lu_panel(int n, int k0, int nb, double
     }
     if ((tid & 31) == 0) { sval[tid >> 5] = best; sidx[tid >> 5] = bi; }
     __syncthreads();
-    if (tid == 0) {
-      double b = -1.0;
-      int p = j;
-      for (int w = 0; w < nt / 32; w++)
-        if (sval[w] > b || (sval[w] == b && sidx[w] < p)) { b = sval[w]; p = sidx[w]; }
-      spiv = p;
-      piv[k0 + j] = k0 + p;
-      if (!(b > 0.0)) atomicOr(flags, 16);
+    if (tid < 32) {
+      double b = tid < (nt >> 5) ? sval[tid] : -1.0;
+      int p = tid < (nt >> 5) ? sidx[tid] : j;
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, b, o);
+        const int op = __shfl_xor_sync(0xffffffffu, p, o);
+        if (ob > b || (ob == b && op < p)) { b = ob; p = op; }
+      }
+      if (tid == 0) {
+        spiv = p;
+        piv[k0 + j] = k0 + p;
+        if (!(b > 0.0)) atomicOr(flags, 16);
+      }
     }
     __syncthreads();
     const int p = spiv;
@@ -77,12 +82,12 @@ __global__ void __launch_bounds__(1024) k_lu_panel(int n, int k0, int nb, double
     const double inv = d != 0.0 ? 1.0 / d : 0.0;
     for (int i = j + 1 + tid; i < m; i += nt) S[i * ld + j] *= inv;
     __syncthreads();
-    const int w = nb - j - 1;
-    if (w > 0)
-      for (int t = tid; t < (m - j - 1) * w; t += nt) {
-        const int i = j + 1 + t / w, c = j + 1 + t % w;
-        S[i * ld + c] -= S[i * ld + j] * S[j * ld + c];
-      }
+    // rank-1 update of the panel: lane = column to the right, warp = row group
+    const int w = nb - j - 1, cc = tid & 31, rg = tid >> 5, ng = nt >> 5;
+    if (cc < w) {
+      const double u = S[j * ld + j + 1 + cc];
+      for (int i = j + 1 + rg; i < m; i += ng) S[i * ld + j + 1 + cc] -= S[i * ld + j] * u;
+    }
     __syncthreads();
   }
   for (int t = tid; t < m * nb; t += nt) A[(size_t)(k0 + t / nb) * n + k0 + t % nb] = S[(t / nb) * ld + t % nb];
@@ -144,13 +149,11 @@ __global__ void __launch_bounds__(256) k_lu_gemm(int n, int k0, int nb, double *
   }
 }
 
-// Inverse from the factors, X = U^{-1} L^{-1} P, by block rows of LU_NB:
-// X starts as the permuted identity; a block-row step updates
-// X_i -= sum_j LU_ij X_j over the block rows already final (j < i for L, j > i
-// for U) and then solves with the diagonal block (unit lower / upper).  Each
-// block of 32 threads x 8 owns 32 right-hand-side columns, so a step is a
-// small GEMM plus a 32-step triangular solve, and the 2 n / LU_NB steps are
-// the only sequential chain (instead of 2 n dependent dot products).
+// Inverse from the factors, X = U^{-1} L^{-1} P: block b of the grid owns
+// the 32 columns [32 b, 32 b + 32) of X and keeps that n x 32 slab in shared
+// memory through both substitutions (left-looking: row i of the slab is
+// finished from the rows already final, L / U streamed from L2), so the whole
+// inverse is one launch; lane = column, warps take rows.
 __global__ void k_lu_perm_identity(int n, const int *__restrict__ piv, int *perm) {
   // perm[i] = original row that the interchanges bring to position i
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -161,99 +164,153 @@ __global__ void k_lu_perm_identity(int n, const int *__restrict__ piv, int *perm
     }
   }
 }
-__global__ void k_lu_fill_perm(int n, const int *__restrict__ perm, double *X) {
-  const int i = blockIdx.x;
-  if (i >= n) return;
-  const int pc = perm[i];
-  for (int c = threadIdx.x; c < n; c += blockDim.x) X[(size_t)i * n + c] = (c == pc) ? 1.0 : 0.0;
-}
 
-template <bool LOWER>
-__global__ void __launch_bounds__(256) k_lu_inv_step(int n, int ib, const double *__restrict__ LU, double *X) {
-  __shared__ double B[LU_NB][LU_NB + 1], T[LU_NB][LU_NB + 1], Xs[LU_NB][LU_NB + 1];
-  const int r0 = ib * LU_NB, nr = min(LU_NB, n - r0);
-  const int c0 = blockIdx.x * LU_NB;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 columns x 8 row groups
-  const int c = c0 + tx;
-  for (int r = ty; r < LU_NB; r += 8) B[r][tx] = (r < nr && c < n) ? X[(size_t)(r0 + r) * n + c] : 0.0;
-  const int nblk = (n + LU_NB - 1) / LU_NB;
-  const int jb0 = LOWER ? 0 : ib + 1, jb1 = LOWER ? ib : nblk;
-  for (int jb = jb0; jb < jb1; jb++) {
-    const int q0 = jb * LU_NB, nq = min(LU_NB, n - q0);
+constexpr int INV_COLS = 16, INV_THREADS = 256, INV_ROWS = INV_THREADS / INV_COLS;
+__global__ void __launch_bounds__(INV_THREADS) k_lu_inverse_slab(int n, const double *__restrict__ LU,
+                                                                const int *__restrict__ perm, double *Inv) {
+  extern __shared__ double sm[];
+  double *Xs = sm;           // n x INV_COLS, the block's columns of X
+  double *Rb = sm + (size_t)n * INV_COLS;  // INV_ROWS rows of L or U, staged
+  const int tid = threadIdx.x, rr = tid / INV_COLS, col = tid % INV_COLS;
+  const int warp = tid >> 5, lane = tid & 31, nwarps = INV_THREADS / 32;
+  const int c = blockIdx.x * INV_COLS + col;
+  for (int i = rr; i < n; i += INV_ROWS) Xs[i * INV_COLS + col] = (c < n && __ldg(perm + i) == c) ? 1.0 : 0.0;
+  // forward with the unit lower factor, INV_ROWS rows per group
+  for (int i0 = 0; i0 < n; i0 += INV_ROWS) {
+    const int rows = min(INV_ROWS, n - i0), width = i0 + rows;
     __syncthreads();
-    for (int r = ty; r < LU_NB; r += 8) {
-      T[r][tx] = (r < nr && tx < nq) ? LU[(size_t)(r0 + r) * n + q0 + tx] : 0.0;
-      Xs[r][tx] = (r < nq && c < n) ? X[(size_t)(q0 + r) * n + c] : 0.0;
+    for (int r = warp; r < rows; r += nwarps)
+      for (int k = lane; k < width; k += 32) Rb[r * width + k] = __ldg(LU + (size_t)(i0 + r) * n + k);
+    __syncthreads();
+    double s = 0.0;
+    if (rr < rows) {
+      const double *Lr = Rb + rr * width;
+      double s1 = 0.0;
+      int k = 0;
+      for (; k + 2 <= i0; k += 2) {
+        s += Lr[k] * Xs[k * INV_COLS + col];
+        s1 += Lr[k + 1] * Xs[(k + 1) * INV_COLS + col];
+      }
+      if (k < i0) s += Lr[k] * Xs[k * INV_COLS + col];
+      s += s1;
     }
-    __syncthreads();
-    for (int r = ty; r < LU_NB; r += 8) {
-      double s = 0.0;
-#pragma unroll 8
-      for (int k = 0; k < LU_NB; k++) s += T[r][k] * Xs[k][tx];
-      B[r][tx] -= s;
+    for (int r = 0; r < rows; r++) {
+      if (rr == r) {
+        const double *Lr = Rb + r * width;
+        double t = Xs[(i0 + r) * INV_COLS + col] - s;
+        for (int k = i0; k < i0 + r; k++) t -= Lr[k] * Xs[k * INV_COLS + col];
+        Xs[(i0 + r) * INV_COLS + col] = t;
+      }
+      __syncthreads();
     }
   }
-  __syncthreads();
-  // diagonal block
-  for (int r = ty; r < LU_NB; r += 8) T[r][tx] = (r < nr && tx < nr) ? LU[(size_t)(r0 + r) * n + r0 + tx] : 0.0;
-  __syncthreads();
-  if (ty == 0) {
-    if (LOWER) {
-      for (int r = 1; r < nr; r++) {
-        double s = B[r][tx];
-        for (int k = 0; k < r; k++) s -= T[r][k] * B[k][tx];
-        B[r][tx] = s;
+  // backward with the upper factor, from the last rows
+  for (int i1 = n; i1 > 0; i1 -= INV_ROWS) {
+    const int lo = max(0, i1 - INV_ROWS), rows = i1 - lo, width = n - lo;
+    __syncthreads();
+    for (int r = warp; r < rows; r += nwarps)
+      for (int k = lane; k < width; k += 32) Rb[r * width + k] = __ldg(LU + (size_t)(lo + r) * n + lo + k);
+    __syncthreads();
+    const int i = i1 - 1 - rr;  // the row this thread sums for
+    double s = 0.0;
+    if (rr < rows) {
+      const double *Ur = Rb + (i - lo) * width - lo;  // Ur[k] = U[i][k] for k >= lo
+      double s1 = 0.0;
+      int k = i1;
+      for (; k + 2 <= n; k += 2) {
+        s += Ur[k] * Xs[k * INV_COLS + col];
+        s1 += Ur[k + 1] * Xs[(k + 1) * INV_COLS + col];
       }
-    } else {
-      for (int r = nr - 1; r >= 0; r--) {
-        double s = B[r][tx];
-        for (int k = r + 1; k < nr; k++) s -= T[r][k] * B[k][tx];
-        B[r][tx] = s / T[r][r];
+      if (k < n) s += Ur[k] * Xs[k * INV_COLS + col];
+      s += s1;
+    }
+    for (int r = 0; r < rows; r++) {
+      const int row = i1 - 1 - r;
+      if (rr == r) {
+        const double *Ur = Rb + (row - lo) * width - lo;
+        double t = Xs[row * INV_COLS + col] - s;
+        for (int k = row + 1; k < i1; k++) t -= Ur[k] * Xs[k * INV_COLS + col];
+        Xs[row * INV_COLS + col] = t / Ur[row];
       }
+      __syncthreads();
     }
   }
-  __syncthreads();
-  for (int r = ty; r < nr; r += 8)
-    if (c < n) X[(size_t)(r0 + r) * n + c] = B[r][tx];
+  if (c < n)
+    for (int i = rr; i < n; i += INV_ROWS) Inv[(size_t)i * n + c] = Xs[i * INV_COLS + col];
 }
 
-__global__ void k_csr_to_dense(int n, const int *__restrict__ rp, const int *__restrict__ kc, const double *__restrict__ a,
-                               double *D) {
-  int i = blockIdx.x;
-  if (i >= n) return;
-  for (int j = threadIdx.x; j < n; j += blockDim.x) D[(size_t)i * n + j] = 0.0;
-  __syncthreads();
-  for (int k = rp[i] + threadIdx.x; k < rp[i + 1]; k += blockDim.x) D[(size_t)i * n + kc[k]] = a[k];
-}
-
-// x = Inv f  (dense GEMV in FP64; f, x in T)
+// the coarsest level's rhs reduced to its active rows: t = f_a - A_ad f_d
+// (rows >= Na are Dirichlet: x_d = f_d); one warp per row
 template <typename T>
-__global__ void __launch_bounds__(256) k_dense_apply(int n, const double *__restrict__ Inv, const T *__restrict__ f, T *x) {
+__global__ void __launch_bounds__(256) k_coarse_rhs(int n, int na, const int *__restrict__ rp, const int *__restrict__ kc,
+                                                    const double *__restrict__ a, const T *__restrict__ f, double *t,
+                                                    T *x) {
   pdl_wait();
   pdl_trigger();
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= n) return;
+  if (warp >= na) {
+    if (lane == 0) x[warp] = f[warp];
+    return;
+  }
+  double s = 0.0;
+  for (int k = rp[warp] + lane; k < rp[warp + 1]; k += 32) {
+    const int j = kc[k];
+    if (j >= na) s += a[k] * (double)f[j];
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) t[warp] = (double)f[warp] - s;
+}
+
+// x_a = Inv t (dense GEMV in FP64 over the active rows; x in T)
+template <typename T>
+__global__ void __launch_bounds__(256) k_dense_apply(int na, const double *__restrict__ Inv, const double *__restrict__ t,
+                                                     T *x) {
+  pdl_wait();
+  pdl_trigger();
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= na) return;
   double s = 0;
-  for (int j = lane; j < n; j += 32) s += Inv[(size_t)warp * n + j] * (double)f[j];
+  for (int j = lane; j < na; j += 32) s += Inv[(size_t)warp * na + j] * t[j];
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if (lane == 0) x[warp] = (T)s;
 }
 
+// dense active block of the coarsest matrix (rows and columns < na)
+__global__ void k_csr_to_dense_active(int na, const int *__restrict__ rp, const int *__restrict__ kc,
+                                      const double *__restrict__ a, double *D) {
+  int i = blockIdx.x;
+  if (i >= na) return;
+  for (int j = threadIdx.x; j < na; j += blockDim.x) D[(size_t)i * na + j] = 0.0;
+  __syncthreads();
+  for (int k = rp[i] + threadIdx.x; k < rp[i + 1]; k += blockDim.x)
+    if (kc[k] < na) D[(size_t)i * na + kc[k]] = a[k];
+}
+
 int coarse_factor(Handle &h) {
   Level &L = h.lv[0];
-  const int n = L.N;
+  // Dirichlet rows are identity rows, so only the active block is factored:
+  // x_a = A_aa^{-1} (f_a - A_ad f_d), x_d = f_d
+  const int n = L.Na;
   if (n > LU_MAX_N) {
-    set_error("coarsest level too large for the dense direct solve (n > 832); use the SSOR coarse smoother");
+    set_error("coarsest level has too many active rows for the dense direct solve (> 832); use the SSOR coarse smoother");
     return PMG_ERR_UNSUPPORTED;
+  }
+  PMG_TRY(h.coarse_t.alloc(std::max(n, 1)));
+  if (n == 0) {
+    h.coarse_ready = true;
+    return PMG_OK;
   }
   PMG_TRY(h.coarse_lu.alloc((size_t)n * n));
   PMG_TRY(h.coarse_inv.alloc((size_t)n * n));
   PMG_TRY(h.coarse_piv.alloc(n));
   PMG_CUDA(cudaMemsetAsync(h.d_flags.p, 0, sizeof(int) * 4, h.stream));
-  k_csr_to_dense<<<n, 256, 0, h.stream>>>(n, L.rowptr.p, L.kcol.p, L.A.p, h.coarse_lu.p); count_launches(1);
+  k_csr_to_dense_active<<<n, 256, 0, h.stream>>>(n, L.rowptr.p, L.kcol.p, L.A.p, h.coarse_lu.p); count_launches(1);
   static bool attr = false;
   if (!attr) {
     PMG_CUDA(cudaFuncSetAttribute(k_lu_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, LU_MAX_N * (LU_NB + 1) * 8));
+    PMG_CUDA(cudaFuncSetAttribute(k_lu_inverse_slab, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  LU_MAX_N * 2 * INV_COLS * 8));
     attr = true;
   }
   for (int k0 = 0; k0 < n; k0 += LU_NB) {
@@ -271,17 +328,9 @@ int coarse_factor(Handle &h) {
   }
   PMG_TRY(h.coarse_perm.alloc(n));
   k_lu_perm_identity<<<1, 32, 0, h.stream>>>(n, h.coarse_piv.p, h.coarse_perm.p);
-  k_lu_fill_perm<<<n, 256, 0, h.stream>>>(n, h.coarse_perm.p, h.coarse_inv.p);
+  k_lu_inverse_slab<<<(n + INV_COLS - 1) / INV_COLS, INV_THREADS, (size_t)n * 2 * INV_COLS * 8, h.stream>>>(
+      n, h.coarse_lu.p, h.coarse_perm.p, h.coarse_inv.p);
   count_launches(2);
-  const int nblk = (n + LU_NB - 1) / LU_NB;
-  for (int ib = 0; ib < nblk; ib++) {
-    k_lu_inv_step<true><<<nblk, 256, 0, h.stream>>>(n, ib, h.coarse_lu.p, h.coarse_inv.p);
-    count_launches(1);
-  }
-  for (int ib = nblk - 1; ib >= 0; ib--) {
-    k_lu_inv_step<false><<<nblk, 256, 0, h.stream>>>(n, ib, h.coarse_lu.p, h.coarse_inv.p);
-    count_launches(1);
-  }
   PMG_CUDA(cudaGetLastError());
   int flags[4];
   PMG_CUDA(cudaMemcpyAsync(flags, h.d_flags.p, sizeof(flags), cudaMemcpyDeviceToHost, h.stream));
@@ -332,9 +381,15 @@ static int vcycle(Handle &h, int i, bool learned) {
   if (!learned && i >= 1 && i == h.cc_top) return coarse_cycle<T>(h, i);
   if (i == 0) {
     if (h.prm.coarse_smoother == PMG_COARSE_DIRECT) {
-      PMG_CUDA(launch_pdl(k_dense_apply<T>, dim3((L.N * 32 + 255) / 256), dim3(256), 0, s, L.N,
-                          (const double *)h.coarse_inv.p, (const T *)PT::f(L), PT::x(L)));
+      PMG_CUDA(launch_pdl(k_coarse_rhs<T>, dim3((L.N * 32 + 255) / 256), dim3(256), 0, s, L.N, L.Na,
+                          (const int *)L.rowptr.p, (const int *)L.kcol.p, (const double *)L.A.p, (const T *)PT::f(L),
+                          h.coarse_t.p, PT::x(L)));
       count_launches(1);
+      if (L.Na > 0) {
+        PMG_CUDA(launch_pdl(k_dense_apply<T>, dim3((L.Na * 32 + 255) / 256), dim3(256), 0, s, L.Na,
+                            (const double *)h.coarse_inv.p, (const double *)h.coarse_t.p, PT::x(L)));
+        count_launches(1);
+      }
       PMG_CUDA(cudaGetLastError());
     } else {
       int it = h.prm.coarse_maxit > 0 ? h.prm.coarse_maxit : 1;
@@ -495,6 +550,8 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
   PMG_CUDA(cudaEventRecord(h.ev[2], h.stream));
   PMG_TRY(prepare_levels(h));
   PMG_TRY(capture_vcycle(h));
+  PMG_CUDA(cudaEventRecord(h.ev[6], h.stream));  // end of the per-solve set-up
+  bool vc_timed = false;
   Level &F = h.lv.back();
   const size_t N = F.N;
   const int m = h.prm.restart > 0 ? h.prm.restart : 10;
@@ -557,7 +614,12 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
     bool done = false;
     for (i = 0; i < m && j <= maxit; i++, j++) {
       double *vi = V + (size_t)i * N, *zi = Z + (size_t)i * N;
+      if (!vc_timed) PMG_CUDA(cudaEventRecord(h.ev[7], s));
       PMG_TRY(precondition(h, vi, zi, guard_phase == 1));
+      if (!vc_timed) {
+        PMG_CUDA(cudaEventRecord(h.ev[8], s));
+        vc_timed = true;
+      }
       PMG_TRY(sell_spmv<double>(s, F, zi, nullptr, w, 0, h.num_sms));
       double *Hc = Hd + (size_t)i * (m + 1);
       for (int k = 0; k <= i; k++) {
@@ -638,6 +700,10 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
     st->mean_contraction = (iters > 0 && res0 > 0 && res_final > 0) ? pow(res_final / res0, 1.0 / iters) : 0.0;
     st->smoother_used = (learned && guard_phase == 1) ? PMG_SMOOTHER_LEARNED : PMG_SMOOTHER_SSOR;
     st->seconds = h.t_solve;
+    float a = 0, b = 0;
+    st->setup_seconds = cudaEventElapsedTime(&a, h.ev[2], h.ev[6]) == cudaSuccess ? a * 1e-3 : 0.0;
+    st->vcycle_seconds = (vc_timed && cudaEventElapsedTime(&b, h.ev[7], h.ev[8]) == cudaSuccess) ? b * 1e-3 : 0.0;
+    cudaGetLastError();
   }
   return status;
 }
