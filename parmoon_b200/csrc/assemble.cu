@@ -456,28 +456,55 @@ __global__ void __launch_bounds__(ASMC_WARPS * 32, 2) k_assemble_cc(AsmArgs a, c
 #pragma unroll
       for (int k = 0; k < 16; k++) Dr[p][k] = W[p * WE + k];
     int bad = 0;
-    for (int m = lane; m < NN; m += 32) {
-      double acc[P];
+    // MB entries per lane per batch: all slot and entry loads of a batch are
+    // issued before any arithmetic, so each lane keeps 2 MB P reads in flight
+    constexpr int MB = 4;
+    const int ne = min(P, a.n_elems - base);
+    for (int m0 = lane; m0 < NN; m0 += 32 * MB) {
+      int sl[MB][P];
+      double old[MB][P];
 #pragma unroll
-      for (int p = 0; p < P; p++) acc[p] = 0.0;
+      for (int b = 0; b < MB; b++) {
+        const int m = m0 + 32 * b;
 #pragma unroll
-      for (int ab = 0; ab < 16; ab++) {
-        const double sv = sS[ab * NN + m];
-#pragma unroll
-        for (int p = 0; p < P; p++) acc[p] += Dr[p][ab] * sv;
+        for (int p = 0; p < P; p++) {
+          sl[b][p] = -2;  // no entry
+          if (m < NN && p < ne) {
+            const int e = base + p;
+            const int i = m / NLOC;
+            const int di = __ldg(a.elem_dof + (size_t)e * NLOC + i);
+            const int s = __ldg(a.slot + (size_t)e * NN + m);
+            if (di < a.Na) {
+              if (s >= 0) sl[b][p] = s;
+              else bad = 1;
+            } else if (i == m - i * NLOC && s >= 0) {
+              sl[b][p] = -3 - s;  // Dirichlet diagonal
+            }
+          }
+        }
       }
-      const int i = m / NLOC, j = m - i * NLOC;
 #pragma unroll
-      for (int p = 0; p < P; p++) {
-        const int e = base + p;
-        if (e >= a.n_elems) break;
-        const int di = __ldg(a.elem_dof + (size_t)e * NLOC + i);
-        const int sl = __ldg(a.slot + (size_t)e * NN + m);
-        if (di < a.Na) {
-          if (sl >= 0) a.entries[sl] += acc[p];
-          else bad = 1;
-        } else if (i == j && sl >= 0) {
-          a.entries[sl] = 1.0;  // Dirichlet row: unit diagonal (AssembleMat3D.C:840-848)
+      for (int b = 0; b < MB; b++)
+#pragma unroll
+        for (int p = 0; p < P; p++) old[b][p] = sl[b][p] >= 0 ? a.entries[sl[b][p]] : 0.0;
+#pragma unroll
+      for (int b = 0; b < MB; b++) {
+        const int m = m0 + 32 * b;
+        if (m >= NN) break;
+        double acc[P];
+#pragma unroll
+        for (int p = 0; p < P; p++) acc[p] = 0.0;
+#pragma unroll
+        for (int ab = 0; ab < 16; ab++) {
+          const double sv = sS[ab * NN + m];
+#pragma unroll
+          for (int p = 0; p < P; p++) acc[p] += Dr[p][ab] * sv;
+        }
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+          const int q = sl[b][p];
+          if (q >= 0) a.entries[q] = old[b][p] + acc[p];
+          else if (q <= -3) a.entries[-3 - q] = 1.0;  // Dirichlet row: unit diagonal (AssembleMat3D.C:840-848)
         }
       }
     }
