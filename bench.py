@@ -306,6 +306,100 @@ def bench_ours(args, rank, world, dist):
     h.close()
 
 
+def config_line(name, extra):
+    line = {"metric": METRIC, "impl": "ours", "config_name": name, "n_gpus": 1, "dtype": "f64+f32",
+            "data": "synthetic", "higher_is_better": False, "unit": "s"}
+    line.update(extra)
+    print(json.dumps(line))
+
+
+def run_config(name, steps):
+    """The other workloads of the benchmark suite, one JSON line each (not the
+    driver's bench line): device times of assembly and solve, FP32 V-cycle vs
+    plain FP64 GMG, FP64 true residual."""
+    import parmoon_b200 as P
+    from parmoon_b200.configs import lognormal_modes
+    if name == "poisson_q1_32":
+        # Poisson Q1 32^3 (35,937 dofs), sine rhs, homogeneous Dirichlet, Gauss2, 4 levels, SSOR(2,2) FGMRES
+        levels = P.struct_hierarchy(P.Q1_HEX, 32, 4)
+        mk = lambda prec: P.default_params(precision=prec)
+        coef = P.coeff(kind=P.COEF_SINE_RHS, eps=1.0)
+        form, dirv, nl = P.FORM_GALERKIN, None, 4
+    elif name == "p2tet_lognormal_64":
+        # P2 tetrahedra: 64^3 hexahedra x 6 Kuhn tetrahedra (1,572,864 cells, 2,146,689 dofs), interior
+        # vertices jittered by up to 0.2 h, lognormal diffusion (sigma 1, correlation 0.1), b = 0, f = 1, Keast-11
+        levels = P.struct_hierarchy(P.P2_TET, 64, 5, jitter=0.2, seed=1)
+        mk = lambda prec: P.default_params(precision=prec)
+        coef = P.coeff(kind=P.COEF_LOGNORMAL, eps=1.0, f=1.0, modes=lognormal_modes(1))
+        form, dirv, nl = P.FORM_GALERKIN, None, 5
+    else:
+        raise ValueError(name)
+    h = P.Handle(nl, mk(P.PREC_FP32))
+    h.set_coefficients(coef)
+    P.load_hierarchy(h, levels, dirichlet=dirv)
+    out = {}
+    for prec, tag in ((P.PREC_FP32, "fp32"), (P.PREC_FP64, "fp64")):
+        h.set_params(mk(prec))
+        ta, ts, its, rel = [], [], 0, 0.0
+        for k in range(steps + 2):
+            h.assemble(-1, form, copy_out=False)
+            t_asm = h.timings()[0]
+            _, st, rc = h.solve()
+            if rc != 0:
+                raise RuntimeError(f"{name}: solve status {rc}")
+            if k >= 2:
+                ta.append(t_asm)
+                ts.append(st.seconds)
+            its, rel = st.iterations, st.rel_res
+        out[tag] = {"assembly_s": statistics.mean(ta), "solve_s": statistics.mean(ts), "iterations": its,
+                    "rel_res_fp64": rel}
+    F = levels[-1]
+    config_line(name, {"value": out["fp32"]["assembly_s"] + out["fp32"]["solve_s"], "steps": steps,
+                       "n_dofs": int(F["N"]), "nnz_fine": int(F["rowptr"][-1]), "levels": nl, **out})
+    h.close()
+
+
+def run_tcd(steps):
+    """Time-dependent CD (TCD3D): Q1 128^3 (2,146,689 dofs, 5 levels), Crank-Nicolson, tau = 1e-3,
+    eps = 1e-4, rotating convection b = (-(y-.5), x-.5, 0.2 sin 2 pi t), Gaussian bump (sigma 0.05 at
+    (0.3, 0.5, 0.5)) as initial value, mass and SUPG stiffness reassembled on every level every step,
+    FP32 V-cycle in FP64 FGMRES: device time per time step."""
+    import parmoon_b200 as P
+    nl, tau = 5, 1e-3
+    levels = P.struct_hierarchy(P.Q1_HEX, 128, nl)
+    h = P.Handle(nl, P.default_params(precision=P.PREC_FP32))
+    P.load_hierarchy(h, levels)
+    F = levels[-1]
+    x = F["dof_xyz"]
+    u = np.exp(-((x[:, 0] - 0.3) ** 2 + (x[:, 1] - 0.5) ** 2 + (x[:, 2] - 0.5) ** 2) / (2 * 0.05 ** 2))
+    u[F["active_bound"]:] = 0.0
+    theta = (0.5, 0.5, 0.5, 0.5)  # Crank-Nicolson (TimeDiscRout.C: THETA1..4)
+    t = 0.0
+    h.set_coefficients(P.coeff(kind=P.COEF_ROTATING, eps=1e-4, f=0.0, t=t))
+    h.assemble(-1, P.FORM_MASS_SUPG, copy_out=False)
+    times, its = [], []
+    for k in range(steps + 2):
+        t += tau
+        h.set_coefficients(P.coeff(kind=P.COEF_ROTATING, eps=1e-4, f=0.0, t=t))
+        h.assemble(-1, P.FORM_MASS_SUPG, copy_out=False)
+        t_m = h.timings()[0]
+        h.assemble(-1, P.FORM_SUPG, copy_out=False)
+        t_a = h.timings()[0]
+        h.tcd_system(tau, theta, u_old=u if k == 0 else None)
+        _, st, rc = h.solve()
+        h.tcd_restore()
+        if rc != 0:
+            raise RuntimeError(f"tcd: solve status {rc}")
+        if k >= 2:
+            times.append(t_m + t_a + st.seconds)
+            its.append(st.iterations)
+    config_line("tcd_q1_128_cn", {"value": statistics.mean(times), "unit": "s per time step", "steps": steps,
+                                  "n_dofs": int(F["N"]), "nnz_fine": int(F["rowptr"][-1]), "levels": nl,
+                                  "iterations_mean": float(np.mean(its)),
+                                  "projected_200_steps_s": 200 * statistics.mean(times)})
+    h.close()
+
+
 KERNELS = {"spmv64": 0, "spmv32": 1, "ssor64": 2, "ssor32": 3, "assemble": 4, "coarse_factor": 6}
 
 
@@ -344,12 +438,20 @@ def main():
     ap.add_argument("--levels", type=int, default=5)
     ap.add_argument("--profile-kernel", choices=sorted(KERNELS), default=None,
                     help="time one kernel on the finest level only (the profiling command)")
+    ap.add_argument("--config", choices=["poisson_q1_32", "p2tet_lognormal_64", "tcd_q1_128_cn"], default=None,
+                    help="run one of the other workloads instead of the bench line")
     args = ap.parse_args()
     global N_CELLS, N_LEVELS, N_FULL
     N_CELLS, N_LEVELS = args.n_cells, args.levels
     N_FULL = (2 * N_CELLS + 1) ** 3
     if args.profile_kernel:
         profile_kernel(args.profile_kernel)
+        return
+    if args.config == "tcd_q1_128_cn":
+        run_tcd(args.steps)
+        return
+    if args.config:
+        run_config(args.config, args.steps)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
