@@ -45,6 +45,11 @@ REF_SAMPLE = dict(order=2, levels=4, coarse_steps=2, problem="cdsupg", eps=EPS, 
                   dump=0, transfer=0, restart=20, red=1e-10)
 N_FULL = (2 * N_CELLS + 1) ** 3
 N_SAMPLE = (2 * 32 + 1) ** 3
+# DRAM traffic of one FP32 SSOR step per algorithmic byte, measured with ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum over the 54 colour launches of
+# one step on the finest level of the 48^3 Q2 hierarchy: 1.103 GB for 0.901 GB
+# algorithmic); the step's traffic scales with the rows and entries it sweeps
+SSOR_TRAFFIC_PER_BYTE = 1.103201 / 0.901129
 
 
 def peaks():
@@ -291,7 +296,8 @@ def bench_ours(args, rank, world, dist):
             "wall_s_per_step": t_wall / args.steps,
             "roofline": {"bound": "hbm", "kernel": "k_sell_gs<float,K> (FP32 multicolour SSOR step on SELL-32, finest level)",
                          "achieved": ssor["gbs"], "peak": hbm, "unit": "GB/s", "frac": ssor["gbs"] / hbm,
-                         "traffic": None, "peak_kind": peak_kind, "bytes_per_launch": ssor["bytes"],
+                         "traffic": ssor["bytes"] * SSOR_TRAFFIC_PER_BYTE,
+                         "traffic_note": "ncu DRAM bytes of one SSOR step at 48^3, scaled by the algorithmic bytes", "peak_kind": peak_kind, "bytes_per_launch": ssor["bytes"],
                          "launch_s": ssor["seconds"]},
             "roofline_spmv64": {"achieved": spmv64["gbs"], "frac": spmv64["gbs"] / hbm, "bytes": spmv64["bytes"]},
             "roofline_spmv32": {"achieved": spmv32["gbs"], "frac": spmv32["gbs"] / hbm, "bytes": spmv32["bytes"]},
