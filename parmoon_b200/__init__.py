@@ -20,6 +20,8 @@ LIB_PATH = os.path.join(HERE, "libpmg_b200.so")
 OK = 0
 ERR = {-1: "ARG", -2: "CUDA", -3: "STATE", -4: "NOT_CONVERGED", -5: "DIVERGED", -6: "SLOT",
        -7: "NONFINITE", -8: "SINGULAR", -9: "UNSUPPORTED"}
+(ERR_ARG, ERR_CUDA, ERR_STATE, ERR_NOT_CONVERGED, ERR_DIVERGED, ERR_SLOT, ERR_NONFINITE, ERR_SINGULAR,
+ ERR_UNSUPPORTED) = range(-1, -10, -1)
 Q1_HEX, Q2_HEX, P1_TET, P2_TET = 1, 2, 11, 12
 FORM_GALERKIN, FORM_SUPG, FORM_MASS, FORM_MASS_SUPG, FORM_STIFF_SUPG = 1, 2, 3, 4, 5
 COEF_CONST, COEF_SINE_RHS, COEF_LOGNORMAL, COEF_CURL_FOURIER, COEF_ROTATING, COEF_AMC, COEF_TABLE = range(7)

@@ -379,6 +379,8 @@ int pmg_set_dirichlet_values(pmg_handle hh, int level, const double *values) {
   int n = L.N - L.Na;
   if (n > 0) {
     if (!values) { set_error("pmg_set_dirichlet_values: null values"); return PMG_ERR_ARG; }
+    for (int k = 0; k < n; k++)
+      if (!std::isfinite(values[k])) { set_error("pmg_set_dirichlet_values: non-finite value"); return PMG_ERR_NONFINITE; }
     PMG_TRY(L.dirval.upload(values, n, h->stream));
     PMG_CUDA(cudaStreamSynchronize(h->stream));
   }

@@ -156,3 +156,13 @@ def test_nested_prolongation_equals_lattice_interpolation():
         srp, scol, sval = P.struct_prolongation(elem, 2, C["dof_lat"], F["dof_lat"])
         assert np.array_equal(rp, srp) and np.array_equal(col, scol)
         assert np.max(np.abs(val - sval)) < 1e-14
+
+
+def test_create_rejects_bad_level_counts():
+    """pmg_create checks its arguments before it looks for a device."""
+    import ctypes
+    import parmoon_b200 as P
+    h = ctypes.c_void_p()
+    p = P.default_params()
+    for n in (0, -1, 17):
+        assert P.lib().pmg_create(ctypes.byref(h), n, ctypes.byref(p)) == P.ERR_ARG
