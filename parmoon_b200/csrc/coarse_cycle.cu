@@ -22,7 +22,9 @@
 // partial sums inside a row.
 #include "pmg_internal.h"
 #include <cooperative_groups.h>
+#include <algorithm>
 #include <cstdlib>
+#include <string>
 
 namespace cg = cooperative_groups;
 
@@ -91,23 +93,32 @@ __device__ void cc_slices(CcCtx<T> &c, const CcLevel<T> &L, int s0, int s1, T om
       const T *vp = L.val + off + c.lane;
       int ci[PF];
       T cv[PF];
+      // column steps in chunks of PF: loads of a chunk, then its gathers
+      for (int c0 = 0; k + c0 * K < lmax; c0 += PF) {
 #pragma unroll
-      for (int u = 0; u < PF; u++) {
-        const int j = k + u * K;
-        ci[u] = j < lmax ? __ldg(cp + 32 * j) : -1;
-        cv[u] = j < lmax ? __ldg(vp + 32 * j) : (T)0;
+        for (int u = 0; u < PF; u++) {
+          const int j = k + (c0 + u) * K;
+          ci[u] = j < lmax ? __ldg(cp + 32 * j) : -1;
+          cv[u] = j < lmax ? __ldg(vp + 32 * j) : (T)0;
+        }
+        if (c0 == 0 && k == 0) {
+          row = __ldg(L.perm + sl * 32 + c.lane);
+          if (row >= 0) {
+            fr = __ldcg(L.f + row);
+            if (GS) id = __ldg(L.invd + sl * 32 + c.lane);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < PF; u++)
+          if (ci[u] >= 0) sum += cv[u] * x[ci[u]];
       }
-      if (k == 0) {
+      if (k == 0 && lmax == 0) {
         row = __ldg(L.perm + sl * 32 + c.lane);
         if (row >= 0) {
           fr = __ldcg(L.f + row);
           if (GS) id = __ldg(L.invd + sl * 32 + c.lane);
         }
       }
-#pragma unroll
-      for (int u = 0; u < PF; u++)
-        if (ci[u] >= 0) sum += cv[u] * x[ci[u]];
-      for (int j = k + PF * K; j < lmax; j += K) sum += __ldg(vp + 32 * j) * x[__ldg(cp + 32 * j)];
     }
     c.part[c.warp][c.lane] = sum;
     __syncthreads();
@@ -275,17 +286,20 @@ static int cluster_ctas() {
 
 // the highest level that, with every level below it, fits the cluster launch
 // (0: none -- the level-by-level path runs)
-int coarse_cycle_top(const Handle &h) {
-  static int on = -1;
-  if (on < 0) {
-    // opt-in (PMG_COARSE_CLUSTER=1): on the 64^3 Q2 hierarchy a colour pass
-    // of this launch (loads, gathers, broadcast stores, cluster barrier)
-    // measured ~7 us against ~4.4 us for a PDL-chained colour launch
+// levels 0..top in one launch, opt-in: PMG_COARSE_CLUSTER=1 runs the levels
+// of at most CC_ONE_CTA_ROWS rows on one CTA, PMG_COARSE_CLUSTER=16 every
+// level whose iterates fit CC_SMEM_X on a 16-CTA cluster.  Both measured
+// slower than the PDL-chained colour launches on the 64^3 Q2 hierarchy (a
+// colour pass here ~5 us), so the default is the level-by-level path.
+constexpr int CC_ONE_CTA_ROWS = 8192;
+
+int coarse_cycle_top(Handle &h) {
+  static int mode = -1;
+  if (mode < 0) {
     const char *e = getenv("PMG_COARSE_CLUSTER");
-    on = (e && e[0] == '1') ? 1 : 0;
+    mode = !e ? 0 : (std::string(e) == "1") ? 1 : (std::string(e) == "16") ? 2 : 0;
   }
-  if (!on) return 0;
-  // levels from the coarsest up while their iterates fit the shared-memory budget
+  if (mode == 0) return 0;
   const size_t vb = h.prm.precision == PMG_PREC_FP32 ? sizeof(float) : sizeof(double);
   size_t bytes = 0;
   int top = 0;
@@ -293,10 +307,18 @@ int coarse_cycle_top(const Handle &h) {
     const Level &L = h.lv[i];
     bytes += ((size_t)L.N * vb + 15) / 16 * 16;
     if (bytes > CC_SMEM_X || (int)L.sell_group.size() > CC_MAX_GROUPS) break;
+    if (mode == 1 && L.N > CC_ONE_CTA_ROWS) break;
     top = i;
   }
-  // the launch shape is queried here, outside any stream capture
-  if (top >= 1 && (!cluster_ctas<float>() || !cluster_ctas<double>())) return 0;
+  if (top < 1) return 0;
+  if (mode == 1) {
+    h.cc_ctas = 1;
+  } else {
+    // the launch shape is queried here, outside any stream capture
+    const int c = std::min(cluster_ctas<float>(), cluster_ctas<double>());
+    if (!c) return 0;
+    h.cc_ctas = c;
+  }
   return top;
 }
 
@@ -345,10 +367,17 @@ int coarse_cycle(Handle &h, int top) {
   a.post = h.prm.post_smooth;
   a.omega = (T)h.prm.smooth_omega;
   a.damp = (T)h.prm.gmg_damp;
-  const int ctas = cluster_ctas<T>();
-  if (!ctas) {
-    set_error("coarse_cycle: no thread-block cluster of 4 or more CTAs can be scheduled");
-    return PMG_ERR_UNSUPPORTED;
+  const int ctas = h.cc_ctas;
+  if (ctas < 1) {
+    set_error("coarse_cycle: launch shape not set");
+    return PMG_ERR_STATE;
+  }
+  if (ctas == 1) {
+    static bool attr = false;
+    if (!attr) {
+      PMG_CUDA(cudaFuncSetAttribute(k_coarse_cycle<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CC_SMEM_X));
+      attr = true;
+    }
   }
   if (smem > CC_SMEM_X) {
     set_error("coarse_cycle: iterates exceed the shared-memory budget");

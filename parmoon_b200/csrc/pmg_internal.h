@@ -192,7 +192,8 @@ struct Handle {
   int vgraph_prec = -1;
   unsigned long long vgraph_kernels = 0;
   bool use_graph = true;  // PMG_NO_GRAPH=1 launches the V-cycle kernels directly (profilers)
-  int cc_top = 0;         // levels 0..cc_top run as one cluster launch (0: none)
+  int cc_top = 0;         // levels 0..cc_top run as one launch (0: none)
+  int cc_ctas = 0;        // CTAs of that launch (1, or a cluster of up to 16)
   // learned smoother: BF16 weights used by the kernels, FP32 master copy, Adam state
   DBuf<uint16_t> lw_bf16;
   DBuf<float> lw_master, lw_grad, lw_m, lw_v;
@@ -260,7 +261,7 @@ int learned_smooth(cudaStream_t s, const Level &L, const T *r, T *x, double omeg
 void invalidate_graphs(Handle *h);
 
 // the coarse end of the V-cycle in one thread-block-cluster launch (coarse_cycle.cu)
-int coarse_cycle_top(const Handle &h);
+int coarse_cycle_top(Handle &h);
 template <typename T>
 int coarse_cycle(Handle &h, int top);
 

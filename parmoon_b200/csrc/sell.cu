@@ -180,17 +180,17 @@ __global__ void __launch_bounds__(32 * K) k_sell_mv(int s0, int s1, const int *_
 }
 
 // Gauss-Seidel update of the rows of one colour (slices [s0, s1)).
-// The first GS_PF column steps of a warp's slice are loaded before
+// The first chunk of column steps of a warp's slice is loaded before
 // pdl_wait(): the predecessor in the stream (the previous colour, a transfer
 // or a defect) writes vectors only, never the matrix, so the colour's matrix
 // streams in while the predecessor drains, and only the x gathers wait.
-constexpr int GS_PF = 16;
 
 template <typename T, int K>
 __global__ void __launch_bounds__(32 * K) k_sell_gs(int s0, int s1, const int *__restrict__ perm,
                                                     const int *__restrict__ sptr, const int *__restrict__ col,
                                                     const T *__restrict__ val, const T *__restrict__ invd,
                                                     const T *__restrict__ f, T *x, T omega) {
+  constexpr int GS_PF = sizeof(T) == 4 ? 16 : 8;  // column steps per chunk (registers)
   __shared__ T part[K][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int s = s0 + blockIdx.x;
@@ -213,13 +213,21 @@ __global__ void __launch_bounds__(32 * K) k_sell_gs(int s0, int s1, const int *_
   pdl_trigger();
   for (; s < s1; s += gridDim.x) {
     T sum = 0;
+    // column steps in chunks of GS_PF: the gathers of a chunk go out, then the
+    // next chunk's column / value loads, so a long row costs one latency per chunk
+    for (int c0 = 0;; c0 += GS_PF) {
 #pragma unroll
-    for (int u = 0; u < GS_PF; u++)
-      if (w + u * K < lmax) sum += cv[u] * x[ci[u]];
-    const int *c = col + off + lane;
-    const T *v = val + off + lane;
-#pragma unroll 4
-    for (int j = w + GS_PF * K; j < lmax; j += K) sum += __ldg(v + 32 * j) * x[__ldg(c + 32 * j)];
+      for (int u = 0; u < GS_PF; u++)
+        if (w + (c0 + u) * K < lmax) sum += cv[u] * x[ci[u]];
+      if (w + (c0 + GS_PF) * K >= lmax) break;
+#pragma unroll
+      for (int u = 0; u < GS_PF; u++) {
+        const int j = w + (c0 + GS_PF + u) * K;
+        const bool in = j < lmax;
+        ci[u] = in ? __ldg(col + off + 32 * j + lane) : 0;
+        cv[u] = in ? __ldg(val + off + 32 * j + lane) : (T)0;
+      }
+    }
     part[w][lane] = sum;
     __syncthreads();
     if (w == 0) {

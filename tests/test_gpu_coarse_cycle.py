@@ -1,10 +1,10 @@
-"""The coarse end of the V-cycle as one thread-block-cluster launch gives the
-same solve as the level-by-level launches: same
+"""The coarse end of the V-cycle as one launch (opt-in: one CTA for the
+smallest levels, PMG_COARSE_CLUSTER=1, or a 16-CTA thread-block cluster,
+PMG_COARSE_CLUSTER=16) gives the same solve as the level-by-level launches: same
 FGMRES iteration count (+-1) and solutions within 1e-8 relative (both stop at
 |r| <= 1e-10 |r0|; the two paths differ only in the order of partial sums
-inside a row).  The cluster launch is opt-in (PMG_COARSE_CLUSTER=1); each
-configuration runs in its own process because the switch is read once per
-process."""
+inside a row).  Each configuration runs in its own process because the switch
+is read once per process."""
 import json
 import os
 import subprocess
@@ -34,22 +34,25 @@ print(json.dumps(dict(rc=rc, its=st.iterations, rel=st.rel_res)))
 """
 
 
-def run(tmp_path, tag, args, cluster):
+def run(tmp_path, tag, args, mode):
     out = str(tmp_path / f"{tag}.npy")
     env = dict(os.environ)
-    env["PMG_COARSE_CLUSTER"] = "1" if cluster else "0"
+    env.pop("PMG_COARSE_CLUSTER", None)
+    if mode is not None:
+        env["PMG_COARSE_CLUSTER"] = mode
     p = subprocess.run([sys.executable, "-c", SCRIPT.format(root=ROOT, args=args, out=out)], env=env,
                        capture_output=True, text=True, timeout=600)
     assert p.returncode == 0, p.stderr[-3000:]
     return json.loads(p.stdout.strip().splitlines()[-1]), np.load(out)
 
 
+@pytest.mark.parametrize("mode", ["1", "16"])  # one CTA, 16-CTA cluster
 @pytest.mark.parametrize("elem,n,nl,prec,coarse", [(2, 16, 3, 1, 17), (1, 32, 4, 1, 17), (1, 32, 4, 0, 17),
                                                    (2, 16, 3, 0, 3)])
-def test_cluster_coarse_cycle_matches_level_launches(tmp_path, elem, n, nl, prec, coarse):
+def test_coarse_cycle_launch_matches_level_launches(tmp_path, elem, n, nl, prec, coarse, mode):
     args = (elem, n, nl, prec, coarse)
-    a, xa = run(tmp_path, "cluster", args, True)
-    b, xb = run(tmp_path, "levels", args, False)
+    a, xa = run(tmp_path, "one", args, mode)
+    b, xb = run(tmp_path, "levels", args, None)
     assert a["rc"] == 0 and b["rc"] == 0 and a["rel"] <= 1e-10 and b["rel"] <= 1e-10
     assert abs(a["its"] - b["its"]) <= 1, (a, b)
     assert np.linalg.norm(xa - xb) <= 1e-8 * np.linalg.norm(xb)
