@@ -156,23 +156,52 @@ __global__ void __launch_bounds__(32 * K) k_sell_mv(int s0, int s1, const int *_
                                                     const int *__restrict__ sptr, const int *__restrict__ col,
                                                     const T *__restrict__ val, const T *__restrict__ x,
                                                     const T *__restrict__ f, T *__restrict__ y) {
+  constexpr int PF = sizeof(T) == 4 ? 16 : 8;  // column steps per chunk
   __shared__ T part[K][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int s = s0 + blockIdx.x;
+  int off = 0, lmax = 0;
+  int ci[PF];
+  T cv[PF];
+  auto load_chunk = [&](int c0) {
+#pragma unroll
+    for (int u = 0; u < PF; u++) {
+      const int j = w + (c0 + u) * K;
+      const bool in = j < lmax;
+      ci[u] = in ? __ldg(col + off + 32 * j + lane) : 0;
+      cv[u] = in ? __ldg(val + off + 32 * j + lane) : (T)0;
+    }
+  };
+  // the matrix is not written by the predecessor: its first chunk streams in while that drains
+  if (s < s1) {
+    off = __ldg(sptr + s);
+    lmax = (__ldg(sptr + s + 1) - off) >> 5;
+    load_chunk(0);
+  }
   pdl_wait();
   pdl_trigger();
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int s = s0 + blockIdx.x; s < s1; s += gridDim.x) {
-    const int off = __ldg(sptr + s), lmax = (__ldg(sptr + s + 1) - off) >> 5;
-    const int *c = col + off + lane;
-    const T *v = val + off + lane;
+  for (; s < s1; s += gridDim.x) {
     T sum = 0;
-#pragma unroll 4
-    for (int j = w; j < lmax; j += K) sum += __ldg(v + 32 * j) * __ldg(x + __ldg(c + 32 * j));
+    for (int c0 = 0;; c0 += PF) {
+#pragma unroll
+      for (int u = 0; u < PF; u++)
+        if (w + (c0 + u) * K < lmax) sum += cv[u] * __ldg(x + ci[u]);
+      if (w + (c0 + PF) * K >= lmax) break;
+      load_chunk(c0 + PF);
+    }
     part[w][lane] = sum;
+    const int sn = s + gridDim.x;
+    const int r = w == 0 ? __ldg(perm + s * 32 + lane) : -1;
+    if (sn < s1) {
+      // next slice's first chunk before the reduction
+      off = __ldg(sptr + sn);
+      lmax = (__ldg(sptr + sn + 1) - off) >> 5;
+      load_chunk(0);
+    }
     __syncthreads();
     if (w == 0) {
 #pragma unroll
       for (int k = 1; k < K; k++) sum += part[k][lane];
-      const int r = __ldg(perm + s * 32 + lane);
       if (r >= 0) y[r] = MODE ? __ldg(f + r) - sum : sum;
     }
     __syncthreads();
