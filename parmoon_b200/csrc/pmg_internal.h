@@ -223,7 +223,7 @@ int defect(cudaStream_t s, const Level &L, const T *A, const T *x, const T *f, T
 template <typename T>
 int ssor_sweep(cudaStream_t s, const Level &L, const T *A, const T *invdiag, const T *f, T *x, double omega);
 template <typename T>
-int restrict_defect(cudaStream_t s, const Level &Lf, const Level &Lc, const T *rval, const T *d, T *fc);
+int restrict_defect(cudaStream_t s, const Level &Lf, const Level &Lc, const T *rval, const T *d, T *fc, T *xc = nullptr);
 template <typename T>
 int prolongate_add(cudaStream_t s, const Level &Lf, const T *pval, const T *xc, T *xf, double damp);
 int compute_invdiag(cudaStream_t s, Level &L);
@@ -245,7 +245,7 @@ int sell_values(Handle &h, Level &L);
 template <typename T>
 int sell_spmv(cudaStream_t s, const Level &L, const T *x, const T *f, T *y, int mode, int num_sms);
 template <typename T>
-int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, int num_sms);
+int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, int num_sms, bool dirichlet = true);
 
 // ------------------------------------------------------------- solver (solver.cu)
 int coarse_factor(Handle &h);

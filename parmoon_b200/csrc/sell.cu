@@ -334,12 +334,13 @@ int sell_spmv(cudaStream_t s, const Level &L, const T *x, const T *f, T *y, int 
 template int sell_spmv<float>(cudaStream_t, const Level &, const float *, const float *, float *, int, int);
 template int sell_spmv<double>(cudaStream_t, const Level &, const double *, const double *, double *, int, int);
 
-// one SSOR step: Dirichlet rows from f, forward over the colours, backward
+// one SSOR step: Dirichlet rows from f (the sweeps never change them, so only the
+// first step of a level visit needs it), forward over the colours, backward
 template <typename T>
-int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, int num_sms) {
+int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, int num_sms, bool dirichlet) {
   const int nc = (int)L.sell_group.size() - 2;  // active colours
   const int nd = L.N - L.Na;
-  if (nd > 0) {
+  if (nd > 0 && dirichlet) {
     PMG_CUDA(launch_pdl(k_sell_copy_dirichlet<T>, dim3((nd + 255) / 256), dim3(256), 0, s, L.Na, L.N, f, x));
     count_launches(1);
   }
@@ -362,7 +363,7 @@ int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, in
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
-template int sell_ssor<float>(cudaStream_t, const Level &, const float *, float *, double, int);
-template int sell_ssor<double>(cudaStream_t, const Level &, const double *, double *, double, int);
+template int sell_ssor<float>(cudaStream_t, const Level &, const float *, float *, double, int, bool);
+template int sell_ssor<double>(cudaStream_t, const Level &, const double *, double *, double, int, bool);
 
 }  // namespace pmg

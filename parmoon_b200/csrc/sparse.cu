@@ -140,7 +140,8 @@ template int ssor_sweep<float>(cudaStream_t, const Level &, const float *, const
 // ----------------------------------------------------------------- transfers
 template <int W, typename T>
 __global__ void __launch_bounds__(256) k_restrict(int Nc, int Nac, const int *__restrict__ rp, const int *__restrict__ col,
-                                                  const T *__restrict__ val, const T *__restrict__ d, T *__restrict__ fc) {
+                                                  const T *__restrict__ val, const T *__restrict__ d, T *__restrict__ fc,
+                                                  T *__restrict__ xc) {
   pdl_wait();
   pdl_trigger();
   const int lane = threadIdx.x & (W - 1);
@@ -152,7 +153,10 @@ __global__ void __launch_bounds__(256) k_restrict(int Nc, int Nac, const int *__
       for (int k = beg + lane; k < end; k += W) s += ldg(val + k) * ldg(d + ldg(col + k));
     }
     s = group_sum<W>(s);
-    if (lane == 0 && row < Nc) fc[row] = s;
+    if (lane == 0 && row < Nc) {
+      fc[row] = s;
+      if (xc) xc[row] = (T)0;  // the coarse cycle starts from zero
+    }
   }
 }
 
@@ -176,11 +180,11 @@ __global__ void __launch_bounds__(256) k_prolong_add(int Naf, const int *__restr
 }
 
 template <typename T>
-int restrict_defect(cudaStream_t s, const Level &Lf, const Level &Lc, const T *rval, const T *d, T *fc) {
+int restrict_defect(cudaStream_t s, const Level &Lf, const Level &Lc, const T *rval, const T *d, T *fc, T *xc) {
   // R = P^T has up to 27 (Q1) / 125 (Q2) entries per coarse row
   int g = grid_for(Lc.N, 16, 148);
   PMG_CUDA(launch_pdl(k_restrict<16, T>, dim3(g), dim3(256), 0, s, Lc.N, Lc.Na, (const int *)Lf.rrp.p,
-                      (const int *)Lf.rcol.p, rval, d, fc));
+                      (const int *)Lf.rcol.p, rval, d, fc, xc));
   count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
@@ -194,8 +198,8 @@ int prolongate_add(cudaStream_t s, const Level &Lf, const T *pval, const T *xc, 
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
-template int restrict_defect<double>(cudaStream_t, const Level &, const Level &, const double *, const double *, double *);
-template int restrict_defect<float>(cudaStream_t, const Level &, const Level &, const float *, const float *, float *);
+template int restrict_defect<double>(cudaStream_t, const Level &, const Level &, const double *, const double *, double *, double *);
+template int restrict_defect<float>(cudaStream_t, const Level &, const Level &, const float *, const float *, float *, float *);
 template int prolongate_add<double>(cudaStream_t, const Level &, const double *, const double *, double *, double);
 template int prolongate_add<float>(cudaStream_t, const Level &, const float *, const float *, float *, double);
 
