@@ -1,25 +1,25 @@
 // The coarse end of the V-cycle in one launch: one thread-block cluster
-// (up to 16 CTAs x 32 warps on one GPC) runs TMultiGrid3D::Cycle
+// (8 CTAs x 16 warps by default, on one GPC) runs TMultiGrid3D::Cycle
 // (src/FE/MultiGrid3D.C:449-695) for every level from `top` down to the
 // coarsest and back up -- pre-smoothing, defect, restriction, the coarsest
-// solve, prolongation, post-smoothing -- with a cluster barrier wherever the
-// level-by-level path starts a new kernel.
+// solve, prolongation, post-smoothing.
 //
-// Why: below ~50k rows a colour sweep is a few microseconds of work, so the
-// colour-by-colour launches (2 x 27 per Q2 SSOR step) are launch and L2
-// latency: levels 1-2 of the 64^3 Q2 hierarchy cost about as much as the
-// 2.1M-row finest level.
+// Why: on a level of a few thousand rows a colour sweep is well under a
+// microsecond of work, so the colour-by-colour launches (2 x 27 per Q2 SSOR
+// step, ~2.8 us each with programmatic dependent launch) are pure launch and
+// L2 latency.
 //
 // Layout: every CTA keeps a full copy of the iterate x of each level of the
-// cycle in its shared memory (35,937 + 4,913 + 729 floats for the 64^3 Q2
-// hierarchy, 166 KB).  A colour pass gathers x from the local copy (no L2
-// round trip) and a row update is stored to all copies through distributed
-// shared memory; barrier.cluster.arrive.release / wait.acquire between passes
-// makes the stores visible.  Matrices, f, d and the transfers stay in global
-// memory (L2-resident at these sizes) and are loaded before the x gathers.
-// The arithmetic is the level-by-level path's -- the same SELL-32 slices,
-// colour order, omega, damping and coarsest solve -- up to the order of the
-// partial sums inside a row.
+// cycle in its shared memory, plus the slice pointers and row permutation of
+// the levels whose Gauss-Seidel passes are pipelined.  A colour pass gathers
+// x from the local copy and sends each updated row to every copy with
+// st.async, whose byte count completes a transaction on the receiving CTA's
+// mbarrier: a CTA waits only for the rows of the pass, not for a
+// cluster-wide barrier.  The matrix, f and 1/a_ii of a pass are loaded two
+// passes ahead.  Defect, restriction, prolongation and the coarsest solve
+// are separated by cluster barriers.  The arithmetic is the level-by-level
+// path's -- the same SELL-32 slices, colour order, omega, damping and
+// coarsest solve -- up to the order of the partial sums inside a row.
 #include "pmg_internal.h"
 #include <cooperative_groups.h>
 #include <algorithm>
@@ -30,13 +30,21 @@ namespace cg = cooperative_groups;
 
 namespace pmg {
 
-constexpr int CC_MAX_LEVELS = 8, CC_MAX_GROUPS = 64, CC_WARPS = 32;
+// 16 warps per CTA: a GS pass keeps up to 32 column steps (64 registers in
+// FP32) in flight per thread plus the next pass's slice, within the 128
+// registers a 512-thread CTA allows
+constexpr int CC_MAX_LEVELS = 8, CC_MAX_GROUPS = 64, CC_WARPS = 16;
 constexpr size_t CC_SMEM_X = 200 * 1024;  // budget for the replicated iterates
 
 template <typename T>
 struct CcLevel {
   int N, Na, ncolors, xoff;  // xoff: offset of the level's x copy in shared memory
   int group[CC_MAX_GROUPS];  // slice range of colour c: [group[c], group[c+1]); group[ncolors+1] = all slices
+  unsigned char lk[CC_MAX_GROUPS];  // log2 of the warps per slice of colour c in a GS pass
+  int rows[CC_MAX_GROUPS];          // rows of colour c (the updates a GS pass sends to each CTA)
+  int one_round;                    // pipelined GS passes: every colour's slices fit one round of the
+                                    // cluster's warps, and sptr / perm are staged in shared memory
+  int soff, nsl;                    // staged sptr at ints [soff, soff + nsl], perm (32 per slice) after it
   const int *perm, *sptr, *col;
   const T *val, *invd;
   // transfer between this level and the one below (this level is the fine side)
@@ -54,6 +62,7 @@ struct CcArgs {
   const int *rp0, *kc0;  // coarsest CSR (FP64 values a0) for the Dirichlet columns of the rhs
   const double *a0;
   double *t0;            // reduced rhs f_a - A_ad f_d
+  int *err;              // set to 1 when a bounded wait gives up
   T omega, damp;
 };
 
@@ -61,8 +70,13 @@ template <typename T>
 struct CcCtx {
   cg::cluster_group cl;
   int warp, lane, gw, tw, rank, nblocks;
-  T (*part)[32];
-  T *xs;  // this CTA's shared memory holding the x copies
+  T (*part)[32];  // 2 x CC_WARPS rows: cross-warp sums, one buffer per pass parity
+  T *xs;          // this CTA's shared memory holding the x copies
+  const int *si;  // the same shared memory as ints (staged slice pointers and row permutations)
+  unsigned mbar;  // shared address of the two pass mbarriers (8 bytes apart)
+  unsigned pc;    // Gauss-Seidel passes completed so far (selects mbarrier and parity)
+  int *err;       // set when a wait gives up
+  bool failed;    // this thread's wait gave up: no further waits
   __device__ void sync() { cl.sync(); }
   // x_i := v in every CTA's copy
   __device__ void bcast(int off, int i, T v) {
@@ -84,7 +98,8 @@ __device__ void cc_slices(CcCtx<T> &c, const CcLevel<T> &L, int s0, int s1, T om
   constexpr int PF = sizeof(T) == 4 ? 16 : 8;  // column steps loaded ahead (64 registers per thread)
   const T *x = c.xs + L.xoff;
   for (int r = 0; r < rounds; r++) {
-    const int sl = s0 + r * per_round + c.rank * spc + c.warp / K;
+    // warps beyond spc * K (K need not divide the warp count) take no slice
+    const int sl = c.warp / K < spc ? s0 + r * per_round + c.rank * spc + c.warp / K : s1;
     T sum = 0, fr = 0, id = 0;
     int row = -1;
     if (sl < s1) {
@@ -131,25 +146,210 @@ __device__ void cc_slices(CcCtx<T> &c, const CcLevel<T> &L, int s0, int s1, T om
   }
 }
 
-// SSOR step of TMGLevel3D::SSOR in colour order: Dirichlet rows from f, forward, backward
+// ---- DSMEM row updates with transaction-count completion -------------------
+// A Gauss-Seidel pass sends every updated row to every CTA's copy with
+// st.async, which counts the bytes on the receiving CTA's mbarrier; a CTA
+// starts the next pass once its mbarrier has seen all rows of the pass.  No
+// cluster-wide barrier (and none of its release fence, which would wait for the
+// warp's outstanding loads) sits between passes.  Ordering: CTA A sends pass
+// p+1 only after it has received pass p from every CTA, and a CTA sends pass
+// p only after its own pass-p gathers, so no update of pass p+1 reaches a copy
+// that is still being read for pass p; and A cannot send pass p+2 before B
+// has finished receiving pass p, so two mbarriers used by pass parity keep the
+// byte counts of consecutive passes apart.
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ unsigned cluster_addr(unsigned a, int rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_async(unsigned addr, float v, unsigned mbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b32 [%0], %1, [%2];\n" ::"r"(addr),
+               "r"(__float_as_uint(v)), "r"(mbar)
+               : "memory");
+}
+__device__ __forceinline__ void st_async(unsigned addr, double v, unsigned mbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b64 [%0], %1, [%2];\n" ::"r"(addr),
+               "l"(__double_as_longlong(v)), "r"(mbar)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_init(unsigned mbar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mbar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect(unsigned mbar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mbar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+// wait for the phase of the given parity, at most 0.2 s; false when it gave up
+__device__ __forceinline__ bool mbar_wait(unsigned mbar, unsigned parity) {
+  unsigned long long t0 = 0;
+  for (int it = 0;; it++) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (it == 0) t0 = global_ns();
+    else if (global_ns() - t0 > 200000000ull) return false;
+  }
+}
+
+// One warp's share of a Gauss-Seidel colour pass whose slices all fit one round
+// (one slice per group of K warps): warp k of the group takes the column steps
+// k, k+K, ...  K = 16 (lk = log2 K, kept per colour for other shapes), so
+// that the column offsets are immediates.  head() (slice offset, length and the permuted row)
+// is issued a whole pass ahead, body() (columns, values, f, 1/a_ii --
+// everything but x) before the wait that ends the previous pass.
 template <typename T>
-__device__ void cc_ssor(CcCtx<T> &c, const CcLevel<T> &L, T omega) {
+struct CcGs {
+  static constexpr int PF = 8;  // column steps held in registers: rows of up to 128 entries in one chunk
+  int ci[PF];
+  T cv[PF];
+  int lk, k, sl, s1, off, lmax, row;  // sl >= s1: no slice for this warp; row < 0: no row for this lane
+  T fr, id;
+
+  template <int K>
+  __device__ __forceinline__ void load_k(const CcLevel<T> &L, int lane) {
+    const int rem = lmax - k;  // column steps u*K + k < lmax
+    const int *cp = L.col + off + 32 * k + lane;
+    const T *vp = L.val + off + 32 * k + lane;
+#pragma unroll
+    for (int u = 0; u < PF; u++) {
+      ci[u] = u * K < rem ? __ldg(cp + 32 * K * u) : 0;
+      cv[u] = u * K < rem ? __ldg(vp + 32 * K * u) : (T)0;
+    }
+    fr = id = 0;
+    if (row >= 0) {
+      fr = __ldcg(L.f + row);
+      id = __ldg(L.invd + sl * 32 + lane);
+    }
+  }
+  // this warp's slice of the colour's pass and everything of it but x: the
+  // slice pointers and rows from shared memory, the rest from global memory
+  __device__ __forceinline__ void load(const CcCtx<T> &c, const CcLevel<T> &L, int colour) {
+    const int s0 = L.group[colour];
+    s1 = L.group[colour + 1];
+    lk = L.lk[colour];
+    k = c.warp & ((1 << lk) - 1);
+    const int spc = CC_WARPS >> lk, slot = c.warp >> lk;
+    sl = slot < spc ? s0 + c.rank * spc + slot : s1;
+    lmax = 0;
+    row = -1;
+    if (sl >= s1) return;  // no slice (warp-uniform)
+    const int *sp = c.si + L.soff;
+    off = sp[sl];
+    lmax = (sp[sl + 1] - off) >> 5;
+    row = sp[L.nsl + 1 + sl * 32 + c.lane];
+    load_k<16>(L, c.lane);
+  }
+  // gathers from the local copy, the cross-warp sum (part: this pass's
+  // buffer), and the update sent to every CTA's copy; the K warps of a slice
+  // share the sends
+  template <int K>
+  __device__ __forceinline__ void run_k(const CcCtx<T> &c, const CcLevel<T> &L, T omega, T (*part)[32],
+                                        unsigned mbar) {
+    const T *x = c.xs + L.xoff;
+    const bool active = sl < s1;
+    T sum = 0, xr = 0;
+    if (active) {
+      const int rem = lmax - k;
+#pragma unroll
+      for (int u = 0; u < PF; u++)
+        if (u * K < rem) sum += cv[u] * x[ci[u]];
+      // rows longer than K * PF column steps: the rest in further chunks
+      for (int c0 = PF; c0 * K < rem; c0 += PF) {
+        const int *cp = L.col + off + 32 * (k + c0 * K) + c.lane;
+        const T *vp = L.val + off + 32 * (k + c0 * K) + c.lane;
+        const int rem2 = rem - c0 * K;
+#pragma unroll
+        for (int u = 0; u < PF; u++) {
+          ci[u] = u * K < rem2 ? __ldg(cp + 32 * K * u) : 0;
+          cv[u] = u * K < rem2 ? __ldg(vp + 32 * K * u) : (T)0;
+        }
+#pragma unroll
+        for (int u = 0; u < PF; u++)
+          if (u * K < rem2) sum += cv[u] * x[ci[u]];
+      }
+      // x_row before the barrier: after it, an update of this row may already
+      // have reached this CTA's copy
+      if (row >= 0) xr = x[row];
+    }
+    part[c.warp][c.lane] = sum;
+    __syncthreads();
+    if (active && row >= 0) {
+      const int w0 = c.warp - k;
+      T s = 0;
+#pragma unroll
+      for (int kk = 0; kk < K; kk++) s += part[w0 + kk][c.lane];
+      const T v = xr + omega * (fr - s) * id;
+      const unsigned a = smem_addr(c.xs + L.xoff + row);
+      for (int b = k; b < c.nblocks; b += K) st_async(cluster_addr(a, b), v, cluster_addr(mbar, b));
+    }
+  }
+  __device__ __forceinline__ void run(const CcCtx<T> &c, const CcLevel<T> &L, T omega, T (*part)[32], unsigned mbar) {
+    run_k<16>(c, L, omega, part, mbar);
+  }
+};
+
+// SSOR step of TMGLevel3D::SSOR in colour order: Dirichlet rows from f (first
+// step of a level visit; the sweeps never change them), forward, backward
+template <typename T>
+__device__ void cc_ssor(CcCtx<T> &c, const CcLevel<T> &L, T omega, bool dirichlet) {
   // every CTA refreshes the Dirichlet rows of its own copy
-  for (int i = L.Na + threadIdx.x; i < L.N; i += blockDim.x) c.xs[L.xoff + i] = __ldcg(L.f + i);
-  __syncthreads();
-  for (int cc = 0; cc < L.ncolors; cc++) {
-    cc_slices<T, true>(c, L, L.group[cc], L.group[cc + 1], omega);
-    c.sync();
+  if (dirichlet) {
+    for (int i = L.Na + threadIdx.x; i < L.N; i += blockDim.x) c.xs[L.xoff + i] = __ldcg(L.f + i);
+    __syncthreads();
   }
-  for (int cc = L.ncolors - 1; cc >= 0; cc--) {
-    cc_slices<T, true>(c, L, L.group[cc], L.group[cc + 1], omega);
-    c.sync();
+  const int nc = L.ncolors;
+  if (!L.one_round) {  // colours that need several rounds: one pass at a time
+    for (int cc = 0; cc < nc; cc++) {
+      cc_slices<T, true>(c, L, L.group[cc], L.group[cc + 1], omega);
+      c.sync();
+    }
+    for (int cc = nc - 1; cc >= 0; cc--) {
+      cc_slices<T, true>(c, L, L.group[cc], L.group[cc + 1], omega);
+      c.sync();
+    }
+    return;
   }
+  // passes p = 0 .. 2nc-1 over colours 0..nc-1, nc-1..0 (an even count); A
+  // runs the even passes and B the odd ones, each loading its next pass two
+  // passes ahead
+  auto colour = [&](int p) { return p < nc ? p : 2 * nc - 1 - p; };
+  auto pass = [&](CcGs<T> &g, int p) {
+    const unsigned mbar = c.mbar + 8 * (c.pc & 1);
+    if (threadIdx.x == 0) mbar_expect(mbar, (unsigned)(L.rows[colour(p)] * sizeof(T)));
+    g.run(c, L, omega, c.part + (c.pc & 1) * CC_WARPS, mbar);
+    if (p + 2 < 2 * nc) g.load(c, L, colour(p + 2));
+    // after one wait has given up (error flagged), the rest of the launch runs
+    // without waiting so that it ends; its result is discarded by the host
+    if (!c.failed && !mbar_wait(mbar, (c.pc >> 1) & 1)) {
+      c.failed = true;
+      atomicExch(c.err, 1);
+    }
+    c.pc++;
+  };
+  CcGs<T> A, B;
+  A.load(c, L, colour(0));
+  B.load(c, L, colour(1));
+  for (int p = 0; p < 2 * nc; p += 2) {
+    pass(A, p);
+    pass(B, p + 1);
+  }
+  __syncthreads();  // the last pass's sums are read before part is reused
 }
 
 template <typename T>
 __global__ void __launch_bounds__(CC_WARPS * 32, 1) k_coarse_cycle(const __grid_constant__ CcArgs<T> a) {
-  __shared__ T part[CC_WARPS][32];
+  __shared__ T part[2 * CC_WARPS][32];
+  __shared__ __align__(8) unsigned long long mbars[2];
   extern __shared__ __align__(16) unsigned char cc_dyn[];
   CcCtx<T> c{cg::this_cluster()};
   c.warp = threadIdx.x >> 5;
@@ -160,9 +360,27 @@ __global__ void __launch_bounds__(CC_WARPS * 32, 1) k_coarse_cycle(const __grid_
   c.tw = c.nblocks * CC_WARPS;
   c.part = part;
   c.xs = reinterpret_cast<T *>(cc_dyn);
+  c.si = reinterpret_cast<const int *>(cc_dyn);
+  c.mbar = smem_addr(mbars);
+  c.pc = 0;
+  c.err = a.err;
+  c.failed = false;
+  if (threadIdx.x == 0) {
+    mbar_init(c.mbar, 1);
+    mbar_init(c.mbar + 8, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
   const int top = a.nlev - 1;
   // the entry level starts from x = 0 (the caller zeroed its global copy)
   for (int i = threadIdx.x; i < a.lv[top].N; i += blockDim.x) c.xs[a.lv[top].xoff + i] = (T)0;
+  // slice pointers and row permutations of the pipelined levels (constant data)
+  for (int l = 0; l <= top; l++) {
+    const CcLevel<T> &L = a.lv[l];
+    if (!L.one_round) continue;
+    int *sp = reinterpret_cast<int *>(cc_dyn) + L.soff;
+    for (int i = threadIdx.x; i <= L.nsl; i += blockDim.x) sp[i] = __ldg(L.sptr + i);
+    for (int i = threadIdx.x; i < L.nsl * 32; i += blockDim.x) sp[L.nsl + 1 + i] = __ldg(L.perm + i);
+  }
   pdl_wait();
   pdl_trigger();
   c.sync();  // every copy initialised before any remote store
@@ -170,7 +388,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, 1) k_coarse_cycle(const __grid_
   for (int l = top; l >= 1; l--) {
     const CcLevel<T> &L = a.lv[l];
     const CcLevel<T> &C = a.lv[l - 1];
-    for (int s = 0; s < a.pre; s++) cc_ssor(c, L, a.omega);
+    for (int s = 0; s < a.pre; s++) cc_ssor(c, L, a.omega, s == 0);
     cc_slices<T, false>(c, L, 0, L.group[L.ncolors + 1], a.omega);
     // each CTA zeroes its own copy of the coarse iterate
     for (int i = threadIdx.x; i < C.N; i += blockDim.x) c.xs[C.xoff + i] = (T)0;
@@ -219,7 +437,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, 1) k_coarse_cycle(const __grid_
     }
     c.sync();
   } else {
-    for (int s = 0; s < a.coarse_it; s++) cc_ssor(c, Z, a.omega);
+    for (int s = 0; s < a.coarse_it; s++) cc_ssor(c, Z, a.omega, s == 0);
   }
   // up: prolongate, smooth
   for (int l = 1; l <= top; l++) {
@@ -235,8 +453,10 @@ __global__ void __launch_bounds__(CC_WARPS * 32, 1) k_coarse_cycle(const __grid_
       c.bcast(L.xoff, row, c.xs[L.xoff + row] + a.damp * v);
     }
     c.sync();
-    for (int s = 0; s < a.post; s++) cc_ssor(c, L, a.omega);
+    for (int s = 0; s < a.post; s++) cc_ssor(c, L, a.omega, s == 0);
   }
+  // every CTA has received all updates; none leaves while a send may be in flight
+  c.sync();
   // the entry level's iterate back to global memory for the finer level
   const CcLevel<T> &E = a.lv[top];
   for (int i = c.rank * blockDim.x + threadIdx.x; i < E.N; i += c.nblocks * blockDim.x) __stcg(E.x + i, c.xs[E.xoff + i]);
@@ -285,19 +505,28 @@ static int cluster_ctas() {
 }
 
 // the highest level that, with every level below it, fits the cluster launch
-// (0: none -- the level-by-level path runs)
-// levels 0..top in one launch, opt-in: PMG_COARSE_CLUSTER=1 runs the levels
-// of at most CC_ONE_CTA_ROWS rows on one CTA, PMG_COARSE_CLUSTER=16 every
-// level whose iterates fit CC_SMEM_X on a 16-CTA cluster.  Both measured
-// slower than the PDL-chained colour launches on the 64^3 Q2 hierarchy (a
-// colour pass here ~5 us), so the default is the level-by-level path.
+// (0: none -- the level-by-level path runs).  PMG_COARSE_CLUSTER=<ctas>[:<max
+// rows>] chooses the shape: the default "8:8192" runs the levels of at most
+// 8192 rows on an 8-CTA cluster (measured: 64^3 Q2 FP32 V-cycle 4.17 ms
+// against 4.31 ms level by level; larger levels stream more matrix per colour
+// pass than one GPC's share of L2 bandwidth carries faster than the 148-SM
+// colour launches); "1" runs the levels of at most CC_ONE_CTA_ROWS rows on one
+// CTA, "16" (2, 4, 8) every level whose iterates fit CC_SMEM_X on a cluster of
+// that size, "0" none.
 constexpr int CC_ONE_CTA_ROWS = 8192;
 
 int coarse_cycle_top(Handle &h) {
-  static int mode = -1;
+  static int mode = -1;  // 0 off, 1 one CTA, 2 cluster
+  static long max_rows = 0;
+  static int want = 0;   // CTAs asked for
   if (mode < 0) {
     const char *e = getenv("PMG_COARSE_CLUSTER");
-    mode = !e ? 0 : (std::string(e) == "1") ? 1 : (std::string(e) == "16") ? 2 : 0;
+    const std::string v(e ? e : "8:8192");
+    const size_t colon = v.find(':');
+    want = atoi(v.substr(0, colon).c_str());
+    mode = want == 1 ? 1 : (want == 2 || want == 4 || want == 8 || want == 16) ? 2 : 0;
+    max_rows = mode == 1 ? CC_ONE_CTA_ROWS : 0;
+    if (mode && colon != std::string::npos) max_rows = atol(v.c_str() + colon + 1);
   }
   if (mode == 0) return 0;
   const size_t vb = h.prm.precision == PMG_PREC_FP32 ? sizeof(float) : sizeof(double);
@@ -307,19 +536,33 @@ int coarse_cycle_top(Handle &h) {
     const Level &L = h.lv[i];
     bytes += ((size_t)L.N * vb + 15) / 16 * 16;
     if (bytes > CC_SMEM_X || (int)L.sell_group.size() > CC_MAX_GROUPS) break;
-    if (mode == 1 && L.N > CC_ONE_CTA_ROWS) break;
+    if (max_rows > 0 && L.N > max_rows) break;
     top = i;
   }
   if (top < 1) return 0;
+  if (!h.cc_err.p) {
+    if (h.cc_err.alloc(1) != PMG_OK) return 0;
+    if (cudaMemset(h.cc_err.p, 0, sizeof(int)) != cudaSuccess) return 0;
+  }
   if (mode == 1) {
     h.cc_ctas = 1;
   } else {
     // the launch shape is queried here, outside any stream capture
     const int c = std::min(cluster_ctas<float>(), cluster_ctas<double>());
     if (!c) return 0;
-    h.cc_ctas = c;
+    h.cc_ctas = std::min(c, want);
   }
   return top;
+}
+
+int coarse_cycle_check(Handle &h) {
+  if (!h.cc_err.p) return PMG_OK;
+  int e = 0;
+  PMG_CUDA(cudaMemcpy(&e, h.cc_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (!e) return PMG_OK;
+  PMG_CUDA(cudaMemset(h.cc_err.p, 0, sizeof(int)));
+  set_error("coarse cycle: a cluster wait gave up (updates of a pass never arrived)");
+  return PMG_ERR_STATE;
 }
 
 template <typename T>
@@ -327,6 +570,10 @@ int coarse_cycle(Handle &h, int top) {
   if (top < 1 || top >= CC_MAX_LEVELS) {
     set_error("coarse_cycle: level out of range");
     return PMG_ERR_ARG;
+  }
+  if (h.cc_ctas < 1) {
+    set_error("coarse_cycle: launch shape not set");
+    return PMG_ERR_STATE;
   }
   CcArgs<T> a{};
   a.nlev = top + 1;
@@ -340,6 +587,16 @@ int coarse_cycle(Handle &h, int top) {
     smem += ((size_t)L.N * sizeof(T) + 15) / 16 * 16;
     d.ncolors = (int)L.sell_group.size() - 2;
     for (size_t g = 0; g < L.sell_group.size(); g++) d.group[g] = L.sell_group[g];
+    // warps per slice of each colour: the most (up to 16) that still cover the
+    // colour's slices in one round of the cluster's warps
+    d.one_round = 1;
+    for (int cc = 0; cc < d.ncolors; cc++) {
+      const int nsl = d.group[cc + 1] - d.group[cc];
+      const int lk = 4;  // K = 16: the instantiated pass shape
+      if (nsl > (CC_WARPS >> lk) * h.cc_ctas) d.one_round = 0;
+      d.lk[cc] = (unsigned char)lk;
+      d.rows[cc] = L.rcolor_ptr[cc + 1] - L.rcolor_ptr[cc];
+    }
     d.perm = L.sell_perm.p;
     d.sptr = L.sell_ptr.p;
     d.col = L.sell_col.p;
@@ -353,6 +610,21 @@ int coarse_cycle(Handle &h, int top) {
     d.f = lv_vec<T>(L, 1);
     d.d = lv_vec<T>(L, 2);
   }
+  // shared memory after the x copies: sptr and perm of the levels whose GS
+  // passes are pipelined (a level that does not fit runs one pass at a time)
+  for (int i = 0; i <= top; i++) {
+    CcLevel<T> &d = a.lv[i];
+    d.soff = 0;
+    d.nsl = h.lv[i].sell_nslices;
+    if (!d.one_round) continue;
+    const size_t need = ((size_t)(d.nsl + 1) + (size_t)d.nsl * 32) * sizeof(int);
+    if (smem + need > CC_SMEM_X) {
+      d.one_round = 0;
+      continue;
+    }
+    d.soff = (int)(smem / sizeof(int));
+    smem += (need + 15) / 16 * 16;
+  }
   const bool direct = h.prm.coarse_smoother == PMG_COARSE_DIRECT;
   a.direct = direct ? 1 : 0;
   a.inv = direct ? h.coarse_inv.p : nullptr;
@@ -362,16 +634,13 @@ int coarse_cycle(Handle &h, int top) {
   a.kc0 = h.lv[0].kcol.p;
   a.a0 = h.lv[0].A.p;
   a.t0 = h.coarse_t.p;
+  a.err = h.cc_err.p;
   a.coarse_it = h.prm.coarse_maxit > 0 ? h.prm.coarse_maxit : 1;
   a.pre = h.prm.pre_smooth;
   a.post = h.prm.post_smooth;
   a.omega = (T)h.prm.smooth_omega;
   a.damp = (T)h.prm.gmg_damp;
   const int ctas = h.cc_ctas;
-  if (ctas < 1) {
-    set_error("coarse_cycle: launch shape not set");
-    return PMG_ERR_STATE;
-  }
   if (ctas == 1) {
     static bool attr = false;
     if (!attr) {

@@ -193,6 +193,7 @@ struct Handle {
   unsigned long long vgraph_kernels = 0;
   bool use_graph = true;  // PMG_NO_GRAPH=1 launches the V-cycle kernels directly (profilers)
   int cc_top = 0;         // levels 0..cc_top run as one launch (0: none)
+  DBuf<int> cc_err;      // set by the one-launch coarse cycle when a bounded wait gives up
   int cc_ctas = 0;        // CTAs of that launch (1, or a cluster of up to 16)
   // learned smoother: BF16 weights used by the kernels, FP32 master copy, Adam state
   DBuf<uint16_t> lw_bf16;
@@ -262,6 +263,8 @@ void invalidate_graphs(Handle *h);
 
 // the coarse end of the V-cycle in one thread-block-cluster launch (coarse_cycle.cu)
 int coarse_cycle_top(Handle &h);
+// PMG_ERR_STATE (and the flag cleared) when a wait of the one-launch coarse cycle gave up
+int coarse_cycle_check(Handle &h);
 template <typename T>
 int coarse_cycle(Handle &h, int top);
 

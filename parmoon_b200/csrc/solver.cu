@@ -691,6 +691,7 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
   h.t_solve = ms * 1e-3;
   if (sol_host) PMG_CUDA(cudaMemcpyAsync(sol_host, h.sol.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
   PMG_CUDA(cudaStreamSynchronize(s));
+  PMG_TRY(coarse_cycle_check(h));
   if (st) {
     st->iterations = iters;
     st->res0 = res0;
@@ -716,5 +717,5 @@ extern "C" int pmg_vcycle(pmg_handle hh, const double *v_dev, double *z_dev) {
   PMG_TRY(pmg::capture_vcycle(*h));
   PMG_TRY(pmg::precondition(*h, v_dev, z_dev, h->prm.smoother == PMG_SMOOTHER_LEARNED));
   PMG_CUDA(cudaStreamSynchronize(h->stream));
-  return PMG_OK;
+  return pmg::coarse_cycle_check(*h);
 }

@@ -1,6 +1,7 @@
-"""The coarse end of the V-cycle as one launch (opt-in: one CTA for the
-smallest levels, PMG_COARSE_CLUSTER=1, or a 16-CTA thread-block cluster,
-PMG_COARSE_CLUSTER=16) gives the same solve as the level-by-level launches: same
+"""The coarse end of the V-cycle as one launch (one CTA for the smallest
+levels, PMG_COARSE_CLUSTER=1; a 16-CTA thread-block cluster, =16; an 8-CTA
+cluster on the levels of at most 8192 rows, =8:8192, the default) gives the
+same solve as the level-by-level launches (=0): same
 FGMRES iteration count (+-1) and solutions within 1e-8 relative (both stop at
 |r| <= 1e-10 |r0|; the two paths differ only in the order of partial sums
 inside a row).  Each configuration runs in its own process because the switch
@@ -37,16 +38,14 @@ print(json.dumps(dict(rc=rc, its=st.iterations, rel=st.rel_res)))
 def run(tmp_path, tag, args, mode):
     out = str(tmp_path / f"{tag}.npy")
     env = dict(os.environ)
-    env.pop("PMG_COARSE_CLUSTER", None)
-    if mode is not None:
-        env["PMG_COARSE_CLUSTER"] = mode
+    env["PMG_COARSE_CLUSTER"] = mode if mode is not None else "0"
     p = subprocess.run([sys.executable, "-c", SCRIPT.format(root=ROOT, args=args, out=out)], env=env,
                        capture_output=True, text=True, timeout=600)
     assert p.returncode == 0, p.stderr[-3000:]
     return json.loads(p.stdout.strip().splitlines()[-1]), np.load(out)
 
 
-@pytest.mark.parametrize("mode", ["1", "16"])  # one CTA, 16-CTA cluster
+@pytest.mark.parametrize("mode", ["1", "16", "8:8192"])  # one CTA, 16-CTA cluster, 8-CTA cluster on small levels
 @pytest.mark.parametrize("elem,n,nl,prec,coarse", [(2, 16, 3, 1, 17), (1, 32, 4, 1, 17), (1, 32, 4, 0, 17),
                                                    (2, 16, 3, 0, 3)])
 def test_coarse_cycle_launch_matches_level_launches(tmp_path, elem, n, nl, prec, coarse, mode):
