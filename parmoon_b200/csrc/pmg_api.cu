@@ -634,6 +634,8 @@ int pmg_time_kernel(pmg_handle hh, int kernel, int level, int form, int reps, do
   if (reps < 1 || !sec) return PMG_ERR_ARG;
   if (!L.assembled && kernel != PMG_KERNEL_ASSEMBLE) { set_error("pmg_time_kernel: assemble first"); return PMG_ERR_STATE; }
   const double N = L.N, nnz = L.nnz;
+  // the solve copy's stored entries: 2-byte column deltas, 4-byte columns in
+  // the slices whose deltas do not fit (known once the copy is built)
   double by = 0, fl = 0;
   DBuf<double> x64, y64;
   DBuf<float> x32, y32;
@@ -653,9 +655,13 @@ int pmg_time_kernel(pmg_handle hh, int kernel, int level, int form, int reps, do
   if (kernel == PMG_KERNEL_SPMV64 || kernel == PMG_KERNEL_SSOR64 || kernel == PMG_KERNEL_CSR_SPMV64) {
     PMG_TRY(x64.alloc(L.N)); PMG_TRY(y64.alloc(L.N));
     PMG_TRY(fill(s, x64.p, 1.0, L.N)); PMG_TRY(fill(s, y64.p, 1.0, L.N));
-    if (kernel != PMG_KERNEL_CSR_SPMV64) PMG_TRY(sell_values<double>(*h, L));
-    // CSR bytes: values + column indices + row pointers + x gather (once) + y write
-    double spmv_b = 12 * nnz + 4 * (N + 1) + 16 * N;
+    double spmv_b = 12 * nnz + 4 * (N + 1) + 16 * N;  // CSR: values + columns + row pointers + x once + y
+    if (kernel != PMG_KERNEL_CSR_SPMV64) {
+      PMG_TRY(sell_values<double>(*h, L));
+      // SELL: values + column deltas / columns + slice pointers + row of each lane + x once + y
+      spmv_b = 8.0 * (L.sell_nnz_narrow + L.sell_nnz_wide) + 2.0 * L.sell_nnz_narrow + 4.0 * L.sell_nnz_wide +
+               4.0 * (L.sell_nslices + 1) + 4 * N + 16 * N;
+    }
     by = kernel == PMG_KERNEL_SSOR64 ? 2 * spmv_b + 16 * N : spmv_b;
     fl = kernel == PMG_KERNEL_SSOR64 ? 4 * nnz : 2 * nnz;
   } else if (kernel == PMG_KERNEL_SPMV32 || kernel == PMG_KERNEL_SSOR32) {
@@ -663,7 +669,8 @@ int pmg_time_kernel(pmg_handle hh, int kernel, int level, int form, int reps, do
     PMG_TRY(x32.alloc(L.N)); PMG_TRY(y32.alloc(L.N));
     PMG_CUDA(cudaMemsetAsync(x32.p, 0, sizeof(float) * L.N, s));
     PMG_CUDA(cudaMemsetAsync(y32.p, 0, sizeof(float) * L.N, s));
-    double spmv_b = 8 * nnz + 4 * (N + 1) + 8 * N;
+    double spmv_b = 4.0 * (L.sell_nnz_narrow + L.sell_nnz_wide) + 2.0 * L.sell_nnz_narrow + 4.0 * L.sell_nnz_wide +
+                    4.0 * (L.sell_nslices + 1) + 4 * N + 8 * N;
     by = kernel == PMG_KERNEL_SPMV32 ? spmv_b : 2 * spmv_b + 8 * N;
     fl = kernel == PMG_KERNEL_SPMV32 ? 2 * nnz : 4 * nnz;
   } else if (kernel == PMG_KERNEL_COARSE_FACTOR) {

@@ -141,6 +141,14 @@ struct Level {
   long sell_nnz = 0;
   std::vector<int> sell_group;  // slice range of each colour group (+ Dirichlet group)
   DBuf<int> sell_perm, sell_ptr, sell_col;
+  // solve copy of an active row = its columns < Na (a prefix: columns are
+  // sorted); the Dirichlet columns are applied separately (dd_row / dd_beg)
+  DBuf<short> sell_c16;          // column - the lane's row, for slices whose deltas fit 16 bits
+  DBuf<unsigned char> sell_wide; // 1: the slice keeps 32-bit columns (sell_col)
+  DBuf<int> sell_alen;           // entries of each row in the solve copy
+  DBuf<int> dd_row, dd_beg;      // active rows with Dirichlet columns, first such CSR position
+  int n_dd = 0;
+  long sell_nnz_narrow = 0, sell_nnz_wide = 0;  // stored entries with 16-bit / 32-bit columns
   DBuf<float> sell_val32, sell_invd32;
   DBuf<double> sell_val64, sell_invd64;
 };
@@ -247,6 +255,10 @@ template <typename T>
 int sell_spmv(cudaStream_t s, const Level &L, const T *x, const T *f, T *y, int mode, int num_sms);
 template <typename T>
 int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, int num_sms, bool dirichlet = true);
+// y_a -= A_aD v_D over the active rows' Dirichlet columns (the part of A the
+// solve copy leaves out)
+template <typename T>
+int dirichlet_cols(cudaStream_t s, const Level &L, const T *v, T *y);
 
 // ------------------------------------------------------------- solver (solver.cu)
 int coarse_factor(Handle &h);

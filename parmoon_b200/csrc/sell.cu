@@ -31,11 +31,26 @@ namespace pmg {
 
 int build_sell(Handle &h, Level &L) {
   if (L.sell_ready) return PMG_OK;
-  const int N = L.N;
+  const int N = L.N, Na = L.Na;
   const std::vector<int> &rp = L.h_rowptr, &kc = L.h_kcol;
   if ((int)rp.size() != N + 1) {
     set_error("build_sell: host copy of the CSR pattern missing");
     return PMG_ERR_STATE;
+  }
+  // entries of each row in the solve copy: an active row keeps its columns < Na
+  // (columns are sorted, so that is a prefix), a Dirichlet row all of its own
+  std::vector<int> alen(N);
+  std::vector<int> dd_row, dd_beg;
+  for (int r = 0; r < N; r++) {
+    int n = rp[r + 1] - rp[r];
+    if (r < Na) {
+      n = (int)(std::lower_bound(kc.begin() + rp[r], kc.begin() + rp[r + 1], Na) - (kc.begin() + rp[r]));
+      if (rp[r] + n < rp[r + 1]) {
+        dd_row.push_back(r);
+        dd_beg.push_back(rp[r] + n);
+      }
+    }
+    alen[r] = n;
   }
   // groups: colours of the active rows, then the Dirichlet rows
   const int nc = (int)L.rcolor_ptr.size() - 1;
@@ -46,10 +61,9 @@ int build_sell(Handle &h, Level &L) {
   for (int g = 0; g <= nc; g++) {
     rows.clear();
     if (g < nc) rows.assign(L.h_row_list.begin() + L.rcolor_ptr[g], L.h_row_list.begin() + L.rcolor_ptr[g + 1]);
-    else for (int r = L.Na; r < N; r++) rows.push_back(r);
+    else for (int r = Na; r < N; r++) rows.push_back(r);
     std::stable_sort(rows.begin(), rows.end(), [&](int a, int b) {
-      int la = rp[a + 1] - rp[a], lb = rp[b + 1] - rp[b];
-      return la > lb || (la == lb && a < b);
+      return alen[a] > alen[b] || (alen[a] == alen[b] && a < b);
     });
     group_slice[g] = (int)(perm.size() / 32);
     perm.insert(perm.end(), rows.begin(), rows.end());
@@ -63,7 +77,7 @@ int build_sell(Handle &h, Level &L) {
     int lmax = 0;
     for (int l = 0; l < 32; l++) {
       int r = perm[(size_t)s * 32 + l];
-      if (r >= 0) lmax = std::max(lmax, rp[r + 1] - rp[r]);
+      if (r >= 0) lmax = std::max(lmax, alen[r]);
     }
     sptr[s] = (int)total;
     total += 32L * lmax;
@@ -73,24 +87,50 @@ int build_sell(Handle &h, Level &L) {
     }
   }
   sptr[nslices] = (int)total;
+  // columns: 32-bit for every slice (the one-launch coarse cycle reads these),
+  // and column - row in 16 bits for the slices where every delta fits, which
+  // the colour sweeps and products read instead (2 bytes per entry, not 4);
+  // padding repeats the row (delta 0), padding lanes read x[0] with value 0
   std::vector<int> col((size_t)total);
-#pragma omp parallel for schedule(dynamic, 256)
+  std::vector<short> c16((size_t)total);
+  std::vector<unsigned char> wide(nslices, 0);
+  long narrow_nnz = 0, wide_nnz = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : narrow_nnz, wide_nnz)
   for (int s = 0; s < nslices; s++) {
     const int off = sptr[s], lmax = (sptr[s + 1] - off) / 32;
+    bool fits = true;
+    long stored = 0;
     for (int l = 0; l < 32; l++) {
       const int r = perm[(size_t)s * 32 + l];
-      const int len = r >= 0 ? rp[r + 1] - rp[r] : 0;
-      for (int j = 0; j < lmax; j++)
-        col[(size_t)off + 32 * j + l] = j < len ? kc[rp[r] + j] : (r >= 0 ? r : 0);
+      const int len = r >= 0 ? alen[r] : 0;
+      stored += len;
+      for (int j = 0; j < lmax; j++) {
+        const int c = j < len ? kc[rp[r] + j] : (r >= 0 ? r : 0);
+        col[(size_t)off + 32 * j + l] = c;
+        const long d = r >= 0 ? (long)c - r : 0;
+        if (d < -32768 || d > 32767) fits = false;
+        c16[(size_t)off + 32 * j + l] = (short)(fits ? d : 0);
+      }
     }
+    wide[s] = fits ? 0 : 1;
+    if (fits) narrow_nnz += stored;
+    else wide_nnz += stored;
   }
   PMG_TRY(L.sell_perm.upload(perm.data(), perm.size(), h.stream));
   PMG_TRY(L.sell_ptr.upload(sptr.data(), sptr.size(), h.stream));
   PMG_TRY(L.sell_col.upload(col.data(), col.size(), h.stream));
+  PMG_TRY(L.sell_c16.upload(c16.data(), c16.size(), h.stream));
+  PMG_TRY(L.sell_wide.upload(wide.data(), wide.size(), h.stream));
+  PMG_TRY(L.sell_alen.upload(alen.data(), alen.size(), h.stream));
+  L.n_dd = (int)dd_row.size();
+  PMG_TRY(L.dd_row.upload(dd_row.data(), dd_row.size(), h.stream));
+  PMG_TRY(L.dd_beg.upload(dd_beg.data(), dd_beg.size(), h.stream));
   PMG_CUDA(cudaStreamSynchronize(h.stream));
   L.sell_group = group_slice;
   L.sell_nslices = nslices;
   L.sell_nnz = total;
+  L.sell_nnz_narrow = narrow_nnz;
+  L.sell_nnz_wide = wide_nnz;
   L.sell_ready = true;
   L.sell_val_fresh32 = L.sell_val_fresh64 = false;
   return PMG_OK;
@@ -99,13 +139,13 @@ int build_sell(Handle &h, Level &L) {
 // values of the CSR matrix into the slice layout (and the permuted inverse diagonal)
 template <typename T>
 __global__ void k_csr_to_sell(int nslices, const int *__restrict__ perm, const int *__restrict__ sptr,
-                              const int *__restrict__ rp, const double *__restrict__ a, const int *__restrict__ dpos,
-                              T *__restrict__ val, T *__restrict__ invd) {
+                              const int *__restrict__ rp, const int *__restrict__ alen, const double *__restrict__ a,
+                              const int *__restrict__ dpos, T *__restrict__ val, T *__restrict__ invd) {
   const int lane = threadIdx.x & 31;
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nslices; s += (gridDim.x * blockDim.x) >> 5) {
     const int off = sptr[s], lmax = (sptr[s + 1] - off) >> 5;
     const int r = perm[s * 32 + lane];
-    const int beg = r >= 0 ? rp[r] : 0, len = r >= 0 ? rp[r + 1] - beg : 0;
+    const int beg = r >= 0 ? rp[r] : 0, len = r >= 0 ? alen[r] : 0;
     for (int j = 0; j < lmax; j++) val[off + 32 * j + lane] = j < len ? (T)a[beg + j] : (T)0;
     T dv = (T)1;
     if (r >= 0) {
@@ -135,7 +175,8 @@ int sell_values(Handle &h, Level &L) {
   }
   int blocks = std::min((L.sell_nslices + 7) / 8, h.num_sms * 16);
   k_csr_to_sell<T><<<std::max(blocks, 1), 256, 0, h.stream>>>(L.sell_nslices, L.sell_perm.p, L.sell_ptr.p, L.rowptr.p,
-                                                                L.A.p, L.diagpos.p, val, invd); count_launches(1);
+                                                                L.sell_alen.p, L.A.p, L.diagpos.p, val, invd);
+  count_launches(1);
   PMG_CUDA(cudaGetLastError());
   if (f32) L.sell_val_fresh32 = true; else L.sell_val_fresh64 = true;
   return PMG_OK;
@@ -150,59 +191,74 @@ template int sell_values<double>(Handle &, Level &);
 // that each warp's chain of dependent loads (column index, then x) stays
 // short; large colours already fill the GPU with K = 4.
 
+// Column indices: a slice whose deltas fit (every slice of a lattice-ordered
+// level) is read as 16-bit column - row deltas and gathered through x + row
+// of the lane; the other slices read the 32-bit columns.  The choice is per
+// slice and warp-uniform.
+template <int PF, int K>
+__device__ __forceinline__ void sell_load_cols(bool wd, const int *__restrict__ col, const short *__restrict__ c16,
+                                               int base, int j0, int lmax, int *ci) {
+  if (wd) {
+#pragma unroll
+    for (int u = 0; u < PF; u++) ci[u] = j0 + u * K < lmax ? __ldg(col + base + 32 * K * u) : 0;
+  } else {
+#pragma unroll
+    for (int u = 0; u < PF; u++) ci[u] = j0 + u * K < lmax ? (int)__ldg(c16 + base + 32 * K * u) : 0;
+  }
+}
+
 // y = A x (MODE 0) or d = f - A x (MODE 1) over slices [s0, s1)
 template <typename T, int MODE, int K>
 __global__ void __launch_bounds__(32 * K) k_sell_mv(int s0, int s1, const int *__restrict__ perm,
                                                     const int *__restrict__ sptr, const int *__restrict__ col,
+                                                    const short *__restrict__ c16,
+                                                    const unsigned char *__restrict__ wide,
                                                     const T *__restrict__ val, const T *__restrict__ x,
                                                     const T *__restrict__ f, T *__restrict__ y) {
   constexpr int PF = sizeof(T) == 4 ? 16 : 8;  // column steps per chunk
   __shared__ T part[K][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int s = s0 + blockIdx.x;
-  int off = 0, lmax = 0;
+  int off = 0, lmax = 0, r = -1;
+  bool wd = false;
   int ci[PF];
   T cv[PF];
   auto load_chunk = [&](int c0) {
+    const int j0 = w + c0 * K;
+    sell_load_cols<PF, K>(wd, col, c16, off + 32 * j0 + lane, j0, lmax, ci);
 #pragma unroll
-    for (int u = 0; u < PF; u++) {
-      const int j = w + (c0 + u) * K;
-      const bool in = j < lmax;
-      ci[u] = in ? __ldg(col + off + 32 * j + lane) : 0;
-      cv[u] = in ? __ldg(val + off + 32 * j + lane) : (T)0;
-    }
+    for (int u = 0; u < PF; u++) cv[u] = j0 + u * K < lmax ? __ldg(val + off + 32 * (j0 + u * K) + lane) : (T)0;
+  };
+  auto start = [&](int sl) {
+    off = __ldg(sptr + sl);
+    lmax = (__ldg(sptr + sl + 1) - off) >> 5;
+    wd = __ldg(wide + sl) != 0;
+    r = __ldg(perm + sl * 32 + lane);
+    load_chunk(0);
   };
   // the matrix is not written by the predecessor: its first chunk streams in while that drains
-  if (s < s1) {
-    off = __ldg(sptr + s);
-    lmax = (__ldg(sptr + s + 1) - off) >> 5;
-    load_chunk(0);
-  }
+  if (s < s1) start(s);
   pdl_wait();
   pdl_trigger();
   for (; s < s1; s += gridDim.x) {
+    const T *xb = wd ? x : x + (r > 0 ? r : 0);
     T sum = 0;
     for (int c0 = 0;; c0 += PF) {
 #pragma unroll
       for (int u = 0; u < PF; u++)
-        if (w + (c0 + u) * K < lmax) sum += cv[u] * __ldg(x + ci[u]);
+        if (w + (c0 + u) * K < lmax) sum += cv[u] * __ldg(xb + ci[u]);
       if (w + (c0 + PF) * K >= lmax) break;
       load_chunk(c0 + PF);
     }
     part[w][lane] = sum;
+    const int rr = r;
     const int sn = s + gridDim.x;
-    const int r = w == 0 ? __ldg(perm + s * 32 + lane) : -1;
-    if (sn < s1) {
-      // next slice's first chunk before the reduction
-      off = __ldg(sptr + sn);
-      lmax = (__ldg(sptr + sn + 1) - off) >> 5;
-      load_chunk(0);
-    }
+    if (sn < s1) start(sn);  // next slice's first chunk before the reduction
     __syncthreads();
     if (w == 0) {
 #pragma unroll
       for (int k = 1; k < K; k++) sum += part[k][lane];
-      if (r >= 0) y[r] = MODE ? __ldg(f + r) - sum : sum;
+      if (rr >= 0) y[rr] = MODE ? __ldg(f + rr) - sum : sum;
     }
     __syncthreads();
   }
@@ -217,52 +273,52 @@ __global__ void __launch_bounds__(32 * K) k_sell_mv(int s0, int s1, const int *_
 template <typename T, int K>
 __global__ void __launch_bounds__(32 * K) k_sell_gs(int s0, int s1, const int *__restrict__ perm,
                                                     const int *__restrict__ sptr, const int *__restrict__ col,
+                                                    const short *__restrict__ c16,
+                                                    const unsigned char *__restrict__ wide,
                                                     const T *__restrict__ val, const T *__restrict__ invd,
                                                     const T *__restrict__ f, T *x, T omega) {
   constexpr int GS_PF = sizeof(T) == 4 ? 16 : 8;  // column steps per chunk (registers)
   __shared__ T part[K][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int s = s0 + blockIdx.x;
-  int off = 0, lmax = 0;
+  int off = 0, lmax = 0, r = -1;
+  bool wd = false;
   int ci[GS_PF];
   T cv[GS_PF];
+  auto load_chunk = [&](int c0) {
+    const int j0 = w + c0 * K;
+    sell_load_cols<GS_PF, K>(wd, col, c16, off + 32 * j0 + lane, j0, lmax, ci);
+#pragma unroll
+    for (int u = 0; u < GS_PF; u++)
+      cv[u] = j0 + u * K < lmax ? __ldg(val + off + 32 * (j0 + u * K) + lane) : (T)0;
+  };
   auto prefetch = [&](int sl) {
     off = __ldg(sptr + sl);
     lmax = (__ldg(sptr + sl + 1) - off) >> 5;
-#pragma unroll
-    for (int u = 0; u < GS_PF; u++) {
-      const int j = w + u * K;
-      const bool in = j < lmax;
-      ci[u] = in ? __ldg(col + off + 32 * j + lane) : 0;
-      cv[u] = in ? __ldg(val + off + 32 * j + lane) : (T)0;
-    }
+    wd = __ldg(wide + sl) != 0;
+    r = __ldg(perm + sl * 32 + lane);
+    load_chunk(0);
   };
   if (s < s1) prefetch(s);
   pdl_wait();
   pdl_trigger();
   for (; s < s1; s += gridDim.x) {
+    const T *xb = wd ? x : x + (r > 0 ? r : 0);
     T sum = 0;
     // column steps in chunks of GS_PF: the gathers of a chunk go out, then the
     // next chunk's column / value loads, so a long row costs one latency per chunk
     for (int c0 = 0;; c0 += GS_PF) {
 #pragma unroll
       for (int u = 0; u < GS_PF; u++)
-        if (w + (c0 + u) * K < lmax) sum += cv[u] * x[ci[u]];
+        if (w + (c0 + u) * K < lmax) sum += cv[u] * xb[ci[u]];
       if (w + (c0 + GS_PF) * K >= lmax) break;
-#pragma unroll
-      for (int u = 0; u < GS_PF; u++) {
-        const int j = w + (c0 + GS_PF + u) * K;
-        const bool in = j < lmax;
-        ci[u] = in ? __ldg(col + off + 32 * j + lane) : 0;
-        cv[u] = in ? __ldg(val + off + 32 * j + lane) : (T)0;
-      }
+      load_chunk(c0 + GS_PF);
     }
     part[w][lane] = sum;
     __syncthreads();
     if (w == 0) {
 #pragma unroll
       for (int k = 1; k < K; k++) sum += part[k][lane];
-      const int r = __ldg(perm + s * 32 + lane);
       if (r >= 0) x[r] += omega * (__ldg(f + r) - sum) * __ldg(invd + s * 32 + lane);
     }
     __syncthreads();
@@ -294,8 +350,42 @@ __global__ void k_sell_copy_dirichlet(int Na, int N, const T *__restrict__ f, T 
   if (i < N) x[i] = f[i];
 }
 
+// y_r -= sum over the Dirichlet columns j of active row r of A_rj v_j (the
+// entries [dd_beg, row end) of the CSR row, FP64 values)
+template <typename T>
+__global__ void k_dirichlet_cols(int n, const int *__restrict__ rows, const int *__restrict__ beg,
+                                 const int *__restrict__ rp, const int *__restrict__ kc, const double *__restrict__ a,
+                                 const T *v, T *y) {
+  pdl_wait();
+  pdl_trigger();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int r = __ldg(rows + i);
+  double s = 0;
+  for (int k = __ldg(beg + i), e = __ldg(rp + r + 1); k < e; k++) s += __ldg(a + k) * (double)v[__ldg(kc + k)];
+  y[r] = (T)((double)y[r] - s);
+}
+
+template <typename T>
+int dirichlet_cols(cudaStream_t s, const Level &L, const T *v, T *y) {
+  if (L.n_dd == 0) return PMG_OK;
+  PMG_CUDA(launch_pdl(k_dirichlet_cols<T>, dim3((L.n_dd + 255) / 256), dim3(256), 0, s, L.n_dd,
+                      (const int *)L.dd_row.p, (const int *)L.dd_beg.p, (const int *)L.rowptr.p,
+                      (const int *)L.kcol.p, (const double *)L.A.p, v, y));
+  count_launches(1);
+  return PMG_OK;
+}
+template int dirichlet_cols<float>(cudaStream_t, const Level &, const float *, float *);
+template int dirichlet_cols<double>(cudaStream_t, const Level &, const double *, double *);
+
 static int slice_grid(int nslices, int num_sms, int k) {
-  int cap = num_sms * (256 / k);  // 64 resident warps per SM, 4 waves
+  // PMG_SELL_CTAS_PER_SM caps the grid (CTAs then loop over slices)
+  static int cps = -1;
+  if (cps < 0) {
+    const char *e = getenv("PMG_SELL_CTAS_PER_SM");
+    cps = e ? std::max(0, atoi(e)) : 0;
+  }
+  int cap = cps ? num_sms * cps : num_sms * (256 / k);  // default: 64 resident warps per SM, 4 waves
   return std::max(1, std::min(nslices, cap));
 }
 
@@ -314,8 +404,8 @@ template <typename T, int MODE, int K>
 static cudaError_t launch_mv(cudaStream_t s, const Level &L, const T *x, const T *f, T *y, int num_sms) {
   const int n = L.sell_nslices;
   return launch_pdl(k_sell_mv<T, MODE, K>, dim3(slice_grid(n, num_sms, K)), dim3(32 * K), 0, s, 0, n,
-                    (const int *)L.sell_perm.p, (const int *)L.sell_ptr.p, (const int *)L.sell_col.p, sell_val<T>(L),
-                    x, f, y);
+                    (const int *)L.sell_perm.p, (const int *)L.sell_ptr.p, (const int *)L.sell_col.p,
+                    (const short *)L.sell_c16.p, (const unsigned char *)L.sell_wide.p, sell_val<T>(L), x, f, y);
 }
 
 template <typename T>
@@ -353,8 +443,9 @@ int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, in
       cudaError_t e;
 #define PMG_GS(K_)                                                                                              \
   launch_pdl(k_sell_gs<T, K_>, dim3(slice_grid(s1 - s0, num_sms, K_)), dim3(32 * K_), 0, s, s0, s1,           \
-             (const int *)L.sell_perm.p, (const int *)L.sell_ptr.p, (const int *)L.sell_col.p, sell_val<T>(L),  \
-             sell_invd<T>(L), f, x, (T)omega)
+             (const int *)L.sell_perm.p, (const int *)L.sell_ptr.p, (const int *)L.sell_col.p,                   \
+             (const short *)L.sell_c16.p, (const unsigned char *)L.sell_wide.p, sell_val<T>(L), sell_invd<T>(L), \
+             f, x, (T)omega)
       e = k == 16 ? PMG_GS(16) : k == 8 ? PMG_GS(8) : k == 4 ? PMG_GS(4) : PMG_GS(2);
 #undef PMG_GS
       PMG_CUDA(e);

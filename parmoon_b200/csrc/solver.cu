@@ -379,6 +379,13 @@ static int vcycle(Handle &h, int i, bool learned) {
   Level &L = h.lv[i];
   using PT = Prec<T>;
   if (!learned && i >= 1 && i == h.cc_top) return coarse_cycle<T>(h, i);
+  // The solve copy of the matrix leaves out the active rows' Dirichlet
+  // columns: on the level the cycle enters, fold them into the right-hand
+  // side (f_a -= A_aD f_D; the smoother keeps x_D = f_D).  Coarser levels need
+  // nothing: the restriction writes 0 into their Dirichlet rows.  The dense
+  // coarse solve reads the full CSR rows itself.
+  if (i == (int)h.lv.size() - 1 && (i >= 1 || h.prm.coarse_smoother != PMG_COARSE_DIRECT))
+    PMG_TRY(dirichlet_cols<T>(s, L, PT::f(L), PT::f(L)));
   if (i == 0) {
     if (h.prm.coarse_smoother == PMG_COARSE_DIRECT) {
       PMG_CUDA(launch_pdl(k_coarse_rhs<T>, dim3((L.N * 32 + 255) / 256), dim3(256), 0, s, L.N, L.Na,
@@ -582,6 +589,7 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
 
   auto residual = [&](double *out_vec, double &nrm) -> int {
     PMG_TRY(sell_spmv<double>(s, F, h.sol.p, h.rhs.p, out_vec, 1, h.num_sms));
+    PMG_TRY(dirichlet_cols<double>(s, F, h.sol.p, out_vec));  // - A_aD x_D
     PMG_TRY(dot(h, out_vec, out_vec, N, sc));
     PMG_CUDA(cudaMemcpyAsync(hcol, sc, sizeof(double), cudaMemcpyDeviceToHost, s));
     PMG_CUDA(cudaStreamSynchronize(s));
@@ -620,6 +628,7 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
         vc_timed = true;
       }
       PMG_TRY(sell_spmv<double>(s, F, zi, nullptr, w, 0, h.num_sms));
+      PMG_TRY(dirichlet_cols<double>(s, F, zi, w));  // w = A z_i with the Dirichlet columns
       double *Hc = Hd + (size_t)i * (m + 1);
       for (int k = 0; k <= i; k++) {
         PMG_TRY(dot(h, w, V + (size_t)k * N, N, Hc + k));
