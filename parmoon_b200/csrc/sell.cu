@@ -378,15 +378,21 @@ int dirichlet_cols(cudaStream_t s, const Level &L, const T *v, T *y) {
 template int dirichlet_cols<float>(cudaStream_t, const Level &, const float *, float *);
 template int dirichlet_cols<double>(cudaStream_t, const Level &, const double *, double *);
 
+// grid of a SELL launch: one CTA per slice up to a cap, beyond which CTAs loop
+// over slices (loading the next slice's first chunk before the reduction).
+// Measured on the 64^3 Q2 finest level (K = 4): a full FP64 product is fastest
+// with one CTA per slice (0.298 ms against 0.319 ms at 64 CTAs per SM), FP32
+// at 128 CTAs per SM (0.203 / 0.212 ms); a colour sweep stays below the cap.
+// PMG_SELL_CTAS_PER_SM overrides the cap.
+template <typename T>
 static int slice_grid(int nslices, int num_sms, int k) {
-  // PMG_SELL_CTAS_PER_SM caps the grid (CTAs then loop over slices)
   static int cps = -1;
   if (cps < 0) {
     const char *e = getenv("PMG_SELL_CTAS_PER_SM");
     cps = e ? std::max(0, atoi(e)) : 0;
   }
-  int cap = cps ? num_sms * cps : num_sms * (256 / k);  // default: 64 resident warps per SM, 4 waves
-  return std::max(1, std::min(nslices, cap));
+  const long cap = cps ? (long)num_sms * cps : (long)num_sms * ((sizeof(T) == 8 ? 2048 : 512) / k);
+  return (int)std::max(1L, std::min((long)nslices, cap));
 }
 
 template <typename T>
@@ -403,7 +409,7 @@ static const T *sell_invd(const Level &L) {
 template <typename T, int MODE, int K>
 static cudaError_t launch_mv(cudaStream_t s, const Level &L, const T *x, const T *f, T *y, int num_sms) {
   const int n = L.sell_nslices;
-  return launch_pdl(k_sell_mv<T, MODE, K>, dim3(slice_grid(n, num_sms, K)), dim3(32 * K), 0, s, 0, n,
+  return launch_pdl(k_sell_mv<T, MODE, K>, dim3(slice_grid<T>(n, num_sms, K)), dim3(32 * K), 0, s, 0, n,
                     (const int *)L.sell_perm.p, (const int *)L.sell_ptr.p, (const int *)L.sell_col.p,
                     (const short *)L.sell_c16.p, (const unsigned char *)L.sell_wide.p, sell_val<T>(L), x, f, y);
 }
@@ -442,7 +448,7 @@ int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, in
       const int k = pick_k(s1 - s0, num_sms);
       cudaError_t e;
 #define PMG_GS(K_)                                                                                              \
-  launch_pdl(k_sell_gs<T, K_>, dim3(slice_grid(s1 - s0, num_sms, K_)), dim3(32 * K_), 0, s, s0, s1,           \
+  launch_pdl(k_sell_gs<T, K_>, dim3(slice_grid<T>(s1 - s0, num_sms, K_)), dim3(32 * K_), 0, s, s0, s1,           \
              (const int *)L.sell_perm.p, (const int *)L.sell_ptr.p, (const int *)L.sell_col.p,                   \
              (const short *)L.sell_c16.p, (const unsigned char *)L.sell_wide.p, sell_val<T>(L), sell_invd<T>(L), \
              f, x, (T)omega)

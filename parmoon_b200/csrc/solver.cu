@@ -630,11 +630,11 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
       PMG_TRY(sell_spmv<double>(s, F, zi, nullptr, w, 0, h.num_sms));
       PMG_TRY(dirichlet_cols<double>(s, F, zi, w));  // w = A z_i with the Dirichlet columns
       double *Hc = Hd + (size_t)i * (m + 1);
-      for (int k = 0; k <= i; k++) {
-        PMG_TRY(dot(h, w, V + (size_t)k * N, N, Hc + k));
-        PMG_TRY(axpy_dev(s, N, Hc + k, -1.0, V + (size_t)k * N, w));
-      }
-      PMG_TRY(dot(h, w, w, N, Hc + i + 1));
+      // modified Gram-Schmidt (FgmresIte.C): h_k = w.v_k, w -= h_k v_k for
+      // k = 0..i, then h_{i+1}^2 = w.w; each update fused with the next product
+      PMG_TRY(dot(h, w, V, N, Hc));
+      for (int k = 0; k <= i; k++)
+        PMG_TRY(mgs_step(h, N, Hc + k, V + (size_t)k * N, k < i ? V + (size_t)(k + 1) * N : w, w, Hc + k + 1));
       PMG_TRY(scale_by_inv_sqrt(s, N, Hc + i + 1, w, V + (size_t)(i + 1) * N));
       PMG_CUDA(cudaMemcpyAsync(hcol, Hc, sizeof(double) * (i + 2), cudaMemcpyDeviceToHost, s));
       PMG_CUDA(cudaStreamSynchronize(s));

@@ -257,6 +257,8 @@ constexpr int RED_THREADS = 512;
 // last block to finish adds the partials in index order (reproducible).
 __global__ void __launch_bounds__(RED_THREADS) k_dot(size_t n, const double *__restrict__ a, const double *__restrict__ b,
                                                      double *partial, unsigned int *counter, double *result) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ double sh[RED_THREADS / 32];
   __shared__ bool last;
   double s = 0;
@@ -288,8 +290,62 @@ __global__ void __launch_bounds__(RED_THREADS) k_dot(size_t n, const double *__r
   }
 }
 
+// One step of modified Gram-Schmidt fused with the next step's inner product:
+//   w -= h_k v_k  (h_k read from device memory),  *h_next = w . u
+// with u = v_{k+1}, or u = w for the squared norm after the last step.  The
+// same fixed-order two-level reduction as k_dot.
+__global__ void __launch_bounds__(RED_THREADS) k_mgs_step(size_t n, const double *__restrict__ hk,
+                                                          const double *__restrict__ vk, const double *u, double *w,
+                                                          double *partial, unsigned int *counter, double *h_next) {
+  pdl_wait();
+  pdl_trigger();
+  __shared__ double sh[RED_THREADS / 32];
+  __shared__ bool last;
+  const double al = *hk;
+  const bool self = u == w;
+  double s = 0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double wi = w[i] - al * __ldg(vk + i);
+    w[i] = wi;
+    s += wi * (self ? wi : u[i]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int q = 0; q < RED_THREADS / 32; q++) t += sh[q];
+    partial[blockIdx.x] = t;
+    __threadfence();
+    unsigned int prev = atomicAdd(counter, 1u);
+    last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x < 32) {
+    __threadfence();
+    double t = 0;
+    for (int q = threadIdx.x; q < (int)gridDim.x; q += 32) t += ((volatile double *)partial)[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) {
+      *h_next = t;
+      *counter = 0;
+    }
+  }
+}
+
+int mgs_step(Handle &h, size_t n, const double *hk_dev, const double *vk, const double *u, double *w, double *h_next) {
+  PMG_CUDA(launch_pdl(k_mgs_step, dim3(RED_BLOCKS), dim3(RED_THREADS), 0, h.stream, n, hk_dev, vk, u, w,
+                      h.red_partial.p, h.red_counter.p, h_next));
+  count_launches(1);
+  return PMG_OK;
+}
+
 int dot(Handle &h, const double *a, const double *b, size_t n, double *result_dev) {
-  k_dot<<<RED_BLOCKS, RED_THREADS, 0, h.stream>>>(n, a, b, h.red_partial.p, h.red_counter.p, result_dev); count_launches(1);
+  PMG_CUDA(launch_pdl(k_dot, dim3(RED_BLOCKS), dim3(RED_THREADS), 0, h.stream, n, a, b, h.red_partial.p,
+                      h.red_counter.p, result_dev));
+  count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
@@ -310,13 +366,16 @@ int axpy_dev(cudaStream_t s, size_t n, const double *alpha_dev, double sign, con
 // y = x / sqrt(*nrm2)   (nrm2 = squared norm in device memory; 0 -> y = 0)
 __global__ void k_scale_inv_sqrt(size_t n, const double *__restrict__ nrm2, const double *__restrict__ x,
                                  double *__restrict__ y) {
+  pdl_wait();
+  pdl_trigger();
   double nv = sqrt(*nrm2);
   double s = nv > 0 ? 1.0 / nv : 0.0;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     y[i] = x[i] * s;
 }
 int scale_by_inv_sqrt(cudaStream_t s, size_t n, const double *nrm2_dev, const double *x, double *y) {
-  k_scale_inv_sqrt<<<vec_grid(n), 256, 0, s>>>(n, nrm2_dev, x, y); count_launches(1);
+  PMG_CUDA(launch_pdl(k_scale_inv_sqrt, dim3(vec_grid(n)), dim3(256), 0, s, n, nrm2_dev, x, y));
+  count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
