@@ -47,9 +47,10 @@ N_FULL = (2 * N_CELLS + 1) ** 3
 N_SAMPLE = (2 * 32 + 1) ** 3
 # DRAM traffic of one FP32 SSOR step per algorithmic byte, measured with ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum over the 54 colour launches of
-# one step on the finest level of the 48^3 Q2 hierarchy: 1.103 GB for 0.901 GB
-# algorithmic); the step's traffic scales with the rows and entries it sweeps
-SSOR_TRAFFIC_PER_BYTE = 1.103201 / 0.901129
+# one step on the finest level of the 48^3 Q2 hierarchy: 0.858 GB for 0.663 GB
+# algorithmic -- FP32 values, 16-bit column deltas, slice pointers, lane rows,
+# vectors); the step's traffic scales with the rows and entries it sweeps
+SSOR_TRAFFIC_PER_BYTE = 0.857810 / 0.662910
 
 
 def peaks():
