@@ -89,6 +89,16 @@ def _c_f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
+def _out_f64(out, n):
+    """A caller-provided output array (contiguous float64 of length n, used in
+    place), or a new one."""
+    if out is None:
+        return np.empty(n)
+    if not (isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous and out.size == n):
+        raise ValueError("out must be a contiguous float64 array of the level's size")
+    return out
+
+
 def default_params(**kw):
     p = Params()
     lib().pmg_default_params(ctypes.byref(p))
@@ -202,8 +212,9 @@ class Handle:
         entries = _c_f64(entries)
         _check(lib().pmg_set_matrix(self.h, _i(level), _i(which), _ptr(entries)))
 
-    def get_rhs(self, level):
-        r = np.empty(self.sizes[level][0])
+    def get_rhs(self, level, out=None):
+        """Right-hand side of a level; `out` (contiguous float64, e.g. page-locked) receives it if given."""
+        r = _out_f64(out, self.sizes[level][0])
         _check(lib().pmg_get_rhs(self.h, _i(level), _ptr(r)))
         return r
 
@@ -238,11 +249,14 @@ class Handle:
         _check(lib().pmg_restrict(self.h, _i(level), _ptr(fine), _ptr(coarse)))
         return coarse
 
-    def solve(self, sol=None, rhs=None, raise_on_error=True):
-        """FGMRES + V-cycle on the finest level; returns (solution or None, stats, status)."""
+    def solve(self, sol=None, rhs=None, raise_on_error=True, inplace=False):
+        """FGMRES + V-cycle on the finest level; returns (solution or None, stats, status).
+
+        sol is the start vector; with inplace=True a contiguous float64 `sol`
+        (e.g. page-locked) receives the solution itself instead of a copy."""
         st = SolveStats()
         if sol is not None:
-            sol = np.array(sol, dtype=np.float64)
+            sol = _out_f64(sol, len(sol)) if inplace else np.array(sol, dtype=np.float64)
         rhs = None if rhs is None else _c_f64(rhs)
         rc = lib().pmg_solve(self.h, _ptr(sol), _ptr(rhs), ctypes.byref(st))
         if raise_on_error and rc != OK:
@@ -297,8 +311,8 @@ class Handle:
         """z = MG(v) on device vectors of the finest level."""
         _check(lib().pmg_vcycle(self.h, _p(v_ptr), _p(z_ptr)))
 
-    def get_solution(self):
-        x = np.empty(self.sizes[-1][0])
+    def get_solution(self, out=None):
+        x = _out_f64(out, self.sizes[-1][0])
         _check(lib().pmg_get_solution(self.h, _ptr(x)))
         return x
 
