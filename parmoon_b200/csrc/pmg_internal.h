@@ -256,7 +256,8 @@ int sell_values(Handle &h, Level &L);
 template <typename T>
 int sell_spmv(cudaStream_t s, const Level &L, const T *x, const T *f, T *y, int mode, int num_sms);
 template <typename T>
-int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, int num_sms, bool dirichlet = true);
+int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, int num_sms, bool dirichlet = true,
+              bool after_ssor = false, bool skip_repeats = false);
 // y_a -= A_aD v_D over the active rows' Dirichlet columns (the part of A the
 // solve copy leaves out)
 template <typename T>

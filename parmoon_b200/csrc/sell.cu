@@ -431,17 +431,25 @@ template int sell_spmv<float>(cudaStream_t, const Level &, const float *, const 
 template int sell_spmv<double>(cudaStream_t, const Level &, const double *, const double *, double *, int, int);
 
 // one SSOR step: Dirichlet rows from f (the sweeps never change them, so only the
-// first step of a level visit needs it), forward over the colours, backward
+// first step of a level visit needs it), forward over the colours, backward.
+// skip_repeats (with omega = 1): a Gauss-Seidel update of a colour directly
+// after an update of the same colour leaves x unchanged (the colour's rows have
+// zero residual and are not coupled to each other), so the backward sweep
+// starts with the second-to-last colour and, when the previous step was also
+// an SSOR step of this level (after_ssor), the forward sweep with colour 1.
 template <typename T>
-int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, int num_sms, bool dirichlet) {
+int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, int num_sms, bool dirichlet,
+              bool after_ssor, bool skip_repeats) {
   const int nc = (int)L.sell_group.size() - 2;  // active colours
   const int nd = L.N - L.Na;
   if (nd > 0 && dirichlet) {
     PMG_CUDA(launch_pdl(k_sell_copy_dirichlet<T>, dim3((nd + 255) / 256), dim3(256), 0, s, L.Na, L.N, f, x));
     count_launches(1);
   }
+  const bool skip = skip_repeats && omega == 1.0;
   for (int pass = 0; pass < 2; pass++)
     for (int cc = 0; cc < nc; cc++) {
+      if (skip && cc == 0 && (pass == 1 || after_ssor)) continue;
       const int c = pass == 0 ? cc : nc - 1 - cc;
       const int s0 = L.sell_group[c], s1 = L.sell_group[c + 1];
       if (s1 <= s0) continue;
@@ -460,7 +468,7 @@ int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, in
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
-template int sell_ssor<float>(cudaStream_t, const Level &, const float *, float *, double, int, bool);
-template int sell_ssor<double>(cudaStream_t, const Level &, const double *, double *, double, int, bool);
+template int sell_ssor<float>(cudaStream_t, const Level &, const float *, float *, double, int, bool, bool, bool);
+template int sell_ssor<double>(cudaStream_t, const Level &, const double *, double *, double, int, bool, bool, bool);
 
 }  // namespace pmg

@@ -366,9 +366,10 @@ template <> struct Prec<float> {
 
 // one pre/post smoothing step: SSOR, or x += omega W (f - A x) with the learned stencil
 template <typename T>
-static int smooth_step(Handle &h, Level &L, bool learned, bool first = true) {
+static int smooth_step(Handle &h, Level &L, bool learned, bool first, bool after_ssor) {
   using PT = Prec<T>;
-  if (!learned) return sell_ssor<T>(h.stream, L, PT::f(L), PT::x(L), h.prm.smooth_omega, h.num_sms, first);
+  if (!learned)
+    return sell_ssor<T>(h.stream, L, PT::f(L), PT::x(L), h.prm.smooth_omega, h.num_sms, first, after_ssor, true);
   PMG_TRY(sell_spmv<T>(h.stream, L, PT::x(L), PT::f(L), PT::d(L), 1, h.num_sms));
   return learned_smooth<T>(h.stream, L, PT::d(L), PT::x(L), h.prm.smooth_omega);
 }
@@ -400,19 +401,19 @@ static int vcycle(Handle &h, int i, bool learned) {
       PMG_CUDA(cudaGetLastError());
     } else {
       int it = h.prm.coarse_maxit > 0 ? h.prm.coarse_maxit : 1;
-      for (int k = 0; k < it; k++) PMG_TRY(smooth_step<T>(h, L, learned, k == 0));
+      for (int k = 0; k < it; k++) PMG_TRY(smooth_step<T>(h, L, learned, k == 0, k > 0));
     }
     return PMG_OK;
   }
   Level &C = h.lv[i - 1];
   const int pre = (learned && h.prm.learned_steps > 0) ? h.prm.learned_steps : h.prm.pre_smooth;
   const int post = (learned && h.prm.learned_steps > 0) ? h.prm.learned_steps : h.prm.post_smooth;
-  for (int k = 0; k < pre; k++) PMG_TRY(smooth_step<T>(h, L, learned, k == 0));
+  for (int k = 0; k < pre; k++) PMG_TRY(smooth_step<T>(h, L, learned, k == 0, k > 0));
   PMG_TRY(sell_spmv<T>(s, L, PT::x(L), PT::f(L), PT::d(L), 1, h.num_sms));
   PMG_TRY(restrict_defect<T>(s, L, C, PT::R(L), PT::d(L), PT::f(C), PT::x(C)));  // also x_C := 0
   PMG_TRY(vcycle<T>(h, i - 1, learned));
   PMG_TRY(prolongate_add<T>(s, L, PT::P(L), PT::x(C), PT::x(L), h.prm.gmg_damp));
-  for (int k = 0; k < post; k++) PMG_TRY(smooth_step<T>(h, L, learned, pre == 0 && k == 0));
+  for (int k = 0; k < post; k++) PMG_TRY(smooth_step<T>(h, L, learned, pre == 0 && k == 0, k > 0));
   return PMG_OK;
 }
 
