@@ -174,6 +174,36 @@ def ssor(rp, kc, a, f, x, active_bound, omega=1.0, colors=None, n_colors=0):
     return x
 
 
+def _levels(levels, keep):
+    """ctypes array of orc_level for a list (coarse..fine) of dicts rp, kc, a, N, Na,
+    [colors, n_colors], [P=(rp,col,val)]; the arrays it points to are kept in `keep`."""
+    arr = (Level * len(levels))()
+    for i, L in enumerate(levels):
+        arr[i].N, arr[i].Na = L["N"], L["Na"]
+        for name in ("rp", "kc", "a"):
+            keep.append(L[name])
+        arr[i].rp, arr[i].kc, arr[i].a = _ptr(L["rp"]), _ptr(L["kc"]), _ptr(L["a"])
+        if L.get("colors") is not None:
+            arr[i].colors, arr[i].n_colors = _ptr(L["colors"]), L["n_colors"]
+            keep.append(L["colors"])
+        if L.get("P") is not None:
+            prp, pcol, pval = L["P"]
+            arr[i].prp, arr[i].pcol, arr[i].pval = _ptr(prp), _ptr(pcol), _ptr(pval)
+            keep += [prp, pcol, pval]
+    return arr
+
+
+def mg_apply(levels, v, pre=2, post=2, coarse_maxit=10, coarse_red=0.1, omega=1.0, damp=1.0, coarse_direct=True):
+    """z = MG(v): one V-cycle from zero with the Dirichlet part of v (MultiGridScaIte.C:89-130)."""
+    keep = []
+    arr = _levels(levels, keep)
+    mp = MGParams(pre, post, coarse_maxit, coarse_red, omega, damp, int(coarse_direct))
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    z = np.zeros(levels[-1]["N"])
+    lib().orc_mg_apply(_i(len(levels)), arr, ctypes.byref(mp), _ptr(v), _ptr(z))
+    return z
+
+
 def fgmres_mg(levels, rhs, sol0=None, pre=2, post=2, coarse_maxit=10, coarse_red=0.1, omega=1.0, damp=1.0,
               coarse_direct=False, red=1e-10, res_min=0.0, maxit=1000, restart=20, div=1e10,
               reference_restart_rule=False):
