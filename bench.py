@@ -69,20 +69,23 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms.  The sampler
+    starts before the warm-up (nvidia-smi takes a moment to begin) and only the
+    samples whose timestamps fall inside the marked timed window are kept."""
 
     def __init__(self, gpu_index):
         self.idx = gpu_index
         self.rows = []
         self.proc = None
+        self.window = None
 
     def __enter__(self):
-        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+        q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                                          "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
@@ -90,13 +93,23 @@ class ClockSampler:
         return self
 
     def _read(self):
+        import datetime
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) == 7:
-                self.rows.append(parts)
+            if len(parts) == 8:
+                try:
+                    ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                except ValueError:
+                    continue
+                self.rows.append([ts] + parts[1:])
+
+    def mark(self, t0, t1):
+        """The timed window, in time.time() seconds."""
+        self.window = (t0, t1)
 
     def __exit__(self, *a):
         if self.proc:
+            time.sleep(0.1)  # let the sample that closes the window arrive
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -104,14 +117,18 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        rows = self.rows
+        if self.window is not None:
+            t0, t1 = self.window
+            rows = [r for r in rows if t0 - 0.025 <= r[0] <= t1 + 0.025]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[3 + k].lower() == "active"})
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[4 + k].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(rows), "interval_ms": 50}
 
 
 def max_over_ranks(value, dist, device=None):
@@ -207,18 +224,19 @@ def bench_ours(args, rank, world, dist):
         _, st, rc = h.solve()
         return t_asm + st.seconds, st, rc
 
-    for _ in range(args.warmup):
-        step()
-    sync()
-    cnt0 = ctypes.c_ulonglong()
-    lib.pmg_launch_count(ctypes.byref(cnt0))
-    times, stats = [], []
-    nvtx = None
-    if os.environ.get("BENCH_NVTX") == "1":  # marks the timed region for profiler range filters
-        import torch
-        nvtx = torch.cuda.nvtx
-        nvtx.range_push("timed_step")
     with ClockSampler(local) as clk:
+        for _ in range(args.warmup):
+            step()
+        sync()
+        cnt0 = ctypes.c_ulonglong()
+        lib.pmg_launch_count(ctypes.byref(cnt0))
+        times, stats = [], []
+        nvtx = None
+        if os.environ.get("BENCH_NVTX") == "1":  # marks the timed region for profiler range filters
+            import torch
+            nvtx = torch.cuda.nvtx
+            nvtx.range_push("timed_step")
+        t_epoch = time.time()
         t_wall = time.perf_counter()
         for _ in range(args.steps):
             t, st, rc = step()
@@ -227,8 +245,9 @@ def bench_ours(args, rank, world, dist):
             times.append(t)
             stats.append(st)
         t_wall = time.perf_counter() - t_wall
-    if nvtx is not None:
-        nvtx.range_pop()
+        clk.mark(t_epoch, time.time())
+        if nvtx is not None:
+            nvtx.range_pop()
     cnt1 = ctypes.c_ulonglong()
     lib.pmg_launch_count(ctypes.byref(cnt1))
     sync()
