@@ -166,3 +166,16 @@ def test_create_rejects_bad_level_counts():
     p = P.default_params()
     for n in (0, -1, 17):
         assert P.lib().pmg_create(ctypes.byref(h), n, ctypes.byref(p)) == P.ERR_ARG
+
+
+def test_output_arrays_are_checked_and_used_in_place():
+    """The binding's caller-provided outputs (get_rhs/get_solution out=, solve
+    inplace=True: page-locked host buffers) are used as given, and anything
+    the C ABI could not write into directly is rejected before any call."""
+    import parmoon_b200 as P
+    a = np.zeros(10)
+    assert P._out_f64(a, 10) is a
+    assert P._out_f64(None, 7).shape == (7,)
+    for bad in (np.zeros(9), np.zeros(10, dtype=np.float32), np.zeros(20)[::2], [0.0] * 10):
+        with pytest.raises(ValueError):
+            P._out_f64(bad, 10)
