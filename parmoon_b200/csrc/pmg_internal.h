@@ -237,12 +237,10 @@ template <typename T>
 int prolongate_add(cudaStream_t s, const Level &Lf, const T *pval, const T *xc, T *xf, double damp);
 int compute_invdiag(cudaStream_t s, Level &L);
 int convert_f64_f32(cudaStream_t s, const double *a, float *b, size_t n);
-int convert_f32_f64(cudaStream_t s, const float *a, double *b, size_t n);
 int copy_dirichlet(cudaStream_t s, int Na, int N, const double *f, double *x);
 int dot(Handle &h, const double *a, const double *b, size_t n, double *result_dev);
 // w -= (*hk_dev) vk, then *h_next = w . u (u = w: the squared norm)
 int mgs_step(Handle &h, size_t n, const double *hk_dev, const double *vk, const double *u, double *w, double *h_next);
-int axpy_dev(cudaStream_t s, size_t n, const double *alpha_dev, double sign, const double *x, double *y);
 int scale_by_inv_sqrt(cudaStream_t s, size_t n, const double *nrm2_dev, const double *x, double *y);
 int fill(cudaStream_t s, double *x, double v, size_t n);
 template <typename T>

@@ -224,21 +224,12 @@ __global__ void k_f64_to_f32(size_t n, const double *__restrict__ a, float *__re
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     b[i] = (float)a[i];
 }
-__global__ void k_f32_to_f64(size_t n, const float *__restrict__ a, double *__restrict__ b) {
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    b[i] = (double)a[i];
-}
 static int vec_grid(size_t n) {
   size_t b = (n + 255) / 256;
   return (int)(b < 148 * 16 ? (b ? b : 1) : 148 * 16);
 }
 int convert_f64_f32(cudaStream_t s, const double *a, float *b, size_t n) {
   k_f64_to_f32<<<vec_grid(n), 256, 0, s>>>(n, a, b); count_launches(1);
-  PMG_CUDA(cudaGetLastError());
-  return PMG_OK;
-}
-int convert_f32_f64(cudaStream_t s, const float *a, double *b, size_t n) {
-  k_f32_to_f64<<<vec_grid(n), 256, 0, s>>>(n, a, b); count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
@@ -346,19 +337,6 @@ int dot(Handle &h, const double *a, const double *b, size_t n, double *result_de
   PMG_CUDA(launch_pdl(k_dot, dim3(RED_BLOCKS), dim3(RED_THREADS), 0, h.stream, n, a, b, h.red_partial.p,
                       h.red_counter.p, result_dev));
   count_launches(1);
-  PMG_CUDA(cudaGetLastError());
-  return PMG_OK;
-}
-
-// y += sign * alpha * x   (alpha read from device memory)
-__global__ void k_axpy_dev(size_t n, const double *__restrict__ alpha, double sign, const double *__restrict__ x,
-                           double *__restrict__ y) {
-  double al = sign * (*alpha);
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    y[i] += al * x[i];
-}
-int axpy_dev(cudaStream_t s, size_t n, const double *alpha_dev, double sign, const double *x, double *y) {
-  k_axpy_dev<<<vec_grid(n), 256, 0, s>>>(n, alpha_dev, sign, x, y); count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
