@@ -118,3 +118,33 @@ def test_reference_build_reproduces_recorded_log():
         row = np.argmin(np.abs(log[:, 0] - t))
         assert abs(log[row, 0] - t) < 1e-6
         assert abs(float(f"{l2:.6e}") - log[row, 1]) <= 1e-12
+
+
+def test_oracle_vcycle_is_a_contracting_linear_operator(oracle):
+    """The oracle's single V-cycle (the reference for tests/test_gpu_vcycle.py)
+    is linear in its input and, on the SPD Q1 Laplace problem (16^3, 3
+    levels), reduces the error of A e = v in the energy norm by at least half
+    with SSOR(2,2) and the dense coarse solve."""
+    import parmoon_b200 as P
+    co = oracle.make_coeff(kind=1, eps=1.0)
+    levels = P.struct_hierarchy(1, 16, 3)
+    olev = []
+    for l, L in enumerate(levels):
+        a, _ = oracle.assemble(1, L["elem_dof"], L["cell_vert"], L["N"], L["active_bound"], L["rowptr"], L["kcol"],
+                               1, co)
+        d = dict(N=L["N"], Na=L["active_bound"], rp=L["rowptr"], kc=L["kcol"], a=a, colors=L["colors"],
+                 n_colors=L["n_colors"])
+        if l > 0:
+            d["P"] = L["P"]
+        olev.append(d)
+    F = olev[-1]
+    rng = np.random.default_rng(11)
+    u, w = rng.standard_normal(F["N"]), rng.standard_normal(F["N"])
+    zu, zw, zs = oracle.mg_apply(olev, u), oracle.mg_apply(olev, w), oracle.mg_apply(olev, 2.0 * u - 3.0 * w)
+    assert np.max(np.abs(zs - (2.0 * zu - 3.0 * zw))) <= 1e-12 * np.max(np.abs(zs))
+    e = np.zeros(F["N"])
+    e[:F["Na"]] = rng.standard_normal(F["Na"])
+    v = oracle.spmv(F["rp"], F["kc"], F["a"], e)
+    err = e - oracle.mg_apply(olev, v)
+    Aa = lambda x: oracle.spmv(F["rp"], F["kc"], F["a"], x)
+    assert float(err @ Aa(err)) <= 0.25 * float(e @ Aa(e))
