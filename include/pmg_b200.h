@@ -75,9 +75,12 @@ typedef struct pmg_coeff_desc {
 /* POD mirror of the TDatabase::ParamDB fields the reference reads on this
  * path (src/General/Database.C:660-780).  pmg_default_params fills the
  * reference defaults. */
-#define PMG_SMOOTHER_JACOBI   1
-#define PMG_SMOOTHER_SSOR     3
+#define PMG_SMOOTHER_JACOBI   1  /* TMGLevel3D::Jacobi (src/FE/MGLevel3D.C:469-560) */
+#define PMG_SMOOTHER_SOR      2  /* TMGLevel3D::SOR (src/FE/MGLevel3D.C:280-361), rows in colour order */
+#define PMG_SMOOTHER_SSOR     3  /* TMGLevel3D::SSOR (src/FE/MGLevel3D.C:363-467), rows in colour order */
 #define PMG_SMOOTHER_LEARNED 30  /* stencil-network smoother with SSOR fallback */
+#define PMG_COARSE_JACOBI     1
+#define PMG_COARSE_SOR        2
 #define PMG_COARSE_SSOR       3
 #define PMG_COARSE_DIRECT    17  /* dense LU of the coarsest level (reference: SolveExact) */
 #define PMG_PREC_FP64         0  /* V-cycle stores level matrices and vectors in FP64 */
@@ -107,6 +110,10 @@ typedef struct pmg_params {
     int    learned_steps;      /* learned-smoother steps per pre/post phase (0: pre_smooth / post_smooth) */
     int    assembly_kernel;    /* 0: automatic (cells with space-constant eps, b, c use the reference-matrix
                                   kernel), 1: per-quadrature-point kernel for every coefficient kind */
+    int    slc_all;            /* SC_STEP_LENGTH_CONTROL_ALL_SCALAR: step-length control on every level >= 1 */
+    int    slc_fine;           /* SC_STEP_LENGTH_CONTROL_FINE_SCALAR: step-length control on the finest level
+                                  (TMultiGrid3D::Cycle, src/FE/MultiGrid3D.C:517-523, 655-663;
+                                  TMGLevel3D::StepLengthControl, src/FE/MGLevel3D.C:908-961) */
 } pmg_params;
 
 typedef struct pmg_solve_stats {
@@ -129,7 +136,9 @@ const char *pmg_last_error(void);
 int         pmg_device_count(int *n);
 
 /* TSystemCD3D ctor (src/System/SystemCD3D.C:62-227): creates the per-level
- * containers; levels are numbered 0 (coarsest) .. n_levels-1 (finest). */
+ * containers; levels are numbered 0 (coarsest) .. n_levels-1 (finest).
+ * pmg_create and pmg_set_params reject parameter sets this library does not
+ * build (unknown smoother codes, out-of-range counts) with PMG_ERR_ARG. */
 int pmg_create(pmg_handle *h, int n_levels, const pmg_params *p);
 int pmg_destroy(pmg_handle h);
 int pmg_set_params(pmg_handle h, const pmg_params *p);
@@ -230,6 +239,11 @@ int pmg_defect(pmg_handle h, int level, const double *x, const double *b, double
  * device-wide wait.  x, b, r and norm are DEVICE pointers (N, N, N and 1
  * doubles) the caller owns; the call computes r = b - A x and norm = |r|_2 on
  * the level's FP64 matrix and returns after the handle's stream is done.
+ * The kernels run on the handle's own stream, which is not ordered after the
+ * caller's streams: x and b must be completely written on the device before
+ * the call (synchronize the stream that produced them, or the device), and r
+ * and norm may be read on any stream once the call has returned.  The level
+ * must hold an assembled (or pmg_set_matrix) matrix, else PMG_ERR_STATE.
  * Its only scratch is a fixed array inside the library (512 KiB per GPU,
  * kept until the process exits), shared by all calls: calls that overlap on
  * the GPU race on it.  The first call on a device looks up the array's

@@ -35,7 +35,8 @@ class Level(ctypes.Structure):
 
 class MGParams(ctypes.Structure):
     _fields_ = [("pre", _i), ("post", _i), ("coarse_maxit", _i), ("coarse_red", _d),
-                ("omega", _d), ("damp", _d), ("coarse_direct", _i)]
+                ("omega", _d), ("damp", _d), ("coarse_direct", _i), ("smoother", _i), ("coarse_smoother", _i),
+                ("slc_all", _i), ("slc_fine", _i)]
 
 
 def build(force=False):
@@ -166,6 +167,22 @@ def spmv(rp, kc, a, x):
     return y
 
 
+def sor(rp, kc, a, f, x, active_bound, omega=1.0, colors=None, n_colors=0):
+    x = np.array(x, dtype=np.float64)
+    N = rp.size - 1
+    lib().orc_sor(_i(N), _i(active_bound), _ptr(rp), _ptr(kc), _ptr(a), _ptr(np.ascontiguousarray(f, dtype=np.float64)),
+                  _ptr(x), _d(omega), _i(n_colors), _ptr(colors))
+    return x
+
+
+def jacobi(rp, kc, a, f, x, active_bound, omega=1.0):
+    x = np.array(x, dtype=np.float64)
+    N = rp.size - 1
+    lib().orc_jacobi(_i(N), _i(active_bound), _ptr(rp), _ptr(kc), _ptr(a),
+                     _ptr(np.ascontiguousarray(f, dtype=np.float64)), _ptr(x), _d(omega))
+    return x
+
+
 def ssor(rp, kc, a, f, x, active_bound, omega=1.0, colors=None, n_colors=0):
     x = np.array(x, dtype=np.float64)
     N = rp.size - 1
@@ -193,11 +210,14 @@ def _levels(levels, keep):
     return arr
 
 
-def mg_apply(levels, v, pre=2, post=2, coarse_maxit=10, coarse_red=0.1, omega=1.0, damp=1.0, coarse_direct=True):
-    """z = MG(v): one V-cycle from zero with the Dirichlet part of v (MultiGridScaIte.C:89-130)."""
+def mg_apply(levels, v, pre=2, post=2, coarse_maxit=10, coarse_red=0.1, omega=1.0, damp=1.0, coarse_direct=True,
+             smoother=3, coarse_smoother=3, slc_all=False, slc_fine=False):
+    """z = MG(v): one V-cycle from zero with the Dirichlet part of v (MultiGridScaIte.C:89-130).
+    smoother / coarse_smoother: 1 Jacobi, 2 SOR, 3 SSOR; slc_*: step-length control."""
     keep = []
     arr = _levels(levels, keep)
-    mp = MGParams(pre, post, coarse_maxit, coarse_red, omega, damp, int(coarse_direct))
+    mp = MGParams(pre, post, coarse_maxit, coarse_red, omega, damp, int(coarse_direct), smoother, coarse_smoother,
+                  int(slc_all), int(slc_fine))
     v = np.ascontiguousarray(v, dtype=np.float64)
     z = np.zeros(levels[-1]["N"])
     lib().orc_mg_apply(_i(len(levels)), arr, ctypes.byref(mp), _ptr(v), _ptr(z))
@@ -206,7 +226,7 @@ def mg_apply(levels, v, pre=2, post=2, coarse_maxit=10, coarse_red=0.1, omega=1.
 
 def fgmres_mg(levels, rhs, sol0=None, pre=2, post=2, coarse_maxit=10, coarse_red=0.1, omega=1.0, damp=1.0,
               coarse_direct=False, red=1e-10, res_min=0.0, maxit=1000, restart=20, div=1e10,
-              reference_restart_rule=False):
+              reference_restart_rule=False, smoother=3, coarse_smoother=3, slc_all=False, slc_fine=False):
     """levels: list (coarse..fine) of dicts rp, kc, a, N, Na, [colors, n_colors], [P=(rp,col,val)]."""
     keep = []
     arr = (Level * len(levels))()
@@ -222,7 +242,8 @@ def fgmres_mg(levels, rhs, sol0=None, pre=2, post=2, coarse_maxit=10, coarse_red
             prp, pcol, pval = L["P"]
             arr[i].prp, arr[i].pcol, arr[i].pval = _ptr(prp), _ptr(pcol), _ptr(pval)
             keep += [prp, pcol, pval]
-    mp = MGParams(pre, post, coarse_maxit, coarse_red, omega, damp, int(coarse_direct))
+    mp = MGParams(pre, post, coarse_maxit, coarse_red, omega, damp, int(coarse_direct), smoother, coarse_smoother,
+                  int(slc_all), int(slc_fine))
     N = levels[-1]["N"]
     sol = np.zeros(N) if sol0 is None else np.array(sol0, dtype=np.float64)
     rhs = np.ascontiguousarray(rhs, dtype=np.float64)

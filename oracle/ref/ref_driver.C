@@ -24,6 +24,8 @@
 //   problem(laplace|cdsupg|cdgal) eps(1) b1 b2 b3 (0) linear_quad(1)
 //   disc(1=Galerkin,2=SUPG) restart(20) red(1e-10) maxit(1000) smoother(3)
 //   pre(2) post(2) coarse_smoother(3) coarse_maxit(10) dump(1) solve(1)
+//   omega(1) slc_all(0) slc_fine(0) dump_solution(0)
+//   repeat(0) warmup(0) start_file (timing mode of the benchmark)
 //   tau, endtime (tcd3d) geo(Wuerfel|SixTetras) order 12 = P2 on tetrahedra
 #include <Domain.h>
 #include <Database.h>
@@ -66,6 +68,8 @@ static int N_Rhs = 1, RhsSpace[1] = {0};
 #include <map>
 #include <vector>
 #include <chrono>
+#include <thread>
+#include <sys/time.h>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -84,6 +88,14 @@ static std::string opts(const char *k, const char *d)
   auto it = g_opt.find(k);
   return it == g_opt.end() ? std::string(d) : it->second;
 }
+// seconds since the Unix epoch (a clock shared by concurrent processes)
+static double epoch()
+{
+  struct timeval tv;
+  gettimeofday(&tv, NULL);
+  return tv.tv_sec + 1e-6 * tv.tv_usec;
+}
+
 static double wall()
 {
   return std::chrono::duration<double>(
@@ -205,11 +217,11 @@ static void set_solver_params()
   TDatabase::ParamDB->SC_GMRES_RESTART = (int)optd("restart", 20);
   TDatabase::ParamDB->SC_FLEXIBLE_KRYLOV_SPACE_SOLVER = 1;
   TDatabase::ParamDB->SC_MG_CYCLE_SCALAR = 1;
-  TDatabase::ParamDB->SC_SMOOTH_DAMP_FACTOR_SCALAR = 1.0;
-  TDatabase::ParamDB->SC_SMOOTH_DAMP_FACTOR_FINE_SCALAR = 1.0;
+  TDatabase::ParamDB->SC_SMOOTH_DAMP_FACTOR_SCALAR = optd("omega", 1.0);
+  TDatabase::ParamDB->SC_SMOOTH_DAMP_FACTOR_FINE_SCALAR = optd("omega", 1.0);
   TDatabase::ParamDB->SC_GMG_DAMP_FACTOR_SCALAR = 1.0;
-  TDatabase::ParamDB->SC_STEP_LENGTH_CONTROL_ALL_SCALAR = 0;
-  TDatabase::ParamDB->SC_STEP_LENGTH_CONTROL_FINE_SCALAR = 0;
+  TDatabase::ParamDB->SC_STEP_LENGTH_CONTROL_ALL_SCALAR = (int)optd("slc_all", 0);
+  TDatabase::ParamDB->SC_STEP_LENGTH_CONTROL_FINE_SCALAR = (int)optd("slc_fine", 0);
   TDatabase::ParamDB->SC_MG_TYPE_SCALAR = 0;
   TDatabase::ParamDB->SC_VERBOSE = 0;
 }
@@ -335,8 +347,12 @@ static int run_cd3d()
                                N_Matrices, N_Rhs, RowSpace, ColumnSpace, RhsSpace,
                                BilinearAssemble, CoeffsFn, NULL);
 
-  double Parameters[2] = {1.0, 1.0};
+  // Parameters[0] is the smoothers' damping (and the step-length fallback),
+  // as TSystemCD3D sets them (SystemCD3D.C:175-177)
+  double Parameters[2] = {optd("omega", 1.0), optd("omega", 1.0)};
   TMultiGrid3D *MG = new TMultiGrid3D(1, 2, Parameters);
+  // step-length control keeps the old iterate and defect in aux vectors 2, 3
+  const int n_aux = (optd("slc_all", 0) != 0 || optd("slc_fine", 0) != 0) ? 4 : 2;
   std::vector<TAssembleMat3D *> asmb(levels);
   BoundCondFunct3D *BC[1] = {BoundCondFn};
   BoundValueFunct3D *BV[1] = {BoundValueFn};
@@ -348,8 +364,74 @@ static int run_cd3d()
     TAuxParam3D *aux = new TAuxParam3D(1, 0, 0, 0, fesp, NULL, NULL, NULL, NULL, 0, NULL);
     asmb[i] = new TAssembleMat3D(1, fesp, 1, SQ, 0, NULL, 1, RHS, ferhs, form, BC, BV, aux);
     asmb[i]->Init();
-    TMGLevel3D *lev = new TMGLevel3D(i, L[i].A, L[i].rhs, L[i].sol, 2, NULL);
+    TMGLevel3D *lev = new TMGLevel3D(i, L[i].A, L[i].rhs, L[i].sol, n_aux, NULL);
     MG->AddLevel(lev);
+  }
+
+  // repeat=R: the timing mode of the benchmark.  The hierarchy above is built
+  // once; then warmup=W untimed and R timed repetitions of Assemble() of all
+  // levels + Solve() from the zero start vector, each bracketed as
+  // CD3D_ParMooN.C:418-463 brackets them.  With start_file given, the timed
+  // repetitions begin once that file exists (concurrent copies start together).
+  const int repeat = (int)optd("repeat", 0);
+  if (repeat > 0)
+  {
+    const int warm = (int)optd("warmup", 0);
+    const std::string start = opts("start_file", "");
+    const int top = levels - 1, N = L[top].N;
+    TItMethod *prec = new TMultiGridScaIte(MatVect_Scalar, Defect_Scalar, NULL, 0, N, MG, 1);
+    TItMethod *itm = new TFgmresIte(MatVect_Scalar, Defect_Scalar, prec, 0, N, 1);
+    TSquareMatrix *sq[1] = {L[top].A};
+    std::vector<double> d(N);
+    for (int k = 0; k < warm + repeat; k++)
+    {
+      if (k == warm)
+      {
+        if (!start.empty())
+        {
+          dumpScalar("ready_epoch", epoch());
+          fflush(g_meta);
+          // bounded wait (one hour) for the go signal
+          for (int w = 0; w < 360000; w++)
+          {
+            FILE *f = fopen(start.c_str(), "r");
+            if (f) { fclose(f); break; }
+            std::this_thread::sleep_for(std::chrono::milliseconds(10));
+          }
+        }
+        dumpScalar("timed_start_epoch", epoch());
+      }
+      for (int i = 0; i < levels; i++) memset(L[i].sol, 0, sizeof(double) * L[i].N);
+      double a = wall();
+      for (int i = 0; i < levels; i++)
+      {
+        asmb[i]->Reset();
+        asmb[i]->Assemble3D();
+        int Na = L[i].space->GetActiveBound();
+        memcpy(L[i].sol + Na, L[i].rhs + Na, (L[i].N - Na) * sizeof(double));
+      }
+      double b = wall();
+      double r0, r1;
+      ScalarDefect(L[top].A, L[top].sol, L[top].rhs, d.data(), r0);
+      int iters = itm->Iterate(sq, NULL, L[top].sol, L[top].rhs);
+      double c = wall();
+      ScalarDefect(L[top].A, L[top].sol, L[top].rhs, d.data(), r1);
+      if (k >= warm)
+      {
+        char key[64];
+        int j = k - warm;
+        snprintf(key, sizeof key, "R%d_t_assemble", j); dumpScalar(key, b - a);
+        snprintf(key, sizeof key, "R%d_t_solve", j); dumpScalar(key, c - b);
+        snprintf(key, sizeof key, "R%d_iterations", j); dumpScalar(key, iters);
+        snprintf(key, sizeof key, "R%d_rel_res", j); dumpScalar(key, r1 / r0);
+      }
+      printf("repetition %d: assemble %.3f s, solve %.3f s, %d iterations, |r|/|r0| = %.3e\n", k, b - a, c - b,
+             iters, r1 / r0);
+      fflush(stdout);
+    }
+    dumpScalar("timed_end_epoch", epoch());
+    dumpScalar("fine_nnz", L[top].A->GetN_Entries());
+    return 0;
   }
 
   // Assemble: TSystemCD3D::Assemble (SystemCD3D.C:340-365), timed per level
@@ -419,7 +501,16 @@ static int run_cd3d()
     dumpScalar("t_solve", t_solve);
     dumpScalar("res0", r0);
     dumpScalar("res_final", r1);
-    if (do_dump) dump("solution", isol.data(), N, "f8");
+    if (do_dump || optd("dump_solution", 0) != 0) dump("solution", isol.data(), N, "f8");
+    if (!do_dump && optd("dump_solution", 0) != 0)
+    {
+      // the finest level's dof positions, to compare with another dof numbering
+      std::vector<double> x(N), y(N), z(N), xyz((size_t)N * 3);
+      L[levels - 1].space->GetDOFPosition(x.data(), y.data(), z.data());
+      for (int i = 0; i < N; i++) { xyz[3 * i] = x[i]; xyz[3 * i + 1] = y[i]; xyz[3 * i + 2] = z[i]; }
+      dump("fine_dof_xyz", xyz.data(), (long)xyz.size(), "f8");
+      dumpScalar("fine_active_bound", L[levels - 1].space->GetActiveBound());
+    }
     printf("solve: %d iterations, %.3f s, |r|/|r0| = %.3e\n", iters, t_solve, r1 / r0);
   }
   for (int i = 0; i < levels; i++)

@@ -25,8 +25,8 @@ ERR = {-1: "ARG", -2: "CUDA", -3: "STATE", -4: "NOT_CONVERGED", -5: "DIVERGED", 
 Q1_HEX, Q2_HEX, P1_TET, P2_TET = 1, 2, 11, 12
 FORM_GALERKIN, FORM_SUPG, FORM_MASS, FORM_MASS_SUPG, FORM_STIFF_SUPG = 1, 2, 3, 4, 5
 COEF_CONST, COEF_SINE_RHS, COEF_LOGNORMAL, COEF_CURL_FOURIER, COEF_ROTATING, COEF_AMC, COEF_TABLE = range(7)
-SMOOTHER_JACOBI, SMOOTHER_SSOR, SMOOTHER_LEARNED = 1, 3, 30
-COARSE_SSOR, COARSE_DIRECT = 3, 17
+SMOOTHER_JACOBI, SMOOTHER_SOR, SMOOTHER_SSOR, SMOOTHER_LEARNED = 1, 2, 3, 30
+COARSE_JACOBI, COARSE_SOR, COARSE_SSOR, COARSE_DIRECT = 1, 2, 3, 17
 PREC_FP64, PREC_FP32 = 0, 1
 
 _i, _d, _p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
@@ -38,7 +38,7 @@ class Params(ctypes.Structure):
                 ("lin_red", _d), ("lin_res_min", _d), ("lin_maxit", _i), ("restart", _i), ("div_factor", _d),
                 ("precision", _i), ("sdfem_type", _i), ("poly_degree", _i), ("delta0", _d),
                 ("reference_restart_rule", _i), ("problem_linear", _i), ("learned_steps", _i),
-                ("assembly_kernel", _i)]
+                ("assembly_kernel", _i), ("slc_all", _i), ("slc_fine", _i)]
 
 
 class CoeffDesc(ctypes.Structure):

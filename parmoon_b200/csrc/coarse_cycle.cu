@@ -529,6 +529,11 @@ int coarse_cycle_top(Handle &h) {
     if (mode && colon != std::string::npos) max_rows = atol(v.c_str() + colon + 1);
   }
   if (mode == 0) return 0;
+  // the one-launch cycle runs SSOR pre/post steps without step-length control
+  if (h.prm.smoother != PMG_SMOOTHER_SSOR && h.prm.smoother != PMG_SMOOTHER_LEARNED) return 0;
+  if (h.prm.slc_all) return 0;
+  // (and the dense coarsest solve; the iterative one checks its residual)
+  if (h.prm.coarse_smoother != PMG_COARSE_DIRECT) return 0;
   const size_t vb = h.prm.precision == PMG_PREC_FP32 ? sizeof(float) : sizeof(double);
   size_t bytes = 0;
   int top = 0;

@@ -107,19 +107,13 @@ using namespace pmg;
 extern "C" int pmg_defect_noalloc(pmg_handle hh, int level, const double *x, const double *b, double *r,
                                   double *norm) {
   Handle *h = reinterpret_cast<Handle *>(hh);
-  if (!h || level < 0 || level >= (int)h->lv.size()) {
-    set_error("pmg_defect_noalloc: bad handle or level");
-    return PMG_ERR_ARG;
-  }
+  // the same checks as pmg_defect: an existing level whose matrix holds values
+  PMG_TRY(check_matrix(h, level, "pmg_defect_noalloc"));
   if (!x || !b || !r || !norm) {
     set_error("pmg_defect_noalloc: x, b, r and norm must be device pointers");
     return PMG_ERR_ARG;
   }
   Level &L = h->lv[level];
-  if (!L.has_csr || !L.A.p) {
-    set_error("pmg_defect_noalloc: the level has no matrix");
-    return PMG_ERR_STATE;
-  }
   if ((long)L.N > (long)PMG_NOALLOC_MAX_ROWS) {
     set_error("pmg_defect_noalloc: the level has more rows than PMG_NOALLOC_MAX_ROWS (16,777,216); "
               "use pmg_defect");

@@ -47,6 +47,49 @@ static int check_level(Handle *h, int level) {
   return PMG_OK;
 }
 
+int check_matrix(Handle *h, int level, const char *who) {
+  PMG_TRY(check_level(h, level));
+  const Level &L = h->lv[level];
+  if (!L.has_csr || !L.assembled) {
+    set_error(std::string(who) + ": the level has no matrix values yet (pmg_assemble or pmg_set_matrix first)");
+    return PMG_ERR_STATE;
+  }
+  return PMG_OK;
+}
+
+// The parameter sets this library builds (the reference exits or falls back
+// to SOR on unknown smoother codes, MultiGrid3D.C:210-213; here they are
+// rejected).
+static int validate_params(const pmg_params *p) {
+  auto bad = [](const char *m) { set_error(std::string("params: ") + m); return PMG_ERR_ARG; };
+  const int sm = p->smoother;
+  if (sm != PMG_SMOOTHER_JACOBI && sm != PMG_SMOOTHER_SOR && sm != PMG_SMOOTHER_SSOR && sm != PMG_SMOOTHER_LEARNED)
+    return bad("smoother must be PMG_SMOOTHER_JACOBI, _SOR, _SSOR or _LEARNED");
+  const int cs = p->coarse_smoother;
+  if (cs != PMG_COARSE_JACOBI && cs != PMG_COARSE_SOR && cs != PMG_COARSE_SSOR && cs != PMG_COARSE_DIRECT)
+    return bad("coarse_smoother must be PMG_COARSE_JACOBI, _SOR, _SSOR or _DIRECT");
+  if (p->pre_smooth < 0 || p->pre_smooth > 64 || p->post_smooth < 0 || p->post_smooth > 64)
+    return bad("pre_smooth / post_smooth must be in [0, 64]");
+  if (p->coarse_maxit < 1 || p->coarse_maxit > 100000) return bad("coarse_maxit must be in [1, 100000]");
+  if (p->restart < 1 || p->restart > 60) return bad("restart must be in [1,60]");
+  if (p->lin_maxit < 1) return bad("lin_maxit must be >= 1");
+  if (p->precision != PMG_PREC_FP64 && p->precision != PMG_PREC_FP32) return bad("precision must be PMG_PREC_FP64 or _FP32");
+  if (p->assembly_kernel != 0 && p->assembly_kernel != 1) return bad("assembly_kernel must be 0 or 1");
+  if (p->problem_linear != 0 && p->problem_linear != 1) return bad("problem_linear must be 0 or 1");
+  if (p->reference_restart_rule != 0 && p->reference_restart_rule != 1) return bad("reference_restart_rule must be 0 or 1");
+  if ((p->slc_all != 0 && p->slc_all != 1) || (p->slc_fine != 0 && p->slc_fine != 1)) return bad("slc_all / slc_fine must be 0 or 1");
+  if (p->learned_steps < 0 || p->learned_steps > 64) return bad("learned_steps must be in [0, 64]");
+  if (p->poly_degree < 0) return bad("poly_degree must be >= 0");
+  const double pos[] = {p->smooth_omega, p->div_factor};
+  for (double v : pos)
+    if (!std::isfinite(v) || v <= 0.0) return bad("smooth_omega and div_factor must be finite and positive");
+  const double nonneg[] = {p->coarse_red, p->lin_red, p->lin_res_min, p->delta0};
+  for (double v : nonneg)
+    if (!std::isfinite(v) || v < 0.0) return bad("coarse_red, lin_red, lin_res_min and delta0 must be finite and >= 0");
+  if (!std::isfinite(p->gmg_damp)) return bad("gmg_damp must be finite");
+  return PMG_OK;
+}
+
 // greedy colouring of the cells so that no two cells of one colour share a dof
 static std::vector<int> color_cells(int n_cells, int nloc, const int *ed, int N, int &ncolors) {
   std::vector<int> cnt(N + 1, 0);
@@ -150,8 +193,11 @@ int pmg_create(pmg_handle *out, int n_levels, const pmg_params *p) {
     set_error("pmg_create: no CUDA device");
     return PMG_ERR_CUDA;
   }
+  pmg_params prm;
+  if (p) prm = *p; else pmg_default_params(&prm);
+  PMG_TRY(validate_params(&prm));
   Handle *h = new Handle();
-  if (p) h->prm = *p; else pmg_default_params(&h->prm);
+  h->prm = prm;
   h->lv.resize(n_levels);
   cudaGetDevice(&h->device);
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
@@ -195,13 +241,13 @@ int pmg_destroy(pmg_handle hh) {
 int pmg_set_params(pmg_handle hh, const pmg_params *p) {
   Handle *h = H(hh);
   if (!h || !p) return PMG_ERR_ARG;
-  if (p->restart < 1 || p->restart > 60) { set_error("restart must be in [1,60]"); return PMG_ERR_ARG; }
-  if (p->assembly_kernel != 0 && p->assembly_kernel != 1) { set_error("assembly_kernel must be 0 or 1"); return PMG_ERR_ARG; }
+  PMG_TRY(validate_params(p));
   bool graph_shape = p->precision != h->prm.precision || p->pre_smooth != h->prm.pre_smooth ||
                      p->post_smooth != h->prm.post_smooth || p->coarse_smoother != h->prm.coarse_smoother ||
                      p->smooth_omega != h->prm.smooth_omega || p->gmg_damp != h->prm.gmg_damp ||
                      p->coarse_maxit != h->prm.coarse_maxit || p->smoother != h->prm.smoother ||
-                     p->learned_steps != h->prm.learned_steps;
+                     p->learned_steps != h->prm.learned_steps || p->slc_all != h->prm.slc_all ||
+                     p->slc_fine != h->prm.slc_fine;
   h->prm = *p;
   if (graph_shape) invalidate_graphs(h);
   return PMG_OK;
@@ -511,7 +557,7 @@ static int with_pinned(Handle *h, size_t n) {
 
 int pmg_matvec(pmg_handle hh, int level, const double *x, double *y) {
   Handle *h = H(hh);
-  PMG_TRY(check_level(h, level));
+  PMG_TRY(check_matrix(h, level, "pmg_matvec"));
   if (!x || !y) return PMG_ERR_ARG;
   Level &L = h->lv[level];
   DBuf<double> dx, dy;
@@ -525,7 +571,7 @@ int pmg_matvec(pmg_handle hh, int level, const double *x, double *y) {
 
 int pmg_defect(pmg_handle hh, int level, const double *x, const double *b, double *r, double *norm) {
   Handle *h = H(hh);
-  PMG_TRY(check_level(h, level));
+  PMG_TRY(check_matrix(h, level, "pmg_defect"));
   if (!x || !b || !r) return PMG_ERR_ARG;
   Level &L = h->lv[level];
   DBuf<double> dx, db, dr, dn;
@@ -545,7 +591,7 @@ int pmg_defect(pmg_handle hh, int level, const double *x, const double *b, doubl
 
 int pmg_ssor(pmg_handle hh, int level, const double *rhs, double *sol, int n_sweeps) {
   Handle *h = H(hh);
-  PMG_TRY(check_level(h, level));
+  PMG_TRY(check_matrix(h, level, "pmg_ssor"));
   if (!rhs || !sol || n_sweeps < 0) return PMG_ERR_ARG;
   Level &L = h->lv[level];
   PMG_TRY(level_invdiag(h->stream, L, h->d_flags.p));

@@ -126,6 +126,10 @@ struct Level {
   // work vectors of the V-cycle (FP64 and FP32)
   DBuf<double> x64, f64, d64;
   DBuf<float> x32, f32, d32;
+  // step-length control (old iterate, old defect, A times the update) and the
+  // Jacobi step's new iterate
+  DBuf<double> slc64[3], jac64;
+  DBuf<float> slc32[3], jac32;
   // lattice and stencil of the learned smoother (learned.cu)
   int lat_n[3] = {0, 0, 0};
   DBuf<int> dof_ijk, lat_dof, tpos;
@@ -183,11 +187,13 @@ struct Handle {
   // coarsest-level dense inverse (FP64)
   DBuf<double> coarse_lu, coarse_inv, coarse_t;  // active block: LU, inverse; reduced rhs
   DBuf<int> coarse_piv, coarse_perm;
+  DBuf<int> coarse_cptr;  // colour pointers of the coarsest level's rows (iterative coarse solve)
   bool coarse_ready = false;
   // FGMRES workspace
   int krylov_n = 0, krylov_restart = 0;
   DBuf<double> V, Z, w, sol, rhs, H, scal;
   DBuf<double> red_partial;
+  DBuf<double> slc_part;  // step-length control: block partials of (d0, y), (y, y) and alpha
   DBuf<unsigned int> red_counter;
   double *h_H = nullptr;  // pinned mirror of one Hessenberg column
   // error flags written by kernels (slot lookups, non-finite values)
@@ -218,6 +224,9 @@ struct Handle {
   DBuf<double> tcd_fold;
   bool sol_preset = false, tcd_active = false;
 };
+
+// the level exists and its system matrix holds values (assembled or set)
+int check_matrix(Handle *h, int level, const char *who);
 
 // ------------------------------------------------------------- kernels (assemble.cu)
 int build_slot_map(Handle &h, Level &L);
@@ -255,7 +264,10 @@ template <typename T>
 int sell_spmv(cudaStream_t s, const Level &L, const T *x, const T *f, T *y, int mode, int num_sms);
 template <typename T>
 int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, int num_sms, bool dirichlet = true,
-              bool after_ssor = false, bool skip_repeats = false);
+              bool after_ssor = false, bool skip_repeats = false, bool forward_only = false);
+// one damped Jacobi step; tmp: a level-sized work vector other than x and f
+template <typename T>
+int sell_jacobi(cudaStream_t s, const Level &L, const T *f, T *x, T *tmp, double omega, int num_sms, bool dirichlet);
 // y_a -= A_aD v_D over the active rows' Dirichlet columns (the part of A the
 // solve copy leaves out)
 template <typename T>

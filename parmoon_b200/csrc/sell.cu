@@ -207,14 +207,17 @@ __device__ __forceinline__ void sell_load_cols(bool wd, const int *__restrict__ 
   }
 }
 
-// y = A x (MODE 0) or d = f - A x (MODE 1) over slices [s0, s1)
+// y = A x (MODE 0), d = f - A x (MODE 1), or the Jacobi update
+// y = x + omega (f - A x) / a_rr (MODE 2, into a vector other than x) over
+// slices [s0, s1)
 template <typename T, int MODE, int K>
 __global__ void __launch_bounds__(32 * K) k_sell_mv(int s0, int s1, const int *__restrict__ perm,
                                                     const int *__restrict__ sptr, const int *__restrict__ col,
                                                     const short *__restrict__ c16,
                                                     const unsigned char *__restrict__ wide,
                                                     const T *__restrict__ val, const T *__restrict__ x,
-                                                    const T *__restrict__ f, T *__restrict__ y) {
+                                                    const T *__restrict__ f, T *__restrict__ y,
+                                                    const T *__restrict__ invd, T omega) {
   constexpr int PF = sizeof(T) == 4 ? 16 : 8;  // column steps per chunk
   __shared__ T part[K][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -258,7 +261,10 @@ __global__ void __launch_bounds__(32 * K) k_sell_mv(int s0, int s1, const int *_
     if (w == 0) {
 #pragma unroll
       for (int k = 1; k < K; k++) sum += part[k][lane];
-      if (rr >= 0) y[rr] = MODE ? __ldg(f + rr) - sum : sum;
+      if (rr >= 0) {
+        if (MODE == 2) y[rr] = __ldg(x + rr) + omega * (__ldg(f + rr) - sum) * __ldg(invd + s * 32 + lane);
+        else y[rr] = MODE ? __ldg(f + rr) - sum : sum;
+      }
     }
     __syncthreads();
   }
@@ -407,11 +413,13 @@ static const T *sell_invd(const Level &L) {
 }
 
 template <typename T, int MODE, int K>
-static cudaError_t launch_mv(cudaStream_t s, const Level &L, const T *x, const T *f, T *y, int num_sms) {
-  const int n = L.sell_nslices;
+static cudaError_t launch_mv(cudaStream_t s, const Level &L, const T *x, const T *f, T *y, int num_sms, int n = -1,
+                             T omega = 0) {
+  if (n < 0) n = L.sell_nslices;
   return launch_pdl(k_sell_mv<T, MODE, K>, dim3(slice_grid<T>(n, num_sms, K)), dim3(32 * K), 0, s, 0, n,
                     (const int *)L.sell_perm.p, (const int *)L.sell_ptr.p, (const int *)L.sell_col.p,
-                    (const short *)L.sell_c16.p, (const unsigned char *)L.sell_wide.p, sell_val<T>(L), x, f, y);
+                    (const short *)L.sell_c16.p, (const unsigned char *)L.sell_wide.p, sell_val<T>(L), x, f, y,
+                    sell_invd<T>(L), omega);
 }
 
 template <typename T>
@@ -430,6 +438,42 @@ int sell_spmv(cudaStream_t s, const Level &L, const T *x, const T *f, T *y, int 
 template int sell_spmv<float>(cudaStream_t, const Level &, const float *, const float *, float *, int, int);
 template int sell_spmv<double>(cudaStream_t, const Level &, const double *, const double *, double *, int, int);
 
+template <typename T>
+__global__ void k_copy_active(int Na, const T *__restrict__ src, T *__restrict__ dst) {
+  pdl_wait();
+  pdl_trigger();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < Na) dst[i] = src[i];
+}
+
+// One damped Jacobi step (TMGLevel3D::Jacobi, MGLevel3D.C:469-560):
+// x_D := f_D, then x_a := x_a + omega (f_a - A_a x) / a_aa from the previous
+// iterate, written into `tmp` (the active rows' slices are the colour groups)
+// and copied back.  In the V-cycle x_D = f_D already holds when a level's
+// smoothing starts, so the previous Dirichlet values the reference keeps in
+// its aux copy equal the new ones.
+template <typename T>
+int sell_jacobi(cudaStream_t s, const Level &L, const T *f, T *x, T *tmp, double omega, int num_sms, bool dirichlet) {
+  const int nc = (int)L.sell_group.size() - 2;
+  const int nd = L.N - L.Na;
+  if (nd > 0 && dirichlet) {
+    PMG_CUDA(launch_pdl(k_sell_copy_dirichlet<T>, dim3((nd + 255) / 256), dim3(256), 0, s, L.Na, L.N, f, x));
+    count_launches(1);
+  }
+  const int na_slices = L.sell_group[nc];
+  if (na_slices <= 0) return PMG_OK;
+  const int k = std::max(4, pick_k(na_slices, num_sms));
+  cudaError_t e = k == 16 ? launch_mv<T, 2, 16>(s, L, x, f, tmp, num_sms, na_slices, (T)omega)
+                : k == 8  ? launch_mv<T, 2, 8>(s, L, x, f, tmp, num_sms, na_slices, (T)omega)
+                          : launch_mv<T, 2, 4>(s, L, x, f, tmp, num_sms, na_slices, (T)omega);
+  PMG_CUDA(e);
+  PMG_CUDA(launch_pdl(k_copy_active<T>, dim3((L.Na + 255) / 256), dim3(256), 0, s, L.Na, (const T *)tmp, x));
+  count_launches(2);
+  return PMG_OK;
+}
+template int sell_jacobi<float>(cudaStream_t, const Level &, const float *, float *, float *, double, int, bool);
+template int sell_jacobi<double>(cudaStream_t, const Level &, const double *, double *, double *, double, int, bool);
+
 // one SSOR step: Dirichlet rows from f (the sweeps never change them, so only the
 // first step of a level visit needs it), forward over the colours, backward.
 // skip_repeats (with omega = 1): a Gauss-Seidel update of a colour directly
@@ -437,17 +481,19 @@ template int sell_spmv<double>(cudaStream_t, const Level &, const double *, cons
 // zero residual and are not coupled to each other), so the backward sweep
 // starts with the second-to-last colour and, when the previous step was also
 // an SSOR step of this level (after_ssor), the forward sweep with colour 1.
+// forward_only: one SOR step (TMGLevel3D::SOR, MGLevel3D.C:280-361): the
+// forward sweep over the colours alone.
 template <typename T>
 int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, int num_sms, bool dirichlet,
-              bool after_ssor, bool skip_repeats) {
+              bool after_ssor, bool skip_repeats, bool forward_only) {
   const int nc = (int)L.sell_group.size() - 2;  // active colours
   const int nd = L.N - L.Na;
   if (nd > 0 && dirichlet) {
     PMG_CUDA(launch_pdl(k_sell_copy_dirichlet<T>, dim3((nd + 255) / 256), dim3(256), 0, s, L.Na, L.N, f, x));
     count_launches(1);
   }
-  const bool skip = skip_repeats && omega == 1.0;
-  for (int pass = 0; pass < 2; pass++)
+  const bool skip = skip_repeats && omega == 1.0 && !forward_only;
+  for (int pass = 0; pass < (forward_only ? 1 : 2); pass++)
     for (int cc = 0; cc < nc; cc++) {
       if (skip && cc == 0 && (pass == 1 || after_ssor)) continue;
       const int c = pass == 0 ? cc : nc - 1 - cc;
@@ -468,7 +514,8 @@ int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, in
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
-template int sell_ssor<float>(cudaStream_t, const Level &, const float *, float *, double, int, bool, bool, bool);
-template int sell_ssor<double>(cudaStream_t, const Level &, const double *, double *, double, int, bool, bool, bool);
+template int sell_ssor<float>(cudaStream_t, const Level &, const float *, float *, double, int, bool, bool, bool, bool);
+template int sell_ssor<double>(cudaStream_t, const Level &, const double *, double *, double, int, bool, bool, bool,
+                               bool);
 
 }  // namespace pmg

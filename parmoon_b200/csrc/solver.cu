@@ -353,6 +353,8 @@ template <> struct Prec<double> {
   static double *d(Level &L) { return L.d64.p; }
   static const double *P(const Level &L) { return L.pval.p; }
   static const double *R(const Level &L) { return L.rval.p; }
+  static double *slc(Level &L, int k) { return L.slc64[k].p; }
+  static double *jac(Level &L) { return L.jac64.p; }
 };
 template <> struct Prec<float> {
   static const float *A(const Level &L) { return L.A32.p; }
@@ -362,16 +364,201 @@ template <> struct Prec<float> {
   static float *d(Level &L) { return L.d32.p; }
   static const float *P(const Level &L) { return L.pval32.p; }
   static const float *R(const Level &L) { return L.rval32.p; }
+  static float *slc(Level &L, int k) { return L.slc32[k].p; }
+  static float *jac(Level &L) { return L.jac32.p; }
 };
 
-// one pre/post smoothing step: SSOR, or x += omega W (f - A x) with the learned stencil
+// one pre/post smoothing step (TMultiGrid3D::Smooth, MultiGrid3D.C:117-446):
+// Jacobi, SOR or SSOR in colour order (kind = PMG_SMOOTHER_*), or
+// x += omega W (f - A x) with the learned stencil
 template <typename T>
-static int smooth_step(Handle &h, Level &L, bool learned, bool first, bool after_ssor) {
+static int smooth_step(Handle &h, Level &L, bool learned, bool first, bool after_ssor, int kind) {
   using PT = Prec<T>;
-  if (!learned)
-    return sell_ssor<T>(h.stream, L, PT::f(L), PT::x(L), h.prm.smooth_omega, h.num_sms, first, after_ssor, true);
-  PMG_TRY(sell_spmv<T>(h.stream, L, PT::x(L), PT::f(L), PT::d(L), 1, h.num_sms));
-  return learned_smooth<T>(h.stream, L, PT::d(L), PT::x(L), h.prm.smooth_omega);
+  if (learned) {
+    PMG_TRY(sell_spmv<T>(h.stream, L, PT::x(L), PT::f(L), PT::d(L), 1, h.num_sms));
+    return learned_smooth<T>(h.stream, L, PT::d(L), PT::x(L), h.prm.smooth_omega);
+  }
+  if (kind == PMG_SMOOTHER_JACOBI)
+    return sell_jacobi<T>(h.stream, L, PT::f(L), PT::x(L), PT::jac(L), h.prm.smooth_omega, h.num_sms, first);
+  if (kind == PMG_SMOOTHER_SOR)
+    return sell_ssor<T>(h.stream, L, PT::f(L), PT::x(L), h.prm.smooth_omega, h.num_sms, first, false, false, true);
+  return sell_ssor<T>(h.stream, L, PT::f(L), PT::x(L), h.prm.smooth_omega, h.num_sms, first, after_ssor, true);
+}
+
+// Step-length control (TMGLevel3D::StepLengthControl, MGLevel3D.C:908-961,
+// applied by TMultiGrid3D::Cycle, MultiGrid3D.C:655-663): with u0 and d0 the
+// iterate and defect before the pre-smoothing and y = A (u - u0),
+// alpha = (d0, y) / (y, y) -- the omega parameter when (y, y) = 0 or
+// |alpha| < 0.1 -- and u := u0 + alpha (u - u0).  Computed on the device
+// (block partials in a fixed order, one block for alpha), so the cycle stays
+// one captured graph.
+template <typename T>
+__global__ void k_slc_diff(int n, const T *__restrict__ x, const T *__restrict__ x0, T *__restrict__ dx) {
+  pdl_wait();
+  pdl_trigger();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dx[i] = x[i] - x0[i];
+}
+constexpr int SLC_BLOCKS = 592;
+template <typename T>
+__global__ void __launch_bounds__(256) k_slc_partials(int n, const T *__restrict__ d0, const T *__restrict__ y,
+                                                      double *__restrict__ part) {
+  pdl_wait();
+  pdl_trigger();
+  __shared__ double sa[256], sb[256];
+  double a = 0, b = 0;
+  for (int i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) {
+    const double yi = (double)y[i];
+    a += (double)d0[i] * yi;
+    b += yi * yi;
+  }
+  sa[threadIdx.x] = a;
+  sb[threadIdx.x] = b;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) { sa[threadIdx.x] += sa[threadIdx.x + o]; sb[threadIdx.x] += sb[threadIdx.x + o]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { part[2 * blockIdx.x] = sa[0]; part[2 * blockIdx.x + 1] = sb[0]; }
+}
+__global__ void __launch_bounds__(256) k_slc_alpha(int nb, const double *__restrict__ part, double omega,
+                                                   double *__restrict__ alpha) {
+  pdl_wait();
+  pdl_trigger();
+  __shared__ double sa[256], sb[256];
+  double a = 0, b = 0;
+  for (int k = threadIdx.x; k < nb; k += 256) { a += part[2 * k]; b += part[2 * k + 1]; }
+  sa[threadIdx.x] = a;
+  sb[threadIdx.x] = b;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) { sa[threadIdx.x] += sa[threadIdx.x + o]; sb[threadIdx.x] += sb[threadIdx.x + o]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double al = sb[0] > 0 ? sa[0] / sb[0] : omega;
+    if (fabs(al) < 0.1) al = omega;
+    *alpha = al;
+  }
+}
+template <typename T>
+__global__ void k_slc_apply(int n, const double *__restrict__ alpha, const T *__restrict__ x0, T *__restrict__ x) {
+  pdl_wait();
+  pdl_trigger();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const double a = *alpha;
+    x[i] = (T)((double)x0[i] + a * ((double)x[i] - (double)x0[i]));
+  }
+}
+
+template <typename T>
+static int slc_begin(Handle &h, Level &L) {
+  using PT = Prec<T>;
+  PMG_TRY(sell_spmv<T>(h.stream, L, PT::x(L), PT::f(L), PT::slc(L, 1), 1, h.num_sms));
+  PMG_CUDA(cudaMemcpyAsync(PT::slc(L, 0), PT::x(L), sizeof(T) * L.N, cudaMemcpyDeviceToDevice, h.stream));
+  return PMG_OK;
+}
+
+template <typename T>
+static int slc_end(Handle &h, Level &L) {
+  using PT = Prec<T>;
+  cudaStream_t s = h.stream;
+  const int nb = (L.N + 255) / 256, np = std::min(SLC_BLOCKS, nb);
+  PMG_CUDA(launch_pdl(k_slc_diff<T>, dim3(nb), dim3(256), 0, s, L.N, (const T *)PT::x(L), (const T *)PT::slc(L, 0),
+                      PT::d(L)));
+  PMG_TRY(sell_spmv<T>(s, L, PT::d(L), PT::f(L), PT::slc(L, 2), 0, h.num_sms));
+  PMG_CUDA(launch_pdl(k_slc_partials<T>, dim3(np), dim3(256), 0, s, L.N, (const T *)PT::slc(L, 1),
+                      (const T *)PT::slc(L, 2), h.slc_part.p));
+  PMG_CUDA(launch_pdl(k_slc_alpha, dim3(1), dim3(256), 0, s, np, (const double *)h.slc_part.p, h.prm.smooth_omega,
+                      h.slc_part.p + 2 * SLC_BLOCKS));
+  PMG_CUDA(launch_pdl(k_slc_apply<T>, dim3(nb), dim3(256), 0, s, L.N, (const double *)(h.slc_part.p + 2 * SLC_BLOCKS),
+                      (const T *)PT::slc(L, 0), PT::x(L)));
+  count_launches(4);
+  return PMG_OK;
+}
+
+// Iterative coarsest-level solve, the CoarseSmooth branch of
+// TMultiGrid3D::Smooth (MultiGrid3D.C:262-330): res = |f - A x|; while
+// res > coarse_red * res_0 and it < coarse_maxit: one Jacobi / SOR / SSOR step
+// (rows in colour order), res = |f - A x|.  The coarsest level is small
+// (hundreds to a few thousand rows), so one block runs the whole loop --
+// colour by colour with block barriers, the residual by a block reduction --
+// on the FP64 CSR values, and the loop's exit test stays on the device.
+__device__ __forceinline__ double cc_block_sum(double v, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0;
+  for (int k = 0; k < nw; k++) t += sh[k];
+  return t;
+}
+
+template <typename T>
+__device__ __forceinline__ double coarse_row_sum(int i, const int *__restrict__ rp, const int *__restrict__ kc,
+                                                 const double *__restrict__ a, const T *x, double &diag) {
+  double s = 0;
+  diag = 1.0;
+  for (int k = rp[i]; k < rp[i + 1]; k++) {
+    const int c = kc[k];
+    if (c == i) diag = a[k];
+    else s += a[k] * (double)x[c];
+  }
+  return s;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) k_coarse_iterate(int N, int Na, const int *__restrict__ rp,
+                                                         const int *__restrict__ kc, const double *__restrict__ a,
+                                                         const int *__restrict__ rows, const int *__restrict__ cptr,
+                                                         int nc, int kind, double omega, double red, int maxit,
+                                                         const T *__restrict__ f, T *x, double *tmp) {
+  pdl_wait();
+  pdl_trigger();
+  __shared__ double sh[32];
+  auto residual = [&]() {
+    double r2 = 0;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+      double dg;
+      const double s = coarse_row_sum<T>(i, rp, kc, a, x, dg);
+      const double d = (double)f[i] - s - dg * (double)x[i];
+      r2 += d * d;
+    }
+    return sqrt(cc_block_sum(r2, sh));
+  };
+  auto relax_colour = [&](int c) {
+    for (int t = cptr[c] + threadIdx.x; t < cptr[c + 1]; t += blockDim.x) {
+      const int i = rows[t];
+      double dg;
+      const double s = (double)f[i] - coarse_row_sum<T>(i, rp, kc, a, x, dg);
+      const double xi = (double)x[i];
+      x[i] = (T)(omega * (s / dg - xi) + xi);
+    }
+    __syncthreads();
+  };
+  double res = residual();
+  const double target = red * res;
+  for (int it = 0; it < maxit && res > target; it++) {
+    for (int i = Na + threadIdx.x; i < N; i += blockDim.x) x[i] = f[i];  // Dirichlet rows from the rhs
+    __syncthreads();
+    if (kind == PMG_SMOOTHER_JACOBI) {
+      for (int i = threadIdx.x; i < Na; i += blockDim.x) {
+        double dg;
+        const double s = (double)f[i] - coarse_row_sum<T>(i, rp, kc, a, x, dg);
+        tmp[i] = (1.0 - omega) * (double)x[i] + omega * s / dg;
+      }
+      __syncthreads();
+      for (int i = threadIdx.x; i < Na; i += blockDim.x) x[i] = (T)tmp[i];
+      __syncthreads();
+    } else {
+      for (int c = 0; c < nc; c++) relax_colour(c);
+      if (kind == PMG_SMOOTHER_SSOR)
+        for (int c = nc - 1; c >= 0; c--) relax_colour(c);
+    }
+    res = residual();
+  }
 }
 
 template <typename T>
@@ -383,10 +570,9 @@ static int vcycle(Handle &h, int i, bool learned) {
   // The solve copy of the matrix leaves out the active rows' Dirichlet
   // columns: on the level the cycle enters, fold them into the right-hand
   // side (f_a -= A_aD f_D; the smoother keeps x_D = f_D).  Coarser levels need
-  // nothing: the restriction writes 0 into their Dirichlet rows.  The dense
-  // coarse solve reads the full CSR rows itself.
-  if (i == (int)h.lv.size() - 1 && (i >= 1 || h.prm.coarse_smoother != PMG_COARSE_DIRECT))
-    PMG_TRY(dirichlet_cols<T>(s, L, PT::f(L), PT::f(L)));
+  // nothing: the restriction writes 0 into their Dirichlet rows.  The
+  // coarsest-level solves (dense or iterative) read the full CSR rows themselves.
+  if (i == (int)h.lv.size() - 1 && i >= 1) PMG_TRY(dirichlet_cols<T>(s, L, PT::f(L), PT::f(L)));
   if (i == 0) {
     if (h.prm.coarse_smoother == PMG_COARSE_DIRECT) {
       PMG_CUDA(launch_pdl(k_coarse_rhs<T>, dim3((L.N * 32 + 255) / 256), dim3(256), 0, s, L.N, L.Na,
@@ -400,20 +586,28 @@ static int vcycle(Handle &h, int i, bool learned) {
       }
       PMG_CUDA(cudaGetLastError());
     } else {
-      int it = h.prm.coarse_maxit > 0 ? h.prm.coarse_maxit : 1;
-      for (int k = 0; k < it; k++) PMG_TRY(smooth_step<T>(h, L, learned, k == 0, k > 0));
+      const int nc = (int)L.rcolor_ptr.size() - 1;
+      PMG_CUDA(launch_pdl(k_coarse_iterate<T>, dim3(1), dim3(1024), 0, s, L.N, L.Na, (const int *)L.rowptr.p,
+                          (const int *)L.kcol.p, (const double *)L.A.p, (const int *)L.row_list.p,
+                          (const int *)h.coarse_cptr.p, nc, h.prm.coarse_smoother, h.prm.smooth_omega,
+                          h.prm.coarse_red, h.prm.coarse_maxit, (const T *)PT::f(L), PT::x(L), h.coarse_t.p));
+      count_launches(1);
     }
     return PMG_OK;
   }
   Level &C = h.lv[i - 1];
   const int pre = (learned && h.prm.learned_steps > 0) ? h.prm.learned_steps : h.prm.pre_smooth;
   const int post = (learned && h.prm.learned_steps > 0) ? h.prm.learned_steps : h.prm.post_smooth;
-  for (int k = 0; k < pre; k++) PMG_TRY(smooth_step<T>(h, L, learned, k == 0, k > 0));
+  const bool slc = h.prm.slc_all || (h.prm.slc_fine && i == (int)h.lv.size() - 1);
+  if (slc) PMG_TRY(slc_begin<T>(h, L));
+  for (int k = 0; k < pre; k++) PMG_TRY(smooth_step<T>(h, L, learned, k == 0, k > 0, h.prm.smoother));
   PMG_TRY(sell_spmv<T>(s, L, PT::x(L), PT::f(L), PT::d(L), 1, h.num_sms));
   PMG_TRY(restrict_defect<T>(s, L, C, PT::R(L), PT::d(L), PT::f(C), PT::x(C)));  // also x_C := 0
   PMG_TRY(vcycle<T>(h, i - 1, learned));
   PMG_TRY(prolongate_add<T>(s, L, PT::P(L), PT::x(C), PT::x(L), h.prm.gmg_damp));
-  for (int k = 0; k < post; k++) PMG_TRY(smooth_step<T>(h, L, learned, pre == 0 && k == 0, k > 0));
+  for (int k = 0; k < post; k++)
+    PMG_TRY(smooth_step<T>(h, L, learned, pre == 0 && k == 0, k > 0, h.prm.smoother));
+  if (slc) PMG_TRY(slc_end<T>(h, L));
   return PMG_OK;
 }
 
@@ -450,6 +644,10 @@ static int prepare_levels(Handle &h) {
       return PMG_ERR_STATE;
     }
     PMG_TRY(L.x64.alloc(L.N)); PMG_TRY(L.f64.alloc(L.N)); PMG_TRY(L.d64.alloc(L.N));
+    const bool slc = i > 0 && (h.prm.slc_all || (h.prm.slc_fine && i + 1 == h.lv.size()));
+    const bool jac = h.prm.smoother == PMG_SMOOTHER_JACOBI || (i == 0 && h.prm.coarse_smoother == PMG_COARSE_JACOBI);
+    for (int k = 0; k < 3 && slc; k++) PMG_TRY(fp32 ? L.slc32[k].alloc(L.N) : L.slc64[k].alloc(L.N));
+    if (jac) PMG_TRY(fp32 ? L.jac32.alloc(L.N) : L.jac64.alloc(L.N));
     if (fp32) {
       PMG_TRY(sell_values<float>(h, L));
       PMG_TRY(L.x32.alloc(L.N)); PMG_TRY(L.f32.alloc(L.N)); PMG_TRY(L.d32.alloc(L.N));
@@ -465,6 +663,13 @@ static int prepare_levels(Handle &h) {
   }
   // the outer Krylov method multiplies with the FP64 finest matrix
   PMG_TRY(sell_values<double>(h, h.lv.back()));
+  if (h.prm.slc_all || h.prm.slc_fine) PMG_TRY(h.slc_part.alloc(2 * SLC_BLOCKS + 1));
+  if (h.prm.coarse_smoother != PMG_COARSE_DIRECT) {
+    // colour pointers of the coarsest level's row list, and the Jacobi scratch
+    const Level &C = h.lv[0];
+    PMG_TRY(h.coarse_cptr.upload(C.rcolor_ptr.data(), C.rcolor_ptr.size(), h.stream));
+    PMG_TRY(h.coarse_t.alloc(std::max(C.N, 1)));
+  }
   if (h.prm.smoother == PMG_SMOOTHER_LEARNED) PMG_TRY(learned_prepare(h));
   if (h.prm.coarse_smoother == PMG_COARSE_DIRECT && !h.coarse_ready) PMG_TRY(coarse_factor(h));
   const int cc = coarse_cycle_top(h);
@@ -482,11 +687,19 @@ static int capture_one(Handle &h, bool learned, cudaGraphExec_t &exec, unsigned 
   PMG_CUDA(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal));
   int top = (int)h.lv.size() - 1;
   int rc = h.prm.precision == PMG_PREC_FP32 ? vcycle<float>(h, top, learned) : vcycle<double>(h, top, learned);
-  cudaError_t e = cudaStreamEndCapture(h.stream, &g);
-  if (rc != PMG_OK) return rc;
-  PMG_CUDA(e);
-  PMG_CUDA(cudaGraphInstantiate(&exec, g, 0));
+  cudaGraph_t g_end = nullptr;
+  cudaError_t e = cudaStreamEndCapture(h.stream, &g_end);
+  g = g_end;
+  if (rc != PMG_OK || e != cudaSuccess) {
+    // the captured launches never ran: take them off the count, free the graph
+    count_launches(0ULL - (launches_so_far() - before));
+    if (e == cudaSuccess && g) cudaGraphDestroy(g);
+    if (rc != PMG_OK) return rc;
+    PMG_CUDA(e);
+  }
+  cudaError_t ei = cudaGraphInstantiate(&exec, g, 0);
   cudaGraphDestroy(g);
+  PMG_CUDA(ei);
   // kernels recorded during capture run at each replay, not now
   kernels = launches_so_far() - before;
   count_launches(0ULL - kernels);

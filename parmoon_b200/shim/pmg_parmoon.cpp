@@ -38,10 +38,20 @@ TPmgSystemCD3D::TPmgSystemCD3D(int N_levels, TFESpace3D **fespaces, double **sol
   pmg_params p;
   pmg_default_params(&p);
   TParamDB *db = TDatabase::ParamDB;
-  p.smoother = db->SC_SMOOTHER_SCALAR == 1 ? PMG_SMOOTHER_JACOBI : PMG_SMOOTHER_SSOR;
+  // 1 Jacobi, 2 SOR, 3 SSOR; the sequential reference runs SOR for the codes
+  // its switch does not list (MultiGrid3D.C:210-213, 430-440); ILU (4) is not
+  // built here and pmg_create rejects it
+  {
+    const int sm = db->SC_SMOOTHER_SCALAR;
+    p.smoother = (sm >= 1 && sm <= 4) ? sm : PMG_SMOOTHER_SOR;
+    const int cs = db->SC_COARSE_SMOOTHER_SCALAR;
+    // unlisted coarse smoothers run SSOR (MultiGrid3D.C:320-327)
+    p.coarse_smoother = (cs >= 1 && cs <= 4) || cs == PMG_COARSE_DIRECT ? cs : PMG_COARSE_SSOR;
+  }
+  p.slc_all = db->SC_STEP_LENGTH_CONTROL_ALL_SCALAR != 0;
+  p.slc_fine = db->SC_STEP_LENGTH_CONTROL_FINE_SCALAR != 0;
   p.pre_smooth = db->SC_PRE_SMOOTH_SCALAR;
   p.post_smooth = db->SC_POST_SMOOTH_SCALAR;
-  p.coarse_smoother = db->SC_COARSE_SMOOTHER_SCALAR == PMG_COARSE_DIRECT ? PMG_COARSE_DIRECT : PMG_COARSE_SSOR;
   p.coarse_maxit = db->SC_COARSE_MAXIT_SCALAR;
   p.coarse_red = db->SC_COARSE_RED_FACTOR_SCALAR;
   p.smooth_omega = db->SC_SMOOTH_DAMP_FACTOR_SCALAR;

@@ -48,6 +48,31 @@ CASES = {
 }
 
 
+# Smoother variants of TMultiGrid3D::Smooth / Cycle on the q1_supg problem
+# (same mesh, space and numbering as q1_supg.npz): only the solutions and
+# iteration counts are kept; the matrices are those of q1_supg.npz.
+SMOOTHER_BASE = dict(order=1, levels=3, coarse_steps=1, problem="cdsupg", eps=1e-3, b1=1, b2=0.5, b3=0.25,
+                     red=1e-12, dump=0, dump_solution=1, restart=30)
+SMOOTHER_VARIANTS = [dict(smoother=1, omega=0.8), dict(smoother=2, omega=1.0), dict(smoother=2, omega=1.2, slc_fine=1),
+                     dict(smoother=3, omega=1.0, slc_all=1), dict(smoother=1, omega=0.7, slc_all=1)]
+
+
+def make_smoothers():
+    out = {}
+    for k, v in enumerate(SMOOTHER_VARIANTS):
+        opt = dict(SMOOTHER_BASE, **v)
+        with tempfile.TemporaryDirectory() as td:
+            subprocess.run([BIN, "cd3d", td] + [f"{a}={b}" for a, b in opt.items()], check=True,
+                           stdout=subprocess.DEVNULL)
+            data = load_dump(td)
+        out[f"V{k}_solution"] = data["solution"]
+        out[f"V{k}_iterations"] = data["solve_iterations"]
+        out[f"V{k}_rel_res"] = data["res_final"] / data["res0"]
+        out[f"V{k}_params"] = np.array([f"{a}={b}" for a, b in opt.items()])
+    np.savez_compressed(os.path.join(HERE, "q1_supg_smoothers.npz"), **out)
+    print("q1_supg_smoothers", {k: v for k, v in out.items() if k.endswith("_iterations")})
+
+
 def load_dump(d):
     out = {}
     with open(os.path.join(d, "meta.txt")) as f:
@@ -75,11 +100,16 @@ def recorded_log(ref):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("PMG_REFERENCE_DIR"),
+                    help="the ParMooN source tree (default: $PMG_REFERENCE_DIR)")
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
+    if not args.ref or not os.path.isdir(args.ref):
+        raise SystemExit("give the ParMooN source tree with --ref or PMG_REFERENCE_DIR")
     if not os.path.exists(BIN):
         raise SystemExit("build the reference oracle first: make -C oracle/ref")
+    if args.only in (None, "q1_supg_smoothers"):
+        make_smoothers()
     for name, (mode, opt) in CASES.items():
         if args.only and name != args.only:
             continue

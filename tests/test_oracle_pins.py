@@ -148,3 +148,35 @@ def test_oracle_vcycle_is_a_contracting_linear_operator(oracle):
     err = e - oracle.mg_apply(olev, v)
     Aa = lambda x: oracle.spmv(F["rp"], F["kc"], F["a"], x)
     assert float(err @ Aa(err)) <= 0.25 * float(e @ Aa(e))
+
+
+@pytest.mark.parametrize("k", range(5))
+def test_oracle_smoother_variants_match_reference(oracle, k):
+    """Jacobi (MGLevel3D.C:469-560), SOR (:280-361) and step-length control
+    (MultiGrid3D.C:517-523, 655-663; MGLevel3D.C:908-961) in the oracle
+    against the compiled reference's FGMRES + GMG on the q1_supg problem
+    (3 levels, lexicographic smoothing, iterative SSOR coarse solve), both to
+    1e-12: the same iteration count and the same solution to 1e-9 relative."""
+    g, v = golden("q1_supg"), golden("q1_supg_smoothers")
+    opt = dict(s.split("=") for s in v[f"V{k}_params"])
+    levels = []
+    for l in range(n_levels(g)):
+        p = f"L{l}_"
+        levels.append(dict(N=int(g[p + "N"]), Na=int(g[p + "active_bound"]), rp=g[p + "rowptr"], kc=g[p + "kcol"],
+                           a=g[p + "entries"]))
+    for l in range(1, len(levels)):
+        nc = 2 ** l
+        latc = lattice_index(g[f"L{l-1}_dof_xyz"], nc + 1)
+        latf = lattice_index(g[f"L{l}_dof_xyz"], 2 * nc + 1)
+        levels[l]["P"] = oracle.prolongation(1, nc, latc, latf)
+    fine = levels[-1]
+    rhs = g[f"L{len(levels)-1}_rhs"]
+    sol0 = np.zeros(fine["N"])
+    sol0[fine["Na"]:] = rhs[fine["Na"]:]
+    sol, it, res, _ = oracle.fgmres_mg(levels, rhs, sol0=sol0, red=float(opt["red"]), restart=int(opt["restart"]),
+                                       coarse_direct=False, coarse_smoother=3, omega=float(opt["omega"]),
+                                       smoother=int(opt["smoother"]), slc_all=opt.get("slc_all") == "1",
+                                       slc_fine=opt.get("slc_fine") == "1", reference_restart_rule=True)
+    assert it == int(v[f"V{k}_iterations"]), (it, v[f"V{k}_iterations"])
+    ref = v[f"V{k}_solution"]
+    assert np.linalg.norm(sol - ref) / np.linalg.norm(ref) < 1e-9
