@@ -5,7 +5,7 @@ Workload (one "step"): the convection-dominated CD3D problem with SUPG on
 Q2 hexahedra, 64^3 cells (2,146,689 dofs, 130,422,149 nnz on the finest of 5
 levels), eps = 1e-6, b = (1, 0.5, 0.25), c = 0, f = 1, u = 1 on x = 0 and
 u = 0 on the rest of the boundary, Gauss3 quadrature: assembly of all five
-levels (TSystemCD3D::Assemble) followed by FGMRES(20) preconditioned by one
+levels (TSystemCD3D::Assemble) followed by FGMRES(40) preconditioned by one
 V-cycle SSOR(2,2) with a dense coarsest solve, run until the FP64 true
 residual satisfies |r| <= 1e-10 |r0| (TSystemCD3D::Solve).
 
@@ -15,7 +15,16 @@ residual satisfies |r| <= 1e-10 |r0| (TSystemCD3D::Solve).
              vector and rhs copied in, solution copied out, inside the timer
   extras     finest-level assembly Mnnz/s, plain FP64-GMG time, iterations,
              FP64 residual, roofline of the dominant kernel (the FP32 SSOR
-             sweep of the finest level) and of the assembly kernel
+             sweep of the finest level) and of the assembly kernel, and the
+             errors of the FP32-V-cycle and FP64 solutions against an
+             FP64-everywhere solve of the same system to 1e-14
+  cpu_baseline  the compiled reference, one sequential process, one step of
+             the same workload (unscaled), timed after the GPU work
+
+--impl reference: the compiled reference on the same workload, one
+sequential process per host thread (up to --steps processes, bounded by host
+memory), all timed steps running at once; value = wall time of the timed
+block / steps (the host's throughput), latency per step reported beside it.
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 For N > 1 (torchrun) every rank solves its own copy (replicas, weak scaling;
@@ -24,6 +33,7 @@ the problem has no exchange step on one GPU), timing is the max over ranks.
 import argparse
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -40,11 +50,12 @@ METRIC = "Time to 1e-10 FP64 residual & assembly Mnnz/s: learned/FP32 MG vs FP64
 N_CELLS, N_LEVELS = 64, 5
 EPS, B, F = 1e-6, (1.0, 0.5, 0.25), 1.0
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "pmg_ref")
-# bounded CPU sample for the reference: the same problem on 32^3 cells (4 levels)
-REF_SAMPLE = dict(order=2, levels=4, coarse_steps=2, problem="cdsupg", eps=EPS, b1=B[0], b2=B[1], b3=B[2],
-                  dump=0, transfer=0, restart=20, red=1e-10)
+# FGMRES restart length of both arms: no restart occurs inside the solve to
+# 1e-10 in either (19 iterations here, 25 in the reference), so both stop on
+# |r| <= 1e-10 |r0| of the first residual (the reference's restart rule,
+# FgmresIte.C:546-566, would otherwise re-base r0 at iteration 20)
+RESTART = 40
 N_FULL = (2 * N_CELLS + 1) ** 3
-N_SAMPLE = (2 * 32 + 1) ** 3
 # DRAM traffic of one FP32 SSOR step per algorithmic byte, measured with ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum over the 54 colour launches of
 # one step on the finest level of the 48^3 Q2 hierarchy: 0.858 GB for 0.663 GB
@@ -149,34 +160,125 @@ def dirichlet(x, y, z):
 
 def setup(P, precision):
     levels = P.struct_hierarchy(P.Q2_HEX, N_CELLS, N_LEVELS)
-    h = P.Handle(N_LEVELS, P.default_params(precision=precision))
+    h = P.Handle(N_LEVELS, P.default_params(precision=precision, restart=RESTART))
     h.set_coefficients(P.coeff(kind=P.COEF_CONST, eps=EPS, b=B, f=F))
     P.load_hierarchy(h, levels, dirichlet=dirichlet)
     return h, levels
 
 
-def run_reference_sample():
-    """One run of the compiled reference on the bounded sample; returns timings dict."""
-    with tempfile.TemporaryDirectory() as td:
-        cmd = [REF_BIN, "cd3d", td] + [f"{k}={v}" for k, v in REF_SAMPLE.items()]
-        t0 = time.perf_counter()
-        subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
-        wall = time.perf_counter() - t0
-        meta = {}
-        with open(os.path.join(td, "meta.txt")) as f:
+def ref_options():
+    """pmg_ref options of the benchmarked workload (the same problem, hierarchy,
+    quadrature and solver settings as this arm): Q2 SUPG 64^3 over 5 levels."""
+    return dict(order=2, levels=N_LEVELS, coarse_steps=2, problem="cdsupg", eps=EPS, b1=B[0], b2=B[1], b3=B[2],
+                red=1e-10, restart=RESTART, dump=0, transfer=0)
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def host_cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
             for line in f:
-                k, kind, v = line.split()
-                if kind == "scalar":
-                    meta[k] = float(v)
-    t_asm = sum(v for k, v in meta.items() if k.endswith("_t_assemble"))
-    return dict(t_assemble=t_asm, t_assemble_fine=meta["L3_t_assemble"], t_solve=meta["t_solve"],
-                iterations=meta["solve_iterations"], rel_res=meta["res_final"] / meta["res0"], wall=wall)
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
 
 
-def ref_sample_desc():
-    return ("reference ParMooN (oracle/_ref/pmg_ref, -O3, 1 thread, sequential build) on the same problem at "
-            "32^3 cells / 4 levels (274,625 dofs): Assemble()+Solve() wall time, scaled by the dof ratio "
-            f"{N_FULL / N_SAMPLE:.3f} to 64^3 (multigrid work is O(N) per iteration)")
+def mem_available():
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except Exception:
+        pass
+    return 0
+
+
+# host memory of one reference process at 64^3 / 5 levels (measured peak RSS 2.83 GB) with headroom
+REF_BYTES_PER_PROCESS = 3.5e9
+
+
+def run_reference(n_steps, n_warm, max_procs=None, timeout=3000):
+    """The compiled reference (oracle/_ref/pmg_ref: the reference's own
+    TSquareStructure3D, TAssembleMat3D, TMultiGrid3D and TFgmresIte) on the
+    benchmarked workload, unscaled.  The reference is sequential, so the host's
+    cores run independent copies: P processes build the hierarchy (untimed),
+    do their share of the n_warm warm-up steps, wait for a common start
+    signal, then do their share of the n_steps timed steps (Assemble() of all
+    levels + Solve() from the zero start vector, bracketed as
+    CD3D_ParMooN.C:418-463 brackets them).  Returns the per-step times, the
+    wall time of the timed block (start signal to the last process's end) and
+    the process count."""
+    cores = host_cores()
+    procs_cap = max(1, min(cores, int(mem_available() // REF_BYTES_PER_PROCESS) or 1))
+    P = max(1, min(n_steps, procs_cap if max_procs is None else min(max_procs, procs_cap)))
+    reps = [n_steps // P + (1 if j < n_steps % P else 0) for j in range(P)]
+    warms = [n_warm // P + (1 if j < n_warm % P else 0) for j in range(P)]
+    td = tempfile.mkdtemp(prefix="pmg_ref_")
+    go = os.path.join(td, "go")
+    workers = []
+    for j in range(P):
+        out = os.path.join(td, f"w{j}")
+        opt = dict(ref_options(), repeat=reps[j], warmup=warms[j], start_file=go)
+        cmd = [REF_BIN, "cd3d", out] + [f"{k}={v}" for k, v in opt.items()]
+        workers.append((subprocess.Popen(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL), out))
+
+    def meta(out):
+        m = {}
+        try:
+            with open(os.path.join(out, "meta.txt")) as f:
+                for line in f:
+                    k, kind, v = line.split()
+                    if kind == "scalar":
+                        m[k] = float(v)
+        except (FileNotFoundError, ValueError):
+            pass
+        return m
+
+    t_end = time.time() + timeout
+    while time.time() < t_end:  # every process ready (hierarchy built, warm-up done)
+        if any(p.poll() not in (None, 0) for p, _ in workers):
+            raise RuntimeError("a reference process failed before the timed block")
+        if all("ready_epoch" in meta(o) for _, o in workers):
+            break
+        time.sleep(0.2)
+    else:
+        for p, _ in workers:
+            p.kill()
+        raise RuntimeError("reference processes not ready in time")
+    t_go = time.time()
+    open(go, "w").close()
+    for p, _ in workers:
+        p.wait(timeout=max(1.0, t_end - time.time()))
+        if p.returncode != 0:
+            raise RuntimeError(f"reference process exited with {p.returncode}")
+    steps = []
+    t_last = t_go
+    for _, o in workers:
+        m = meta(o)
+        t_last = max(t_last, m["timed_end_epoch"])
+        k = 0
+        while f"R{k}_t_solve" in m:
+            steps.append(dict(t_assemble=m[f"R{k}_t_assemble"], t_solve=m[f"R{k}_t_solve"],
+                              iterations=m[f"R{k}_iterations"], rel_res=m[f"R{k}_rel_res"]))
+            k += 1
+    shutil.rmtree(td, ignore_errors=True)
+    return dict(steps=steps, wall=t_last - t_go, procs=P, cores=cores, reps=reps)
+
+
+def ref_desc(P, cores):
+    return (f"reference ParMooN compiled from its sources (oracle/_ref/pmg_ref, g++ -O3 -march=native, sequential "
+            f"build) on the benchmarked workload itself (Q2 SUPG 64^3, 5 levels, FGMRES({RESTART}) + V-cycle "
+            f"SSOR(2,2) to 1e-10, no scaling): {P} concurrent independent processes on the host's {cores} "
+            f"threads ({host_cpu_model()}); per step Assemble() of all levels + Solve() wall time")
 
 
 def bench_reference(args, rank, world):
@@ -185,21 +287,26 @@ def bench_reference(args, rank, world):
     if not os.path.exists(REF_BIN):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/pmg_ref not built (make -C oracle/ref)"}))
         return
-    for _ in range(args.warmup):
-        run_reference_sample()
-    runs = [run_reference_sample() for _ in range(args.steps)]
-    scale = N_FULL / N_SAMPLE
-    step = statistics.median([(r["t_assemble"] + r["t_solve"]) * scale for r in runs])
-    r0 = runs[0]
-    line = {"metric": METRIC, "value": step, "unit": "s", "impl": "reference", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": False, "scaling": "weak",
+    r = run_reference(args.steps, args.warmup)
+    per = [s["t_assemble"] + s["t_solve"] for s in r["steps"]]
+    value = r["wall"] / args.steps  # throughput of the whole host: seconds per solved system
+    line = {"metric": METRIC, "value": value, "unit": "s", "impl": "reference", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "CD3D SUPG Q2 hexahedra 64^3 (5 levels), eps=1e-6, b=(1,.5,.25), FGMRES+GMG to 1e-10",
-                       "sample": "32^3 / 4 levels, scaled by dof ratio"},
-            "assembly_mnnz_s": 15837829 / r0["t_assemble_fine"] / 1e6, "iterations": r0["iterations"],
-            "rel_res": r0["rel_res"],
-            "cpu_baseline": {"value": step, "unit": "s", "cores": 1, "kind": "reference", "sample": ref_sample_desc()},
-            "e2e": {"value": step, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": {"workload": f"CD3D SUPG Q2 hexahedra {N_CELLS}^3 ({N_LEVELS} levels), eps=1e-6, b=(1,.5,.25), "
+                                   f"f=1, FGMRES({RESTART}) + V-cycle SSOR(2,2), to 1e-10",
+                       "n_dofs": N_FULL, "levels": N_LEVELS,
+                       "parallelism": f"{r['procs']} concurrent sequential processes"},
+            "value_kind": "host throughput: wall time of the timed block / steps, all processes running at once",
+            "latency_s": {"median": statistics.median(per), "min": min(per), "max": max(per)},
+            "assembly_s_median": statistics.median(s["t_assemble"] for s in r["steps"]),
+            "solve_s_median": statistics.median(s["t_solve"] for s in r["steps"]),
+            "iterations": r["steps"][0]["iterations"], "rel_res": max(s["rel_res"] for s in r["steps"]),
+            "timed_wall_s": r["wall"], "processes": r["procs"], "host_threads": r["cores"],
+            "host_cpu": host_cpu_model(),
+            "cpu_baseline": {"value": value, "unit": "s", "cores": r["procs"], "kind": "reference",
+                             "sample": ref_desc(r["procs"], r["cores"])},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
@@ -289,29 +396,46 @@ def bench_ours(args, rank, world, dist):
     e2e = statistics.median(e2e_t)
 
     # plain FP64 GMG on the same problem (the method the FP32 V-cycle is compared with)
-    h.set_params(P.default_params(precision=P.PREC_FP64))
+    x32 = h.get_solution()
+    h.set_params(P.default_params(precision=P.PREC_FP64, restart=RESTART))
     fp64 = []
     for _ in range(2):
         _, st64, rc64 = h.solve()
         fp64.append((st64.seconds, st64.iterations, st64.rel_res, rc64, st64.vcycle_seconds))
     fp64_s = min(x[0] for x in fp64)
+    x64 = h.get_solution()
+    # error of both 1e-10 solutions against an FP64-everywhere solve of the
+    # same system to |r| <= 1e-14 |r0| (FP64 V-cycle, FP64 FGMRES)
+    h.set_params(P.default_params(precision=P.PREC_FP64, restart=RESTART, lin_red=1e-14, lin_maxit=300))
+    _, st_t, rc_t = h.solve()
+    xt = h.get_solution()
+    nt = float(np.linalg.norm(xt))
+    err = {"fp32_vcycle_solve": float(np.linalg.norm(x32 - xt)) / nt,
+           "fp64_gmg_solve": float(np.linalg.norm(x64 - xt)) / nt,
+           "fp32_vs_fp64_solve": float(np.linalg.norm(x32 - x64)) / float(np.linalg.norm(x64)),
+           "fp64_everywhere_rel_res": st_t.rel_res, "fp64_everywhere_status": rc_t,
+           "note": "relative L2 errors of the 1e-10 solutions against the FP64-everywhere solve to 1e-14"}
 
     line = None
     if rank == 0:
         cpu = None
         if os.path.exists(REF_BIN) and not args.no_cpu:
-            r = run_reference_sample()
-            v = (r["t_assemble"] + r["t_solve"]) * N_FULL / N_SAMPLE
-            cpu = {"value": v, "unit": "s", "cores": 1, "kind": "reference", "sample": ref_sample_desc(),
-                   "sample_assembly_mnnz_s": 15837829 / r["t_assemble_fine"] / 1e6,
-                   "sample_iterations": r["iterations"]}
+            # one sequential reference process, one step of the same workload
+            # (after the GPU timing, so the two do not share the host)
+            r = run_reference(1, 0, max_procs=1)
+            s0 = r["steps"][0]
+            cpu = {"value": s0["t_assemble"] + s0["t_solve"], "unit": "s", "cores": 1, "kind": "reference",
+                   "sample": ref_desc(1, r["cores"]).replace("concurrent independent processes", "process")
+                   + "; one step",
+                   "assembly_s": s0["t_assemble"], "solve_s": s0["t_solve"], "iterations": s0["iterations"],
+                   "rel_res": s0["rel_res"], "host_cpu": host_cpu_model()}
         st = stats[-1]
         line = {
             "metric": METRIC, "value": step_time, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_time * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
             "config": {"workload": f"CD3D SUPG Q2 hexahedra {N_CELLS}^3 ({N_LEVELS} levels), eps=1e-6, b=(1,.5,.25), f=1, "
-                                   "FGMRES(20) + V-cycle SSOR(2,2) FP32, dense coarse solve, to 1e-10",
+                                   f"FGMRES({RESTART}) + V-cycle SSOR(2,2) FP32, dense coarse solve, to 1e-10",
                        "n_dofs": N, "nnz_fine": nnz_fine, "levels": N_LEVELS,
                        "l2": "inputs larger than L2 (finest matrix 1.04 GB FP64 values + 0.52 GB indices)",
                        "parallelism": f"replicas x{world}"},
@@ -319,6 +443,7 @@ def bench_ours(args, rank, world, dist):
             "assembly_mnnz_s": nnz_fine / t_asm_fine / 1e6, "assembly_fine_s": t_asm_fine,
             "fp64_gmg": {"solve_s": fp64_s, "iterations": fp64[0][1], "rel_res": fp64[0][2], "status": fp64[0][3],
                          "vcycle_s": fp64[0][4]},
+            "err_vs_fp64": err,
             "fp32_solve_s": statistics.mean(s.seconds for s in stats),
             "fp32_solve_setup_s": statistics.mean(s.setup_seconds for s in stats),
             "fp32_vcycle_s": statistics.mean(s.vcycle_seconds for s in stats),

@@ -411,11 +411,16 @@ static int run_cd3d()
         memcpy(L[i].sol + Na, L[i].rhs + Na, (L[i].N - Na) * sizeof(double));
       }
       double b = wall();
+      // Solve() through copies of sol / rhs: the finest MG level aliases the
+      // level arrays (TSystemCD3D::Solve copies through Itmethod_sol / _rhs,
+      // SystemCD3D.C:377-395)
+      std::vector<double> isol(L[top].sol, L[top].sol + N), irhs(L[top].rhs, L[top].rhs + N);
       double r0, r1;
-      ScalarDefect(L[top].A, L[top].sol, L[top].rhs, d.data(), r0);
-      int iters = itm->Iterate(sq, NULL, L[top].sol, L[top].rhs);
+      ScalarDefect(L[top].A, isol.data(), irhs.data(), d.data(), r0);
+      int iters = itm->Iterate(sq, NULL, isol.data(), irhs.data());
+      memcpy(L[top].sol, isol.data(), sizeof(double) * N);
       double c = wall();
-      ScalarDefect(L[top].A, L[top].sol, L[top].rhs, d.data(), r1);
+      ScalarDefect(L[top].A, isol.data(), irhs.data(), d.data(), r1);
       if (k >= warm)
       {
         char key[64];

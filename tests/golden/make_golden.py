@@ -32,18 +32,26 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 BIN = os.path.join(ROOT, "oracle", "_ref", "pmg_ref")
 
 # name -> (mode, driver options)
+# the solves stop at |r| <= 1e-14 |r0| (red), near the FP64 rounding floor, so
+# the stored solution is the discrete solution to ~cond(A) * 1e-14
+TIGHT = dict(red=1e-14, maxit=300)
 CASES = {
-    "q1_laplace": ("cd3d", dict(order=1, levels=3, coarse_steps=1, problem="laplace")),
+    "q1_laplace": ("cd3d", dict(order=1, levels=3, coarse_steps=1, problem="laplace", **TIGHT)),
     "q1_supg": ("cd3d", dict(order=1, levels=3, coarse_steps=1, problem="cdsupg",
-                             eps=1e-3, b1=1, b2=0.5, b3=0.25)),
+                             eps=1e-3, b1=1, b2=0.5, b3=0.25, **TIGHT)),
     "q2_supg": ("cd3d", dict(order=2, levels=2, coarse_steps=1, problem="cdsupg",
-                             eps=1e-6, b1=1, b2=0.5, b3=0.25)),
+                             eps=1e-6, b1=1, b2=0.5, b3=0.25, **TIGHT)),
+    # (an assembly pin only: Galerkin at this mesh Peclet number is not a solve case)
     "q2_galerkin": ("cd3d", dict(order=2, levels=2, coarse_steps=1, problem="cdsupg", disc=1,
                                  eps=1e-2, b1=1, b2=0.5, b3=0.25)),
     "p2tet_supg": ("cd3d", dict(order=2, levels=2, coarse_steps=1, problem="cdsupg",
-                                eps=1e-3, b1=1, b2=0.5, b3=0.25, geo="SixTetras")),
+                                eps=1e-3, b1=1, b2=0.5, b3=0.25, geo="SixTetras", **TIGHT)),
     "p1tet_laplace": ("cd3d", dict(order=1, levels=2, coarse_steps=1, problem="laplace",
-                                   geo="SixTetras")),
+                                   geo="SixTetras", **TIGHT)),
+    # the C1 configuration exactly: Poisson, Q1, 4^3 -> 32^3 cells over 4 levels,
+    # Gauss2; the solution and the finest dof positions only (no matrices)
+    "c1_poisson_q1_32": ("cd3d", dict(order=1, levels=4, coarse_steps=2, problem="laplace", dump=0,
+                                      dump_solution=1, **TIGHT)),
     "tcd3d_amc": ("tcd3d", dict(order=1, levels=3, coarse_steps=2, endtime=0.5)),
 }
 

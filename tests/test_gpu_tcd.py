@@ -5,7 +5,8 @@
    device path reproduces the printed L2 errors at every step to all 7
    printed digits, and the H1-semi errors of the compiled reference.
 2. A SUPG step with the rotating convection field of the TCD3D benchmark
-   configuration against the oracle's dense theta-scheme step (1e-8)."""
+   configuration against the oracle's dense theta-scheme step (1e-10; solved
+   to |r| <= 1e-14 |r0|)."""
 import numpy as np
 import pytest
 
@@ -73,7 +74,7 @@ def test_tcd_supg_step_matches_oracle(pmg, oracle):
     F = levels[-1]
     N, Na = F["N"], F["active_bound"]
     tau, t0 = 1e-3, 0.25
-    h = pmg.Handle(2, pmg.default_params(lin_red=1e-13, restart=30))
+    h = pmg.Handle(2, pmg.default_params(lin_red=1e-14, lin_maxit=300, restart=30))
     ck = lambda t: dict(kind=pmg.COEF_ROTATING, eps=1e-4, f=1.0, t=t)
     pmg.load_hierarchy(h, levels)
     h.set_coefficients(pmg.coeff(**ck(t0)))
@@ -110,5 +111,5 @@ def test_tcd_supg_step_matches_oracle(pmg, oracle):
     S = Md + tau * 0.5 * Ad
     S[Na:, :] = Md[Na:, :]
     xo = np.linalg.solve(S, Bo)
-    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-8
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-10
     h.close()
