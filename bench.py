@@ -455,7 +455,10 @@ def bench_ours(args, rank, world, dist):
                          "launch_s": ssor["seconds"]},
             "roofline_spmv64": {"achieved": spmv64["gbs"], "frac": spmv64["gbs"] / hbm, "bytes": spmv64["bytes"]},
             "roofline_spmv32": {"achieved": spmv32["gbs"], "frac": spmv32["gbs"] / hbm, "bytes": spmv32["bytes"]},
-            "roofline_assembly": {"achieved_gbs": asm["gbs"], "frac_hbm": asm["gbs"] / hbm,
+            "roofline_assembly": {"kernel": "k_assemble_tc<Q2,27,CONST> (reference-table contraction on the FP64 "
+                                            "tensor cores, mma.sync m8n8k4 f64; finest level, all 8 element colours, "
+                                            "matrix and rhs zeroed first)",
+                                  "achieved_gbs": asm["gbs"], "frac_hbm": asm["gbs"] / hbm,
                                   "achieved_tflops_fp64": asm["tflops"], "bytes": asm["bytes"], "launch_s": asm["seconds"]},
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": 2 * N * 8, "d2h_bytes_per_step": 2 * N * 8},
             "gpu_launches": int(cnt1.value - cnt0.value),

@@ -108,8 +108,11 @@ typedef struct pmg_params {
     int    problem_linear;     /* INTERNAL_PROBLEM_LINEAR: 1 -> Q1 Gauss2 / Q2 Gauss3 / P1 Keast4 / P2 Keast11,
                                   0 -> Q1 Gauss3 / Q2 Gauss4 / P1 Keast11 (FEDatabase3D.C:1203-1309) */
     int    learned_steps;      /* learned-smoother steps per pre/post phase (0: pre_smooth / post_smooth) */
-    int    assembly_kernel;    /* 0: automatic (cells with space-constant eps, b, c use the reference-matrix
-                                  kernel), 1: per-quadrature-point kernel for every coefficient kind */
+    int    assembly_kernel;    /* 0: automatic -- space-constant eps, b, c, and pure diffusion with a varying
+                                  eps on Q1 / P1 / P2, contract reference tables on the FP64 tensor cores;
+                                  the rest runs per quadrature point; 1: per-quadrature-point kernel for
+                                  every coefficient kind; 2: reference-matrix kernel on the FP64 CUDA cores
+                                  for space-constant coefficients (per point otherwise) */
     int    slc_all;            /* SC_STEP_LENGTH_CONTROL_ALL_SCALAR: step-length control on every level >= 1 */
     int    slc_fine;           /* SC_STEP_LENGTH_CONTROL_FINE_SCALAR: step-length control on the finest level
                                   (TMultiGrid3D::Cycle, src/FE/MultiGrid3D.C:517-523, 655-663;

@@ -20,6 +20,8 @@
 #include "pmg_internal.h"
 #include "fe_tables.h"
 #include <cstdio>
+#include <functional>
+#include <cstdlib>
 
 namespace pmg {
 
@@ -40,10 +42,12 @@ __device__ __forceinline__ void coeff_eval(const CoefDev &C, double x, double y,
       c[5] = 3 * PI * PI * C.eps * sin(PI * x) * sin(PI * y) * sin(PI * z);
       break;
     case PMG_COEF_LOGNORMAL: {
+      // cos(2 pi k.x + phi) as cospi(2 k.x + phi / pi): the reduction of an
+      // argument in units of pi is exact, so no general range reduction
       double g = 0;
       for (int m = 0; m < C.n_modes; m++) {
         const double *M = C.modes + 8 * m;
-        g += M[3] * cos(2 * PI * (M[0] * x + M[1] * y + M[2] * z) + M[4]);
+        g += M[3] * cospi(2.0 * (M[0] * x + M[1] * y + M[2] * z) + M[4] * (1.0 / PI));
       }
       c[0] = C.eps * exp(g);
       break;
@@ -52,8 +56,7 @@ __device__ __forceinline__ void coeff_eval(const CoefDev &C, double x, double y,
       double bx = 0, by = 0, bz = 0;
       for (int m = 0; m < C.n_modes; m++) {
         const double *M = C.modes + 8 * m;
-        double arg = 2 * PI * (M[0] * x + M[1] * y + M[2] * z) + M[4];
-        double s = -M[3] * sin(arg) * 2 * PI;
+        double s = -M[3] * sinpi(2.0 * (M[0] * x + M[1] * y + M[2] * z) + M[4] * (1.0 / PI)) * 2 * PI;
         double gx = s * M[0], gy = s * M[1], gz = s * M[2];
         bx += gy * M[7] - gz * M[6];
         by += gz * M[5] - gx * M[7];
@@ -178,6 +181,14 @@ template <> struct ET<PMG_ELEM_P1_TET> { static constexpr int NLOC = 4, NV = 4; 
 template <> struct ET<PMG_ELEM_P2_TET> { static constexpr int NLOC = 10, NV = 4; static constexpr bool HEX = false; };
 
 constexpr int ASM_WARPS = 8;
+
+// Add v into the entry of slot s (>= 0) as an L2 reduction: no value comes
+// back, so the scatter carries no load latency.  The cells of one launch share
+// no row, so no two adds of a launch meet, and the order of the adds into an
+// entry is the colour order, the same on every run.  (Storing instead of
+// adding at an entry's first touch, to drop the zeroing, was measured slower:
+// 8-byte stores into sectors not in L2 cost more than the zeroing.)
+__device__ __forceinline__ void scatter_entry(double *entries, int s, double v) { atomicAdd(entries + s, v); }
 
 struct AsmArgs {
   int n_elems;              // elements of this colour
@@ -354,23 +365,16 @@ __global__ void __launch_bounds__(ASM_WARPS * 32, 2) k_assemble(AsmArgs a) {
       // scatter through the slot map (no two elements of a colour share a row)
       const int *dof = a.elem_dof + (size_t)e * NLOC;
       const int *sl = a.slot + (size_t)e * NLOC * NLOC;
-      int bad = 0;
 #pragma unroll
       for (int i = 0; i < NLOC; i++) {
-        const int di = __ldg(dof + i);
         const int s = __ldg(sl + i * NLOC + t);
-        if (di < a.Na) {
-          if (s >= 0) a.entries[s] += acc[i];
-          else bad = 1;
-        } else if (i == t && s >= 0) {
-          a.entries[s] = 1.0;  // Dirichlet row: unit diagonal (AssembleMat3D.C:840-848)
-        }
+        if (s >= 0) scatter_entry(a.entries, s, acc[i]);
+        else if (s <= -3) a.entries[-3 - s] = 1.0;  // Dirichlet row: unit diagonal (AssembleMat3D.C:840-848)
       }
       if (a.rhs) {
         const int dt = __ldg(dof + t);
         if (dt < a.Na) a.rhs[dt] += racc;
       }
-      if (bad) atomicOr(a.flags, 1);
     }
     __syncwarp();
   }
@@ -455,7 +459,6 @@ __global__ void __launch_bounds__(ASMC_WARPS * 32, 2) k_assemble_cc(AsmArgs a, c
     for (int p = 0; p < P; p++)
 #pragma unroll
       for (int k = 0; k < 16; k++) Dr[p][k] = W[p * WE + k];
-    int bad = 0;
     // MB entries per lane per batch: all slot and entry loads of a batch are
     // issued before any arithmetic, so each lane keeps 2 MB P reads in flight
     constexpr int MB = 4;
@@ -468,25 +471,14 @@ __global__ void __launch_bounds__(ASMC_WARPS * 32, 2) k_assemble_cc(AsmArgs a, c
         const int m = m0 + 32 * b;
 #pragma unroll
         for (int p = 0; p < P; p++) {
-          sl[b][p] = -2;  // no entry
-          if (m < NN && p < ne) {
-            const int e = base + p;
-            const int i = m / NLOC;
-            const int di = __ldg(a.elem_dof + (size_t)e * NLOC + i);
-            const int s = __ldg(a.slot + (size_t)e * NN + m);
-            if (di < a.Na) {
-              if (s >= 0) sl[b][p] = s;
-              else bad = 1;
-            } else if (i == m - i * NLOC && s >= 0) {
-              sl[b][p] = -3 - s;  // Dirichlet diagonal
-            }
-          }
+          sl[b][p] = (m < NN && p < ne) ? __ldg(a.slot + (size_t)(base + p) * NN + m) : -1;
         }
       }
 #pragma unroll
       for (int b = 0; b < MB; b++)
 #pragma unroll
-        for (int p = 0; p < P; p++) old[b][p] = sl[b][p] >= 0 ? a.entries[sl[b][p]] : 0.0;
+        for (int p = 0; p < P; p++)
+          old[b][p] = sl[b][p] >= 0 ? a.entries[sl[b][p]] : 0.0;
 #pragma unroll
       for (int b = 0; b < MB; b++) {
         const int m = m0 + 32 * b;
@@ -526,14 +518,331 @@ __global__ void __launch_bounds__(ASMC_WARPS * 32, 2) k_assemble_cc(AsmArgs a, c
           a.rhs[di] += r;
         }
       }
-    if (bad) atomicOr(a.flags, 1);
     __syncwarp();
   }
 }
 
+// ------------------------------------------- tensor-core contraction kernel
+// The local matrix as a product of a fixed reference table and per-cell
+// coefficients, on the FP64 tensor cores (mma.sync.m8n8k4 .f64, DMMA):
+//   A_cell[m] = sum_k T[m][k] d_cell[k],   m = i * n_loc + j
+// CONST (eps, b, c constant in space, affine cells; the form of
+//   BilinearAssemble / _SD, ConvDiff3D.C:87-214, and the TCD forms):
+//   k = ab (16), d = |det J| D_ab (D as form_matrix), T[m][ab] = S_ab[i][j]
+//   = sum_q w_q u_ia(q) u_jb(q), the reference-element integrals.
+// DIFF (pure diffusion, eps varying in space: b = 0, c = 0): k = (q, p) with p
+//   over the 6 entries of the symmetric K = Ji Ji^T, d = w_q |det J| eps(x_q) K_p,
+//   T[m][(q,p)] = u_ia u_ja (p = aa) or u_ia u_jb + u_ib u_ja (p = ab, a < b).
+// A warp takes 8 cells.  Per 8 x 8 output block (8 entries x 8 cells) the
+// mma chain runs over the k steps of 4: the A operand (8 entries x 4 k) comes
+// from T in shared memory, stored per (entry block, k step) as the 32 lane
+// values of the fragment; the B operand (4 k x 8 cells) from the warp's
+// staged d.  Lane l ends with entries m = 8t + l/4 of cells 2(l%4), 2(l%4)+1
+// and adds them into the CSR through the slot map with L2 reductions (cells
+// of one colour share no row, so no two adds of a launch meet).  Slot loads
+// of the next batch go out before the current batch's mma chains.  The sums
+// equal the per-point ones up to rounding order.
+
+__device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+      : "+d"(c0), "+d"(c1)
+      : "d"(a), "d"(b));
+}
+
+template <int E, int NQ, bool DIFF>
+struct TcShape {
+  static constexpr int NLOC = ET<E>::NLOC, NN = NLOC * NLOC, MT = (NN + 7) / 8;
+  static constexpr int KD = DIFF ? 6 * NQ : 16, KS = (KD + 3) / 4, KP = 4 * KS;
+  static constexpr int CW = DIFF ? 23 : 17;            // per cell: J 9, x0 3, |det J|, delta, bh 3 (, K 6)
+  static constexpr int WARP_DOUBLES = KP * 8 + 8 * NQ + 8 * CW;  // d staging, rhs weights, cell data
+  static constexpr size_t TABLE_DOUBLES = (size_t)MT * KS * 32;
+};
+
+// Up to 16 warps per block (fewer when the tables leave less shared memory);
+// 8 entry blocks per batch (slot loads in flight per lane: 2 x TC_MB).  A
+// 1024-thread variant (64 registers, 4 blocks per batch) spilled and was
+// measured slower on the P2 lognormal 64^3 level (7.24 against 6.77 ms).
+template <int E, int NQ, bool DIFF>
+__global__ void __launch_bounds__(512, 1) k_assemble_tc(AsmArgs a, const double *__restrict__ tfrag) {
+  constexpr int TC_MB = 8;
+  using S = TcShape<E, NQ, DIFF>;
+  constexpr int NLOC = S::NLOC, NN = S::NN, MT = S::MT, KS = S::KS, KP = S::KP, KD = S::KD, CW = S::CW;
+  constexpr int NV = ET<E>::NV;
+  constexpr bool HEX = ET<E>::HEX;
+  extern __shared__ double sm[];
+  double *sT = sm;
+  for (int k = threadIdx.x; k < (int)S::TABLE_DOUBLES; k += blockDim.x) sT[k] = tfrag[k];
+  // Fourier modes of the coefficient field next to the table
+  double *sM = sm + S::TABLE_DOUBLES;
+  for (int k = threadIdx.x; k < 8 * a.coef.n_modes; k += blockDim.x) sM[k] = a.coef.modes[k];
+  __syncthreads();
+  if (a.coef.n_modes > 0) a.coef.modes = sM;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  double *Bs = sm + S::TABLE_DOUBLES + 8 * (size_t)a.coef.n_modes + (size_t)warp * S::WARP_DOUBLES;  // d[k][cell]
+  double *RW = Bs + KP * 8;                                                // w_q |det J| f(x_q), [cell][q]
+  double *Cs = RW + 8 * NQ;                                                // [cell][CW]
+  const bool supg = !DIFF && (a.form == PMG_FORM_SUPG || a.form == PMG_FORM_MASS_SUPG || a.form == PMG_FORM_STIFF_SUPG);
+  const int row = lane >> 2, c0 = 2 * (lane & 3);
+
+  for (int base = (blockIdx.x * nwarps + warp) * 8; base < a.n_elems; base += gridDim.x * nwarps * 8) {
+    const int ne = min(8, a.n_elems - base);
+    // 1) cell geometry and (CONST) the 16 coefficients of each cell
+    if (lane < 8) {
+      double *cw = Cs + lane * CW;
+      if (lane < ne) {
+        const int e = base + lane;
+        const double *cv = a.cell_vert + (size_t)e * NV * 3;
+        double J[9], x0[3], Ji[9], K[9], adet;
+        cell_map<HEX>(cv, J, x0, Ji, adet, K);
+        double delta = 0.0, bh[3] = {0.0, 0.0, 0.0};
+        if (!DIFF) {
+          const double *q0 = a.qtab;
+          double c[7];
+          coeff_eval(a.coef, x0[0] + J[0] * q0[1] + J[1] * q0[2] + J[2] * q0[3],
+                     x0[1] + J[3] * q0[1] + J[4] * q0[2] + J[5] * q0[3],
+                     x0[2] + J[6] * q0[1] + J[7] * q0[2] + J[8] * q0[3], c);
+          const double hconv = supg ? hk_convection(HEX, a.brick != 0, cv, Ji, c[1], c[2], c[3]) : 0.0;
+          delta = supg ? sdfem_delta(hconv, c[0], c[1], c[2], c[3], a.poly, a.delta0) : 0.0;
+#pragma unroll
+          for (int p = 0; p < 3; p++) bh[p] = Ji[p * 3 + 0] * c[1] + Ji[p * 3 + 1] * c[2] + Ji[p * 3 + 2] * c[3];
+          double D[16];
+          form_matrix(a.form, supg, c, K, bh, delta, D);
+#pragma unroll
+          for (int k = 0; k < 16; k++) Bs[k * 8 + lane] = D[k] * adet;
+        }
+#pragma unroll
+        for (int k = 0; k < 9; k++) cw[k] = J[k];
+        cw[9] = x0[0]; cw[10] = x0[1]; cw[11] = x0[2];
+        cw[12] = adet;
+        cw[13] = delta;
+        cw[14] = bh[0]; cw[15] = bh[1]; cw[16] = bh[2];
+        if (DIFF) { cw[17] = K[0]; cw[18] = K[4]; cw[19] = K[8]; cw[20] = K[1]; cw[21] = K[2]; cw[22] = K[5]; }
+      } else {
+        if (!DIFF)
+#pragma unroll
+          for (int k = 0; k < 16; k++) Bs[k * 8 + lane] = 0.0;
+        cw[12] = 0.0;
+      }
+    }
+    __syncwarp();
+    // 2) per cell and quadrature point: the rhs weights and (DIFF) the coefficients
+    for (int pq = lane; pq < 8 * NQ; pq += 32) {
+      const int c = pq / NQ, q = pq - c * NQ;
+      const double *cw = Cs + c * CW;
+      double fw = 0.0, ew = 0.0;
+      if (c < ne) {
+        const double *qq = a.qtab + q * 4;
+        const double X = cw[9] + cw[0] * qq[1] + cw[1] * qq[2] + cw[2] * qq[3];
+        const double Y = cw[10] + cw[3] * qq[1] + cw[4] * qq[2] + cw[5] * qq[3];
+        const double Z = cw[11] + cw[6] * qq[1] + cw[7] * qq[2] + cw[8] * qq[3];
+        double cf[7];
+        coeff_eval(a.coef, X, Y, Z, cf);
+        const double w = qq[0] * cw[12];
+        fw = w * cf[5];
+        ew = w * cf[0];
+      }
+      RW[c * NQ + q] = fw;
+      if (DIFF)
+#pragma unroll
+        for (int p = 0; p < 6; p++) Bs[(q * 6 + p) * 8 + c] = c < ne ? ew * cw[(17 + p) % CW] : 0.0;
+    }
+    for (int k = KD * 8 + lane; k < KP * 8; k += 32) Bs[k] = 0.0;  // padded k rows
+    __syncwarp();
+    // 3) rhs: f_i = sum_q w_q |det J| f(x_q) (u_i3(q) + delta bh . u_i(q))
+    if (a.rhs)
+      for (int ci = lane; ci < 8 * NLOC; ci += 32) {
+        const int c = ci / NLOC, i = ci - c * NLOC;
+        if (c >= ne) continue;
+        const int di = __ldg(a.elem_dof + (size_t)(base + c) * NLOC + i);
+        if (di >= a.Na) continue;
+        const double *cw = Cs + c * CW;
+        double r = 0.0;
+        for (int q = 0; q < NQ; q++) {
+          const double *u = a.utab + ((size_t)q * NLOC + i) * 4;
+          r += RW[c * NQ + q] * (__ldg(u + 3) + cw[13] * (cw[14] * __ldg(u) + cw[15] * __ldg(u + 1) + cw[16] * __ldg(u + 2)));
+        }
+        atomicAdd(a.rhs + di, r);
+      }
+    // 4) the local matrices, 8 entries x 8 cells per mma chain, and the scatter
+    auto load_slots = [&](int t0, int (&sl)[TC_MB][2]) {
+#pragma unroll
+      for (int b = 0; b < TC_MB; b++) {
+        const int m = 8 * (t0 + b) + row;
+#pragma unroll
+        for (int u = 0; u < 2; u++)
+          sl[b][u] = (t0 + b < MT && m < NN && c0 + u < ne) ? __ldg(a.slot + (size_t)(base + c0 + u) * NN + m) : -1;
+      }
+    };
+    int slc[TC_MB][2], sln[TC_MB][2];
+    load_slots(0, slc);
+    for (int t0 = 0; t0 < MT; t0 += TC_MB) {
+      if (t0 + TC_MB < MT) load_slots(t0 + TC_MB, sln);
+      double acc[TC_MB][2];
+#pragma unroll
+      for (int b = 0; b < TC_MB; b++) {
+        acc[b][0] = 0.0;
+        acc[b][1] = 0.0;
+        if (t0 + b < MT) {
+          const double *tb = sT + (size_t)(t0 + b) * KS * 32 + lane;
+#pragma unroll 4
+          for (int s = 0; s < KS; s++) dmma_8x8x4(acc[b][0], acc[b][1], tb[s * 32], Bs[(4 * s + (lane & 3)) * 8 + row]);
+        }
+      }
+      // the adds are reductions performed at L2 (no value comes back, so no
+      // load latency per entry); the cells of one launch share no row, so each
+      // entry gets at most one add per launch and the sum order is the launch
+      // order, the same on every run
+#pragma unroll
+      for (int b = 0; b < TC_MB; b++)
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const int q = slc[b][u];
+          if (q >= 0) scatter_entry(a.entries, q, acc[b][u]);
+          else if (q <= -3) a.entries[-3 - q] = 1.0;  // Dirichlet row: unit diagonal (AssembleMat3D.C:840-848)
+        }
+#pragma unroll
+      for (int b = 0; b < TC_MB; b++) {
+        slc[b][0] = sln[b][0];
+        slc[b][1] = sln[b][1];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// --- space-constant coefficients: per-cell set-up, then the contraction ----
+// k_tc_setup (one thread per cell, all cells of the level in one launch):
+// d_e = |det J| D_ab (16 values) and the cell's local rhs
+//   r_i = sum_q w_q |det J| f(x_q) (u_i3(q) + delta bh . u_i(q))
+// into per-cell buffers.  k_assemble_tc16 (per colour) then only contracts and
+// scatters: per 8 cells a warp loads its B fragments straight from d (8 cells
+// x 4 consecutive k per load), runs the 4-step mma chain per 8-entry block, and
+// adds the local rhs of its cells.  Shared memory holds the table alone, so
+// two blocks of 16 warps fit on an SM even for Q2 (94 KB).
+template <int E, int NQ>
+__global__ void __launch_bounds__(128) k_tc_setup(AsmArgs a, double *__restrict__ dbuf, double *__restrict__ rbuf,
+                                                  const double *__restrict__ rtab) {
+  constexpr int NLOC = ET<E>::NLOC, NV = ET<E>::NV;
+  constexpr bool HEX = ET<E>::HEX;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= a.n_elems) return;
+  const bool supg = a.form == PMG_FORM_SUPG || a.form == PMG_FORM_MASS_SUPG || a.form == PMG_FORM_STIFF_SUPG;
+  const double *cv = a.cell_vert + (size_t)e * NV * 3;
+  double J[9], x0[3], Ji[9], K[9], adet;
+  cell_map<HEX>(cv, J, x0, Ji, adet, K);
+  const double *q0 = a.qtab;
+  double c[7];
+  coeff_eval(a.coef, x0[0] + J[0] * q0[1] + J[1] * q0[2] + J[2] * q0[3], x0[1] + J[3] * q0[1] + J[4] * q0[2] + J[5] * q0[3],
+             x0[2] + J[6] * q0[1] + J[7] * q0[2] + J[8] * q0[3], c);
+  const double hconv = supg ? hk_convection(HEX, a.brick != 0, cv, Ji, c[1], c[2], c[3]) : 0.0;
+  const double delta = supg ? sdfem_delta(hconv, c[0], c[1], c[2], c[3], a.poly, a.delta0) : 0.0;
+  double bh[3];
+#pragma unroll
+  for (int p = 0; p < 3; p++) bh[p] = Ji[p * 3 + 0] * c[1] + Ji[p * 3 + 1] * c[2] + Ji[p * 3 + 2] * c[3];
+  double D[16];
+  form_matrix(a.form, supg, c, K, bh, delta, D);
+  double *d = dbuf + (size_t)e * 16;
+#pragma unroll
+  for (int k = 0; k < 16; k++) d[k] = D[k] * adet;
+  if (!rbuf) return;
+  double *r = rbuf + (size_t)e * NLOC;
+  if (a.coef.kind == PMG_COEF_CONST) {
+    // f constant: r_i = |det J| f (R_3[i] + delta bh . R[i]), R_a[i] = sum_q w_q u_ia(q)
+    const double af = adet * c[5];
+    for (int i = 0; i < NLOC; i++)
+      r[i] = af * (__ldg(rtab + 3 * NLOC + i) +
+                   delta * (bh[0] * __ldg(rtab + i) + bh[1] * __ldg(rtab + NLOC + i) + bh[2] * __ldg(rtab + 2 * NLOC + i)));
+    return;
+  }
+  double fw[NQ];
+  for (int q = 0; q < NQ; q++) {
+    const double *qq = a.qtab + q * 4;
+    double cq[7];
+    coeff_eval(a.coef, x0[0] + J[0] * qq[1] + J[1] * qq[2] + J[2] * qq[3], x0[1] + J[3] * qq[1] + J[4] * qq[2] + J[5] * qq[3],
+               x0[2] + J[6] * qq[1] + J[7] * qq[2] + J[8] * qq[3], cq);
+    fw[q] = qq[0] * adet * cq[5];
+  }
+  for (int i = 0; i < NLOC; i++) {
+    double acc = 0.0;
+    for (int q = 0; q < NQ; q++) {
+      const double *u = a.utab + ((size_t)q * NLOC + i) * 4;
+      acc += fw[q] * (__ldg(u + 3) + delta * (bh[0] * __ldg(u) + bh[1] * __ldg(u + 1) + bh[2] * __ldg(u + 2)));
+    }
+    r[i] = acc;
+  }
+}
+
+template <int E>
+__global__ void __launch_bounds__(512, 2) k_assemble_tc16(AsmArgs a, const double *__restrict__ tfrag,
+                                                          const double *__restrict__ dbuf,
+                                                          const double *__restrict__ rbuf) {
+  constexpr int NLOC = ET<E>::NLOC, NN = NLOC * NLOC, MT = (NN + 7) / 8, MB = 4;
+  extern __shared__ double sT[];
+  for (int k = threadIdx.x; k < MT * 4 * 32; k += blockDim.x) sT[k] = tfrag[k];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const int row = lane >> 2, c0 = 2 * (lane & 3);
+  for (int base = (blockIdx.x * nwarps + warp) * 8; base < a.n_elems; base += gridDim.x * nwarps * 8) {
+    const int ne = min(8, a.n_elems - base);
+    // B fragments: d[cell row][4 s + lane % 4]
+    double bf[4];
+#pragma unroll
+    for (int s = 0; s < 4; s++) bf[s] = row < ne ? __ldg(dbuf + (size_t)(base + row) * 16 + 4 * s + (lane & 3)) : 0.0;
+    auto load_slots = [&](int t0, int (&sl)[MB][2]) {
+#pragma unroll
+      for (int b = 0; b < MB; b++) {
+        const int m = 8 * (t0 + b) + row;
+#pragma unroll
+        for (int u = 0; u < 2; u++)
+          sl[b][u] = (t0 + b < MT && m < NN && c0 + u < ne) ? __ldg(a.slot + (size_t)(base + c0 + u) * NN + m) : -1;
+      }
+    };
+    int slc[MB][2], sln[MB][2];
+    load_slots(0, slc);
+    for (int t0 = 0; t0 < MT; t0 += MB) {
+      if (t0 + MB < MT) load_slots(t0 + MB, sln);
+      double acc[MB][2];
+#pragma unroll
+      for (int b = 0; b < MB; b++) {
+        acc[b][0] = 0.0;
+        acc[b][1] = 0.0;
+        if (t0 + b < MT) {
+          const double *tb = sT + (size_t)(t0 + b) * 4 * 32 + lane;
+#pragma unroll
+          for (int s = 0; s < 4; s++) dmma_8x8x4(acc[b][0], acc[b][1], tb[s * 32], bf[s]);
+        }
+      }
+      // L2 reductions (no value returned): the cells of one launch share no
+      // row, so no two adds of a launch meet and the order is the launch order
+#pragma unroll
+      for (int b = 0; b < MB; b++)
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const int q = slc[b][u];
+          if (q >= 0) scatter_entry(a.entries, q, acc[b][u]);
+          else if (q <= -3) a.entries[-3 - q] = 1.0;  // Dirichlet row: unit diagonal (AssembleMat3D.C:840-848)
+        }
+#pragma unroll
+      for (int b = 0; b < MB; b++) {
+        slc[b][0] = sln[b][0];
+        slc[b][1] = sln[b][1];
+      }
+    }
+    // the cells' local rhs (active rows)
+    if (a.rhs)
+      for (int ci = lane; ci < ne * NLOC; ci += 32) {
+        const int di = __ldg(a.elem_dof + (size_t)base * NLOC + ci);
+        if (di < a.Na) atomicAdd(a.rhs + di, __ldg(rbuf + (size_t)base * NLOC + ci));
+      }
+  }
+}
+
 // ----------------------------------------------------------------- slot map
-// slot[e][i][j] = position of column dof_j in the sorted CSR row dof_i
-// (-1 where the row is a Dirichlet row and j != i, or the pair is missing).
+// slot[e][i][j] = position of column dof_j in the sorted CSR row dof_i when
+// dof_i is an active row; for a Dirichlet row -3 - (position of the diagonal)
+// when j = i (the kernels set that entry to 1) and -1 otherwise.  A coupling
+// of an active row missing from the pattern fails the build (flag 2), so the
+// kernels need neither the dofs nor a check to scatter.
 __global__ void k_slot_map(int n_cells, int nloc, int Na, const int *__restrict__ elem_dof,
                            const int *__restrict__ rowptr, const int *__restrict__ kcol, int *__restrict__ slot,
                            int *flags) {
@@ -551,6 +860,7 @@ __global__ void k_slot_map(int n_cells, int nloc, int Na, const int *__restrict_
     if (v < col) lo = mid + 1; else hi = mid - 1;
   }
   if (pos < 0 && row < Na) atomicOr(flags, 2);
+  if (row >= Na) pos = (col == row && pos >= 0) ? -3 - pos : -1;
   slot[tid] = pos;
 }
 
@@ -578,8 +888,25 @@ struct TableCache {
   int elem = -1, rule = -1;
   DBuf<double> utab, qtab;
   DBuf<double> stab;  // 16 x n_loc^2: S_ab[i][j] = sum_q w_q u_ia(q) u_jb(q)
+  // the tensor-core kernel's tables in mma A-fragment order (see k_assemble_tc):
+  // [entry block t][k step s][lane l] = T[8t + l/4][4s + l%4]
+  DBuf<double> tc_const, tc_diff;
+  DBuf<double> rtab;  // 4 x n_loc: R_a[i] = sum_q w_q u_ia(q)
   int nq = 0;
 };
+
+// T[m][k] of k_assemble_tc in A-fragment order; tk(m, k) gives the entry
+static std::vector<double> tc_fragments(int nn, int kd, const std::function<double(int, int)> &tk) {
+  const int mt = (nn + 7) / 8, ks = (kd + 3) / 4;
+  std::vector<double> f((size_t)mt * ks * 32, 0.0);
+  for (int t = 0; t < mt; t++)
+    for (int sk = 0; sk < ks; sk++)
+      for (int l = 0; l < 32; l++) {
+        const int m = 8 * t + (l >> 2), k = 4 * sk + (l & 3);
+        f[((size_t)t * ks + sk) * 32 + l] = (m < nn && k < kd) ? tk(m, k) : 0.0;
+      }
+  return f;
+}
 static TableCache g_tab[4];
 
 // quadrature rule of the reference (TFEDatabase3D::GetOrig, FEDatabase3D.C:1203-1309):
@@ -617,6 +944,23 @@ static int get_tables(int elem, int rule, TableCache *&out) {
     PMG_TRY(T.utab.upload(u.data(), u.size(), 0));
     PMG_TRY(T.qtab.upload(qt.data(), qt.size(), 0));
     PMG_TRY(T.stab.upload(st.data(), st.size(), 0));
+    // CONST: T[m][ab] = S_ab[m]
+    std::vector<double> fc = tc_fragments((int)nn, 16, [&](int m, int k) { return st[(size_t)k * nn + m]; });
+    PMG_TRY(T.tc_const.upload(fc.data(), fc.size(), 0));
+    // DIFF: T[m][(q, p)], p over (00, 11, 22, 01, 02, 12) of the reference gradients
+    static const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+    std::vector<double> fd = tc_fragments((int)nn, 6 * q.n, [&](int m, int k) {
+      const int i = m / nl, j = m % nl, qq = k / 6, pp = k % 6;
+      const double *ui = &u[((size_t)qq * nl + i) * 4], *uj = &u[((size_t)qq * nl + j) * 4];
+      const int x = pa[pp], y = pb[pp];
+      return x == y ? ui[x] * uj[x] : ui[x] * uj[y] + ui[y] * uj[x];
+    });
+    PMG_TRY(T.tc_diff.upload(fd.data(), fd.size(), 0));
+    std::vector<double> rt((size_t)4 * nl, 0.0);
+    for (int a4 = 0; a4 < 4; a4++)
+      for (int i = 0; i < nl; i++)
+        for (int k = 0; k < q.n; k++) rt[(size_t)a4 * nl + i] += q.w[k] * u[((size_t)k * nl + i) * 4 + a4];
+    PMG_TRY(T.rtab.upload(rt.data(), rt.size(), 0));
     PMG_CUDA(cudaDeviceSynchronize());
     T.elem = elem; T.rule = rule; T.nq = q.n;
   }
@@ -633,6 +977,7 @@ static int launch_assemble(Handle &h, Level &L, AsmArgs a) {
     PMG_CUDA(cudaFuncSetAttribute(k_assemble<E, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr_set = true;
   }
+  h.asm_path = 3;
   int per_block = ASM_WARPS * GPW;
   const int *ed0 = a.elem_dof;
   const double *cv0 = a.cell_vert;
@@ -665,6 +1010,7 @@ static int launch_assemble_cc(Handle &h, Level &L, AsmArgs a, const double *stab
     PMG_CUDA(cudaFuncSetAttribute(k_assemble_cc<E, NQ>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     attr_set = true;
   }
+  h.asm_path = 2;
   const int per_block = ASMC_WARPS * ASMC_P;
   const int *ed0 = a.elem_dof;
   const double *cv0 = a.cell_vert;
@@ -679,6 +1025,81 @@ static int launch_assemble_cc(Handle &h, Level &L, AsmArgs a, const double *stab
     b.slot = sl0 + (size_t)beg * NLOC * NLOC;
     int blocks = std::min((n + per_block - 1) / per_block, h.num_sms * 2);
     k_assemble_cc<E, NQ><<<blocks, ASMC_WARPS * 32, smem, h.stream>>>(b, stab); count_launches(1);
+    PMG_CUDA(cudaGetLastError());
+  }
+  return PMG_OK;
+}
+
+// warps per block of k_assemble_tc (0: the table does not leave room for 4)
+template <int E, int NQ, bool DIFF>
+static int tc_warps(int n_modes) {
+  using S = TcShape<E, NQ, DIFF>;
+  const long avail = 227L * 1024 / 8 - (long)S::TABLE_DOUBLES - 8L * n_modes;
+  const long w = std::min(16L, avail / S::WARP_DOUBLES);
+  return w >= 4 ? (int)w : 0;
+}
+
+template <int E, int NQ, bool DIFF>
+static int launch_assemble_tc(Handle &h, Level &L, AsmArgs a, const double *tfrag) {
+  using S = TcShape<E, NQ, DIFF>;
+  const int WARPS = tc_warps<E, NQ, DIFF>(a.coef.n_modes);
+  const size_t smem = sizeof(double) * (S::TABLE_DOUBLES + 8 * (size_t)a.coef.n_modes + (size_t)WARPS * S::WARP_DOUBLES);
+  auto kern = k_assemble_tc<E, NQ, DIFF>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    PMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    attr_set = true;
+  }
+  h.asm_path = DIFF ? 1 : 0;
+  h.asm_kd = S::KD;
+  const int *ed0 = a.elem_dof;
+  const double *cv0 = a.cell_vert;
+  const int *sl0 = a.slot;
+  for (size_t c = 0; c + 1 < L.ecolor_ptr.size(); c++) {
+    const int beg = L.ecolor_ptr[c], n = L.ecolor_ptr[c + 1] - beg;
+    if (n <= 0) continue;
+    AsmArgs b = a;
+    b.n_elems = n;
+    b.elem_dof = ed0 + (size_t)beg * S::NLOC;
+    b.cell_vert = cv0 + (size_t)beg * ET<E>::NV * 3;
+    b.slot = sl0 + (size_t)beg * S::NN;
+    const int blocks = std::min((n + WARPS * 8 - 1) / (WARPS * 8), h.num_sms);
+    kern<<<blocks, WARPS * 32, smem, h.stream>>>(b, tfrag); count_launches(1);
+    PMG_CUDA(cudaGetLastError());
+  }
+  return PMG_OK;
+}
+
+template <int E, int NQ>
+static int launch_assemble_tc16(Handle &h, Level &L, AsmArgs a, const double *tfrag, const double *rtab) {
+  constexpr int NLOC = ET<E>::NLOC, NN = NLOC * NLOC, MT = (NN + 7) / 8, WARPS = 16;
+  const size_t smem = sizeof(double) * (size_t)MT * 4 * 32;
+  static bool attr_set = false;
+  if (!attr_set) {
+    PMG_CUDA(cudaFuncSetAttribute(k_assemble_tc16<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  h.asm_path = 0;
+  h.asm_kd = 16;
+  PMG_TRY(h.tc_dbuf.reserve((size_t)L.n_cells * 16));
+  PMG_TRY(h.tc_rbuf.reserve((size_t)L.n_cells * NLOC));
+  AsmArgs all = a;
+  all.n_elems = L.n_cells;
+  k_tc_setup<E, NQ><<<(L.n_cells + 127) / 128, 128, 0, h.stream>>>(all, h.tc_dbuf.p, a.rhs ? h.tc_rbuf.p : nullptr,
+                                                                     rtab);
+  count_launches(1);
+  PMG_CUDA(cudaGetLastError());
+  for (size_t c = 0; c + 1 < L.ecolor_ptr.size(); c++) {
+    const int beg = L.ecolor_ptr[c], n = L.ecolor_ptr[c + 1] - beg;
+    if (n <= 0) continue;
+    AsmArgs b = a;
+    b.n_elems = n;
+    b.elem_dof = a.elem_dof + (size_t)beg * NLOC;
+    b.slot = a.slot + (size_t)beg * NN;
+    const int blocks = std::min((n + WARPS * 8 - 1) / (WARPS * 8), 2 * h.num_sms);
+    k_assemble_tc16<E><<<blocks, WARPS * 32, smem, h.stream>>>(b, tfrag, h.tc_dbuf.p + (size_t)beg * 16,
+                                                               h.tc_rbuf.p + (size_t)beg * NLOC);
+    count_launches(1);
     PMG_CUDA(cudaGetLastError());
   }
   return PMG_OK;
@@ -716,7 +1137,7 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
     set_error("assemble: PMG_COEF_TABLE needs pmg_set_coefficient_table for this level and quadrature rule");
     return PMG_ERR_STATE;
   }
-  PMG_CUDA(cudaMemsetAsync(target, 0, sizeof(double) * L.nnz, h.stream));
+  PMG_CUDA(cudaMemsetAsync(target, 0, sizeof(double) * L.nnz, h.stream));  // TAssembleMat3D::Reset
   if (rhs_target && zero_rhs) PMG_CUDA(cudaMemsetAsync(rhs_target, 0, sizeof(double) * L.N, h.stream));
   PMG_CUDA(cudaMemsetAsync(h.d_flags.p, 0, sizeof(int) * 4, h.stream));
   AsmArgs a{};
@@ -742,7 +1163,42 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
   a.utab = T->utab.p;
   a.qtab = T->qtab.p;
   a.flags = h.d_flags.p;
-  if (constant_matrix_coefficients(h.coeff.kind) && h.prm.assembly_kernel != 1) {
+  // tensor-core kernel: space-constant coefficients (any element), or pure
+  // diffusion with a varying eps on Q1 / P1 / P2 (whose DIFF table fits in
+  // shared memory)
+  const bool pure_diffusion = h.coeff.kind == PMG_COEF_LOGNORMAL && h.coeff.b[0] == 0.0 && h.coeff.b[1] == 0.0 &&
+                              h.coeff.b[2] == 0.0 && h.coeff.c == 0.0 && form != PMG_FORM_MASS &&
+                              form != PMG_FORM_MASS_SUPG;
+  const int nm = h.coeff.n_modes;
+#define PMG_TC(E_, NQ_, DIFF_) \
+  if (tc_warps<E_, NQ_, DIFF_>(nm)) return launch_assemble_tc<E_, NQ_, DIFF_>(h, L, a, tf); \
+  break
+  if (h.prm.assembly_kernel == 0 && constant_matrix_coefficients(h.coeff.kind)) {
+    const double *tf = T->tc_const.p;
+    switch (L.elem * 1000 + T->nq) {
+      case PMG_ELEM_Q1_HEX * 1000 + 8: return launch_assemble_tc16<PMG_ELEM_Q1_HEX, 8>(h, L, a, tf, T->rtab.p);
+      case PMG_ELEM_Q1_HEX * 1000 + 27: return launch_assemble_tc16<PMG_ELEM_Q1_HEX, 27>(h, L, a, tf, T->rtab.p);
+      case PMG_ELEM_Q2_HEX * 1000 + 27: return launch_assemble_tc16<PMG_ELEM_Q2_HEX, 27>(h, L, a, tf, T->rtab.p);
+      case PMG_ELEM_Q2_HEX * 1000 + 64: return launch_assemble_tc16<PMG_ELEM_Q2_HEX, 64>(h, L, a, tf, T->rtab.p);
+      case PMG_ELEM_P1_TET * 1000 + 4: return launch_assemble_tc16<PMG_ELEM_P1_TET, 4>(h, L, a, tf, T->rtab.p);
+      case PMG_ELEM_P1_TET * 1000 + 11: return launch_assemble_tc16<PMG_ELEM_P1_TET, 11>(h, L, a, tf, T->rtab.p);
+      case PMG_ELEM_P2_TET * 1000 + 11: return launch_assemble_tc16<PMG_ELEM_P2_TET, 11>(h, L, a, tf, T->rtab.p);
+      default: break;
+    }
+  }
+  if (h.prm.assembly_kernel == 0 && pure_diffusion) {
+    const double *tf = T->tc_diff.p;
+    switch (L.elem * 1000 + T->nq) {
+      case PMG_ELEM_Q1_HEX * 1000 + 8: PMG_TC(PMG_ELEM_Q1_HEX, 8, true);
+      case PMG_ELEM_Q1_HEX * 1000 + 27: PMG_TC(PMG_ELEM_Q1_HEX, 27, true);
+      case PMG_ELEM_P1_TET * 1000 + 4: PMG_TC(PMG_ELEM_P1_TET, 4, true);
+      case PMG_ELEM_P1_TET * 1000 + 11: PMG_TC(PMG_ELEM_P1_TET, 11, true);
+      case PMG_ELEM_P2_TET * 1000 + 11: PMG_TC(PMG_ELEM_P2_TET, 11, true);
+      default: break;
+    }
+  }
+#undef PMG_TC
+  if (h.prm.assembly_kernel == 2 && constant_matrix_coefficients(h.coeff.kind)) {
     const double *st = T->stab.p;
     switch (L.elem * 1000 + T->nq) {
       case PMG_ELEM_Q1_HEX * 1000 + 8: return launch_assemble_cc<PMG_ELEM_Q1_HEX, 8>(h, L, a, st);

@@ -74,7 +74,7 @@ static int validate_params(const pmg_params *p) {
   if (p->restart < 1 || p->restart > 60) return bad("restart must be in [1,60]");
   if (p->lin_maxit < 1) return bad("lin_maxit must be >= 1");
   if (p->precision != PMG_PREC_FP64 && p->precision != PMG_PREC_FP32) return bad("precision must be PMG_PREC_FP64 or _FP32");
-  if (p->assembly_kernel != 0 && p->assembly_kernel != 1) return bad("assembly_kernel must be 0 or 1");
+  if (p->assembly_kernel < 0 || p->assembly_kernel > 2) return bad("assembly_kernel must be 0, 1 or 2");
   if (p->problem_linear != 0 && p->problem_linear != 1) return bad("problem_linear must be 0 or 1");
   if (p->reference_restart_rule != 0 && p->reference_restart_rule != 1) return bad("reference_restart_rule must be 0 or 1");
   if ((p->slc_all != 0 && p->slc_all != 1) || (p->slc_fine != 0 && p->slc_fine != 1)) return bad("slc_all / slc_fine must be 0 or 1");
@@ -732,6 +732,12 @@ int pmg_time_kernel(pmg_handle hh, int kernel, int level, int form, int reps, do
     fl = L.n_cells * (nq * nl * nl * 8 + nq * nl * 32);  // 4 FMA per (q,i,j) + D_q u_j (16 FMA per q,j)
   }
   PMG_TRY(run());  // warm-up
+  if (kernel == PMG_KERNEL_ASSEMBLE) {
+    // flops of the contraction the chosen kernel does
+    const double nn = (double)L.nloc * L.nloc;
+    if (h->asm_path <= 1) fl = L.n_cells * nn * 2.0 * h->asm_kd;
+    else if (h->asm_path == 2) fl = L.n_cells * nn * 2.0 * 16;
+  }
   PMG_CUDA(cudaEventRecord(h->ev[4], s));
   for (int r = 0; r < reps; r++) PMG_TRY(run());
   PMG_CUDA(cudaEventRecord(h->ev[5], s));

@@ -73,6 +73,11 @@ struct DBuf {
     n = count;
     return PMG_OK;
   }
+  // grow only: keep the buffer when it already holds count elements
+  int reserve(size_t count) {
+    if (p && n >= count) return PMG_OK;
+    return alloc(count);
+  }
   int upload(const T *h, size_t count, cudaStream_t s) {
     PMG_TRY(alloc(count));
     if (count) PMG_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
@@ -201,6 +206,12 @@ struct Handle {
   // timing
   cudaEvent_t ev[10];
   double t_assemble = 0, t_solve = 0, t_assemble_kernel = 0;
+  // kernel of the last assemble_level: 0 tensor-core (space-constant
+  // coefficients), 1 tensor-core (pure diffusion), 2 reference matrices on
+  // CUDA cores, 3 per quadrature point; asm_kd: contraction length of 0 / 1
+  int asm_path = 3, asm_kd = 0;
+  // per-cell coefficients (16) and local rhs of the space-constant tensor-core assembly
+  DBuf<double> tc_dbuf, tc_rbuf;
   // V-cycle graph
   cudaGraphExec_t vgraph = nullptr;
   int vgraph_prec = -1;

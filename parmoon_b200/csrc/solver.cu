@@ -921,13 +921,15 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
     st->res_final = res_final;
     st->rel_res = res0 > 0 ? res_final / res0 : 0.0;
     st->mean_contraction = (iters > 0 && res0 > 0 && res_final > 0) ? pow(res_final / res0, 1.0 / iters) : 0.0;
-    st->smoother_used = (learned && guard_phase == 1) ? PMG_SMOOTHER_LEARNED : PMG_SMOOTHER_SSOR;
+    st->smoother_used = learned ? (guard_phase == 1 ? PMG_SMOOTHER_LEARNED : PMG_SMOOTHER_SSOR) : h.prm.smoother;
     st->seconds = h.t_solve;
     float a = 0, b = 0;
     st->setup_seconds = cudaEventElapsedTime(&a, h.ev[2], h.ev[6]) == cudaSuccess ? a * 1e-3 : 0.0;
     st->vcycle_seconds = (vc_timed && cudaEventElapsedTime(&b, h.ev[7], h.ev[8]) == cudaSuccess) ? b * 1e-3 : 0.0;
     cudaGetLastError();
   }
+  if (status == PMG_ERR_NOT_CONVERGED)
+    set_error("solve: the iteration limit (lin_maxit) was reached before |r| <= max(lin_res_min, lin_red |r0|)");
   return status;
 }
 

@@ -1,8 +1,11 @@
-"""The two assembly kernels agree: for coefficients constant in space the
-library assembles A = |det J| sum_ab D_ab S_ab from reference matrices
-(assembly_kernel = 0, automatic); the per-quadrature-point kernel
-(assembly_kernel = 1) sums over the points.  Same matrices and rhs up to
-rounding order: 1e-13 relative to the largest entry of the row."""
+"""The assembly kernels agree.  For coefficients constant in space the
+library assembles A = |det J| sum_ab D_ab S_ab from reference matrices, on the
+FP64 tensor cores (assembly_kernel = 0, automatic) or on the FP64 CUDA cores
+(assembly_kernel = 2); for pure diffusion with a varying eps on Q1 / P1 / P2
+the tensor-core kernel contracts per-point coefficients with a reference
+table; the per-quadrature-point kernel (assembly_kernel = 1) sums over the
+points.  Same matrices and rhs up to rounding order: 1e-13 relative to the
+largest entry of the row."""
 import numpy as np
 import pytest
 
@@ -12,14 +15,20 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("elem,form,kind,jitter,linear", [
     ("Q2_HEX", "SUPG", "CONST", 0.0, 1), ("Q2_HEX", "SUPG", "CONST", 0.0, 0), ("Q1_HEX", "SUPG", "SINE_RHS", 0.0, 1),
     ("Q1_HEX", "MASS_SUPG", "CONST", 0.0, 1), ("P2_TET", "SUPG", "CONST", 0.2, 1), ("P1_TET", "GALERKIN", "AMC", 0.2, 1),
-    ("Q2_HEX", "MASS", "AMC", 0.0, 1)])
+    ("Q2_HEX", "MASS", "AMC", 0.0, 1), ("P2_TET", "STIFF_SUPG", "CONST", 0.2, 1), ("Q1_HEX", "GALERKIN", "CONST", 0.0, 0),
+    ("P2_TET", "GALERKIN", "LOGNORMAL", 0.2, 1), ("Q1_HEX", "GALERKIN", "LOGNORMAL", 0.0, 1),
+    ("P1_TET", "SUPG", "LOGNORMAL", 0.2, 0), ("Q1_HEX", "GALERKIN", "LOGNORMAL", 0.0, 0)])
 def test_reference_matrix_kernel_equals_point_kernel(pmg, elem, form, kind, jitter, linear):
+    from parmoon_b200.configs import lognormal_modes
     et = getattr(pmg, elem)
     fm = getattr(pmg, "FORM_" + form)
     levels = pmg.struct_hierarchy(et, 4, 2, jitter=jitter, seed=7)
-    ck = pmg.coeff(kind=getattr(pmg, "COEF_" + kind), eps=1e-3, b=(1.0, -0.5, 0.25), c=0.3, f=2.0, t=0.4)
+    if kind == "LOGNORMAL":  # pure diffusion: b = 0, c = 0
+        ck = pmg.coeff(kind=pmg.COEF_LOGNORMAL, eps=1e-2, f=2.0, modes=lognormal_modes(3))
+    else:
+        ck = pmg.coeff(kind=getattr(pmg, "COEF_" + kind), eps=1e-3, b=(1.0, -0.5, 0.25), c=0.3, f=2.0, t=0.4)
     out = []
-    for path in (0, 1):
+    for path in (0, 1, 2):
         h = pmg.Handle(2, pmg.default_params(assembly_kernel=path, problem_linear=linear))
         h.set_coefficients(ck)
         pmg.load_hierarchy(h, levels, dirichlet=lambda x, y, z: x + 2 * y - z)
@@ -27,8 +36,10 @@ def test_reference_matrix_kernel_equals_point_kernel(pmg, elem, form, kind, jitt
         out.append([(h.get_matrix(l, 1 if form.startswith("MASS") else 0), h.get_rhs(l)) for l in range(2)])
         h.close()
     for l, L in enumerate(levels):
-        (A0, r0), (A1, r1) = out[0][l], out[1][l]
+        A1, r1 = out[1][l]
         rows = np.repeat(np.arange(L["N"]), np.diff(L["rowptr"]))
         rowmax = np.maximum.reduceat(np.abs(A1), L["rowptr"][:-1])[rows]
-        assert np.max(np.abs(A0 - A1) / rowmax) <= 1e-13
-        assert np.max(np.abs(r0 - r1)) <= 1e-13 * max(1.0, np.max(np.abs(r1)))
+        for path in (0, 2):
+            A0, r0 = out[path][l]
+            assert np.max(np.abs(A0 - A1) / rowmax) <= 1e-13, path
+            assert np.max(np.abs(r0 - r1)) <= 1e-13 * max(1.0, np.max(np.abs(r1))), path
