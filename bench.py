@@ -395,6 +395,28 @@ def bench_ours(args, rank, world, dist):
         e2e_t.append(time.perf_counter() - t0)
     e2e = statistics.median(e2e_t)
 
+    # level set-up of the finest level (TSquareStructure3D + Sort): host builder
+    # (OpenMP) against the device builder (pmg_build_level_csr: pattern on the
+    # device, then installed with pattern checks, row colouring and host mirror)
+    import ctypes as C_
+    rp_h = np.empty(N + 1, dtype=np.int32)
+    ed = np.ascontiguousarray(Fl["elem_dof"], dtype=np.int32)
+    t0 = time.perf_counter()
+    P._check(lib.pmg_struct_csr(C_.c_int(ed.size // 27), C_.c_int(27), ed.ctypes.data_as(C_.c_void_p), C_.c_int(N),
+                                C_.c_int(Fl["active_bound"]), rp_h.ctypes.data_as(C_.c_void_p), None))
+    kc_h = np.empty(int(rp_h[-1]), dtype=np.int32)
+    P._check(lib.pmg_struct_csr(C_.c_int(ed.size // 27), C_.c_int(27), ed.ctypes.data_as(C_.c_void_p), C_.c_int(N),
+                                C_.c_int(Fl["active_bound"]), rp_h.ctypes.data_as(C_.c_void_p),
+                                kc_h.ctypes.data_as(C_.c_void_p)))
+    t_host_csr = time.perf_counter() - t0
+    hs = P.Handle(1)
+    t0 = time.perf_counter()
+    hs.build_level_csr(0, ed, 27, N, Fl["active_bound"])
+    t_dev_csr = time.perf_counter() - t0
+    c_dev, c_inst = C_.c_double(), C_.c_double()
+    P._check(lib.pmg_setup_timings(hs.h, C_.byref(c_dev), C_.byref(c_inst)))
+    hs.close()
+
     # plain FP64 GMG on the same problem (the method the FP32 V-cycle is compared with)
     x32 = h.get_solution()
     h.set_params(P.default_params(precision=P.PREC_FP64, restart=RESTART))
@@ -444,6 +466,11 @@ def bench_ours(args, rank, world, dist):
             "fp64_gmg": {"solve_s": fp64_s, "iterations": fp64[0][1], "rel_res": fp64[0][2], "status": fp64[0][3],
                          "vcycle_s": fp64[0][4]},
             "err_vs_fp64": err,
+            "setup_csr_s": {"host_builder": t_host_csr, "device_builder": c_dev.value,
+                            "device_entry_total": t_dev_csr, "device_entry_install": c_inst.value,
+                            "note": "finest-level CSR pattern (TSquareStructure3D + Sort), wall time; "
+                                    "device_builder = the pattern on the device (upload included); the entry "
+                                    "then installs it (pattern checks, greedy row colouring, host mirror)"},
             "fp32_solve_s": statistics.mean(s.seconds for s in stats),
             "fp32_solve_setup_s": statistics.mean(s.setup_seconds for s in stats),
             "fp32_vcycle_s": statistics.mean(s.vcycle_seconds for s in stats),

@@ -164,6 +164,23 @@ int pmg_set_level_mesh(pmg_handle h, int level, int elem_type, int n_cells,
 int pmg_set_level_csr(pmg_handle h, int level, int n_rows, int active_bound,
                       const int *row_ptr, const int *kcol);
 
+/* The same pattern built on the device from the element -> dof map
+ * (GlobalNumbers + BeginIndex flattened, n_cells x nloc): every dof of every
+ * cell holding an active row, sorted; a Dirichlet row (>= active_bound) its
+ * diagonal alone -- what TSquareStructure3D + Sort produce for conforming
+ * spaces.  Installed as the level's pattern as pmg_set_level_csr would;
+ * nnz_out (may be NULL) receives its size.  Rows may gather at most 1024
+ * candidate columns (incident cells x nloc), else PMG_ERR_UNSUPPORTED. */
+int pmg_build_level_csr(pmg_handle h, int level, int n_rows, int active_bound, int n_cells, int nloc,
+                        const int *elem_dof, int *nnz_out);
+/* Wall times of the last pmg_build_level_csr: the pattern built on the device
+ * (element map upload included) and its installation (pattern checks, greedy
+ * row colouring, host mirror). */
+int pmg_setup_timings(pmg_handle h, double *csr_device_s, double *csr_install_s);
+/* Copy a level's pattern out (TSquareStructure3D::GetRowPtr / GetKCol
+ * consumers): row_ptr n_rows + 1 entries, kcol (may be NULL) nnz entries. */
+int pmg_get_level_csr(pmg_handle h, int level, int *row_ptr, int *kcol);
+
 /* Optional multicolour ordering of the rows of one level for the parallel
  * SSOR (n_rows colour ids in [0, n_colors)).  Rows sharing a matrix entry
  * must have different colours.  Without it a greedy colouring is built. */
@@ -175,6 +192,16 @@ int pmg_set_level_row_colors(pmg_handle h, int level, int n_colors, const int *c
  * Restriction is its transpose (DefectRestriction, :732-1014). */
 int pmg_set_transfer(pmg_handle h, int level, int n_fine, int n_coarse,
                      const int *p_row_ptr, const int *p_col, const double *p_val);
+
+/* The prolongation from level-1 to level built on the device for conforming
+ * nested spaces (what pmg_nested_prolongation in pmg_mesh.h builds on the
+ * host): fine dof r (position f_dof_xyz[3r..3r+2]) lies in coarse cell
+ * f_dof_cell[r] (the caller's cell index of level-1, whose mesh must be set);
+ * its row holds that cell's coarse basis at the dof, entries below 1e-12
+ * dropped.  R = P^T is formed on the device.  pmg_get_transfer copies P out
+ * (p_row_ptr n_fine + 1 entries; p_col / p_val may be NULL). */
+int pmg_build_transfer(pmg_handle h, int level, int n_fine, const double *f_dof_xyz, const int *f_dof_cell);
+int pmg_get_transfer(pmg_handle h, int level, int *p_row_ptr, int *p_col, double *p_val);
 
 /* Dirichlet values of one level (the BoundValueFunct3D callback evaluated at
  * the dof nodes, AssembleMat3D.C:1031-1081): n_rows - active_bound values. */
@@ -274,6 +301,20 @@ int pmg_solve(pmg_handle h, double *sol, const double *rhs, pmg_solve_stats *sta
 
 /* Copy the device-resident finest-level solution out. */
 int pmg_get_solution(pmg_handle h, double *sol_out);
+
+/* ------------------------------------------------------------ output */
+/* TOutput3D::WriteVtk (src/FE/Output3D.C:1773-2292) for one scalar function:
+ * legacy ASCII VTK unstructured grid of the level's cells (VTK_HEXAHEDRON /
+ * VTK_TETRA, corners in the cell's own vertex order, the caller's cell order)
+ * with the function's vertex values as POINT_DATA `name` and the cells'
+ * region ids (region_ids, n_cells values, or NULL for 0) as CELL_DATA
+ * RegionID.  values: host array of the level's N coefficients, or NULL for
+ * the device-resident solution of the finest level (the last pmg_solve); the
+ * vertex values are gathered on the device.  Vertices are numbered in dof
+ * order (the reference numbers them by memory address, so files agree up to
+ * that numbering). */
+int pmg_write_vtk(pmg_handle h, int level, const double *values, const int *region_ids, const char *path,
+                  const char *name);
 
 /* ------------------------------------------------------------ learned smoother */
 /* No counterpart in the reference.  A stencil network maps each node's

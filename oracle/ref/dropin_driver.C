@@ -16,6 +16,10 @@
 #include <SystemCD3D.h>
 #include <LinAlg.h>
 #include <MooNMD_Io.h>
+#include <FEFunction3D.h>
+#include <Output3D.h>
+#include <Collection.h>
+#include <BaseCell.h>
 #include "../../parmoon_b200/shim/pmg_parmoon.h"
 
 #include <chrono>
@@ -193,6 +197,20 @@ int main(int argc, char **argv) {
          "pmg_iterations=%d t_ref_assemble=%.4f t_pmg_assemble=%.4f t_ref_solve=%.4f t_pmg_solve=%.4f\n",
          N, levels, mat / mat_scale, rhs / rhs_scale, sol / sol_scale, res_ref, res_pmg,
          P->GetSolveStats().iterations, t_ref_asm, t_pmg_asm, t_ref_solve, t_pmg_solve);
+  // vtk=1: the finest solution of each arm as a VTK file, the reference's
+  // through TOutput3D::WriteVtk (as CD3D_ParMooN.C:477-495), ours through
+  // pmg_write_vtk from the device-resident solution
+  if (optd("vtk", 0) != 0) {
+    TFEFunction3D *fe = new TFEFunction3D(sp[F], Name, Desc, Sol_ref[F], N);
+    TOutput3D *out3 = new TOutput3D(2, 2, 1, 1, Domain);
+    out3->AddFEFunction(fe);
+    out3->WriteVtk((out + "/ref.vtk").c_str());
+    TCollection *coll = sp[F]->GetCollection();
+    std::vector<int> region(coll->GetN_Cells());
+    for (int c = 0; c < coll->GetN_Cells(); c++) region[c] = coll->GetCell(c)->GetRegionID();
+    const int rc = pmg_write_vtk(P->GetHandle(), F, NULL, region.data(), (out + "/pmg.vtk").c_str(), Name);
+    printf("vtk status=%d\n", rc);
+  }
   delete P;
   (void)Database; (void)FEDatabase;
   return 0;

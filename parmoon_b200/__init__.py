@@ -161,6 +161,36 @@ class Handle:
                                         _ptr(cell_vert), _i(int(brick))))
         self._ncells[level] = n_cells
 
+    def build_level_csr(self, level, elem_dof, nloc, n_rows, active_bound):
+        """TSquareStructure3D + Sort on the device from the element->dof map; returns nnz."""
+        ed = _c_i32(elem_dof)
+        nnz = _i()
+        _check(lib().pmg_build_level_csr(self.h, _i(level), _i(n_rows), _i(active_bound), _i(ed.size // nloc),
+                                         _i(nloc), _ptr(ed), ctypes.byref(nnz)))
+        self.sizes[level] = (n_rows, nnz.value, active_bound)
+        return nnz.value
+
+    def get_level_csr(self, level):
+        n, nnz, _ = self.sizes[level]
+        rp = np.empty(n + 1, dtype=np.int32)
+        kc = np.empty(nnz, dtype=np.int32)
+        _check(lib().pmg_get_level_csr(self.h, _i(level), _ptr(rp), _ptr(kc)))
+        return rp, kc
+
+    def build_transfer(self, level, f_dof_xyz, f_dof_cell):
+        """The prolongation from level-1 built on the device (fine dof r in coarse cell f_dof_cell[r])."""
+        xyz, fc = _c_f64(f_dof_xyz), _c_i32(f_dof_cell)
+        _check(lib().pmg_build_transfer(self.h, _i(level), _i(fc.size), _ptr(xyz), _ptr(fc)))
+
+    def get_transfer(self, level):
+        n = self.sizes[level][0]
+        rp = np.empty(n + 1, dtype=np.int32)
+        _check(lib().pmg_get_transfer(self.h, _i(level), _ptr(rp), None, None))
+        col = np.empty(int(rp[-1]), dtype=np.int32)
+        val = np.empty(int(rp[-1]))
+        _check(lib().pmg_get_transfer(self.h, _i(level), _ptr(rp), _ptr(col), _ptr(val)))
+        return rp, col, val
+
     def set_row_colors(self, level, colors, n_colors):
         colors = _c_i32(colors)
         _check(lib().pmg_set_level_row_colors(self.h, _i(level), _i(n_colors), _ptr(colors)))
@@ -315,6 +345,14 @@ class Handle:
         x = _out_f64(out, self.sizes[-1][0])
         _check(lib().pmg_get_solution(self.h, _ptr(x)))
         return x
+
+    def write_vtk(self, path, name="u", level=-1, values=None, region_ids=None):
+        """Legacy VTK file of a level's function (TOutput3D::WriteVtk); values=None
+        writes the device-resident solution of the finest level."""
+        lv = self.n_levels - 1 if level < 0 else level
+        v = None if values is None else _c_f64(values)
+        r = None if region_ids is None else _c_i32(region_ids)
+        _check(lib().pmg_write_vtk(self.h, _i(lv), _ptr(v), _ptr(r), str(path).encode(), name.encode()))
 
     def timings(self):
         a, s, k = _d(), _d(), _d()

@@ -210,6 +210,9 @@ struct Handle {
   // coefficients), 1 tensor-core (pure diffusion), 2 reference matrices on
   // CUDA cores, 3 per quadrature point; asm_kd: contraction length of 0 / 1
   int asm_path = 3, asm_kd = 0;
+  // wall times of the last pmg_build_level_csr: pattern on the device (upload
+  // included), install (checks, colouring, host mirror)
+  double t_setup_csr_device = 0, t_setup_csr_install = 0;
   // per-cell coefficients (16) and local rhs of the space-constant tensor-core assembly
   DBuf<double> tc_dbuf, tc_rbuf;
   // V-cycle graph
