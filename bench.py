@@ -410,6 +410,7 @@ def bench_ours(args, rank, world, dist):
                                 kc_h.ctypes.data_as(C_.c_void_p)))
     t_host_csr = time.perf_counter() - t0
     hs = P.Handle(1)
+    hs.build_level_csr(0, ed, 27, N, Fl["active_bound"])  # first use: module loading, allocations
     t0 = time.perf_counter()
     hs.build_level_csr(0, ed, 27, N, Fl["active_bound"])
     t_dev_csr = time.perf_counter() - t0

@@ -63,6 +63,7 @@ struct CcArgs {
   const double *a0;
   double *t0;            // reduced rhs f_a - A_ad f_d
   int *err;              // set to 1 when a bounded wait gives up
+  unsigned extra_tx;     // bytes expected on top of a pass's updates: 0, except in the test of the give-up path
   T omega, damp;
 };
 
@@ -76,7 +77,8 @@ struct CcCtx {
   unsigned mbar;  // shared address of the two pass mbarriers (8 bytes apart)
   unsigned pc;    // Gauss-Seidel passes completed so far (selects mbarrier and parity)
   int *err;       // set when a wait gives up
-  bool failed;    // this thread's wait gave up: no further waits
+  unsigned extra_tx;  // see CcArgs
+  bool failed;    // a wait of this CTA gave up: no further sends, expects or waits
   __device__ void sync() { cl.sync(); }
   // x_i := v in every CTA's copy
   __device__ void bcast(int off, int i, T v) {
@@ -253,8 +255,7 @@ struct CcGs {
   // buffer), and the update sent to every CTA's copy; the K warps of a slice
   // share the sends
   template <int K>
-  __device__ __forceinline__ void run_k(const CcCtx<T> &c, const CcLevel<T> &L, T omega, T (*part)[32],
-                                        unsigned mbar) {
+  __device__ __forceinline__ void run_k(CcCtx<T> &c, const CcLevel<T> &L, T omega, T (*part)[32], unsigned mbar) {
     const T *x = c.xs + L.xoff;
     const bool active = sl < s1;
     T sum = 0, xr = 0;
@@ -282,8 +283,10 @@ struct CcGs {
       if (row >= 0) xr = x[row];
     }
     part[c.warp][c.lane] = sum;
-    __syncthreads();
-    if (active && row >= 0) {
+    // the CTA barrier of the cross-warp sum also makes a failed wait of the
+    // previous pass (seen by any thread) known to the whole CTA
+    c.failed = __syncthreads_or(c.failed) != 0;
+    if (active && row >= 0 && !c.failed) {
       const int w0 = c.warp - k;
       T s = 0;
 #pragma unroll
@@ -293,7 +296,7 @@ struct CcGs {
       for (int b = k; b < c.nblocks; b += K) st_async(cluster_addr(a, b), v, cluster_addr(mbar, b));
     }
   }
-  __device__ __forceinline__ void run(const CcCtx<T> &c, const CcLevel<T> &L, T omega, T (*part)[32], unsigned mbar) {
+  __device__ __forceinline__ void run(CcCtx<T> &c, const CcLevel<T> &L, T omega, T (*part)[32], unsigned mbar) {
     run_k<16>(c, L, omega, part, mbar);
   }
 };
@@ -325,11 +328,17 @@ __device__ void cc_ssor(CcCtx<T> &c, const CcLevel<T> &L, T omega, bool dirichle
   auto colour = [&](int p) { return p < nc ? p : 2 * nc - 1 - p; };
   auto pass = [&](CcGs<T> &g, int p) {
     const unsigned mbar = c.mbar + 8 * (c.pc & 1);
-    if (threadIdx.x == 0) mbar_expect(mbar, (unsigned)(L.rows[colour(p)] * sizeof(T)));
+    if (threadIdx.x == 0 && !c.failed) mbar_expect(mbar, (unsigned)(L.rows[colour(p)] * sizeof(T)) + c.extra_tx);
     g.run(c, L, omega, c.part + (c.pc & 1) * CC_WARPS, mbar);
     if (p + 2 < 2 * nc) g.load(c, L, colour(p + 2));
-    // after one wait has given up (error flagged), the rest of the launch runs
-    // without waiting so that it ends; its result is discarded by the host
+    // Give-up path: a CTA whose wait runs out flags the error and from its next
+    // pass on (once its CTA barrier has spread the failure) sends, expects and
+    // waits no more; a peer still waiting for its updates then runs out in turn,
+    // so every CTA ends up failed, runs the rest of the control flow (the
+    // cluster barriers) without waits and ends; the host discards the result
+    // (PMG_ERR_STATE).  Updates sent before a CTA failed may still be in flight
+    // towards a failed receiver: the grace period at the end of the kernel keeps
+    // every receiver resident until they have landed.
     if (!c.failed && !mbar_wait(mbar, (c.pc >> 1) & 1)) {
       c.failed = true;
       atomicExch(c.err, 1);
@@ -364,6 +373,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, 1) k_coarse_cycle(const __grid_
   c.mbar = smem_addr(mbars);
   c.pc = 0;
   c.err = a.err;
+  c.extra_tx = a.extra_tx;
   c.failed = false;
   if (threadIdx.x == 0) {
     mbar_init(c.mbar, 1);
@@ -455,8 +465,18 @@ __global__ void __launch_bounds__(CC_WARPS * 32, 1) k_coarse_cycle(const __grid_
     c.sync();
     for (int s = 0; s < a.post; s++) cc_ssor(c, L, a.omega, s == 0);
   }
-  // every CTA has received all updates; none leaves while a send may be in flight
+  // Without a failed wait every CTA has received all updates of every pass, so
+  // no send is in flight once the cluster barrier below is passed.  After a
+  // failure that does not hold: every CTA stopped sending before it arrived at
+  // the barrier, and a send takes well under a microsecond to land, so a
+  // failed CTA stays resident 200 us more (bounded) before it exits.
+  const bool any_failed = __syncthreads_or(c.failed) != 0;
   c.sync();
+  if (any_failed) {
+    const unsigned long long t0 = global_ns();
+    while (global_ns() - t0 < 200000ull) {
+    }
+  }
   // the entry level's iterate back to global memory for the finer level
   const CcLevel<T> &E = a.lv[top];
   for (int i = c.rank * blockDim.x + threadIdx.x; i < E.N; i += c.nblocks * blockDim.x) __stcg(E.x + i, c.xs[E.xoff + i]);
@@ -640,6 +660,13 @@ int coarse_cycle(Handle &h, int top) {
   a.a0 = h.lv[0].A.p;
   a.t0 = h.coarse_t.p;
   a.err = h.cc_err.p;
+  // PMG_TEST_CC_EXTRA_TX=<bytes>: every pass expects that many bytes that no
+  // CTA sends, so every wait runs out -- the test of the give-up path (read at
+  // every launch; a captured V-cycle graph keeps the value it was captured with)
+  {
+    const char *e = getenv("PMG_TEST_CC_EXTRA_TX");
+    a.extra_tx = e ? (unsigned)atoi(e) : 0u;
+  }
   a.coarse_it = h.prm.coarse_maxit > 0 ? h.prm.coarse_maxit : 1;
   a.pre = h.prm.pre_smooth;
   a.post = h.prm.post_smooth;
