@@ -299,6 +299,37 @@ int pmg_restrict(pmg_handle h, int level, const double *fine, double *coarse);
  * device (start vector = assembled Dirichlet values, zero elsewhere). */
 int pmg_solve(pmg_handle h, double *sol, const double *rhs, pmg_solve_stats *stats);
 
+/* ------------------------------------------------------------ domain decomposition */
+/* The parallel path of the reference (TParFECommunicator3D::CommUpdate /
+ * CommUpdateReduce and the all-reduced inner products, src/Parallel/
+ * ParFECommunicator3D.C:218-346, src/FE/MGLevel3D.C:220-272) with the transport
+ * left to the caller.  Each rank's handle holds one subdomain: its levels are
+ * the cells of the subdomain plus a layer of neighbouring cells, numbered with
+ * the rank's active owned dofs first; its own Dirichlet dofs and the ghost
+ * dofs (dofs of the neighbouring layer owned by other ranks) are rows past
+ * active_bound.  pmg_set_halo names, on the finest level, the owned dofs the
+ * neighbours need (send_idx, packed in the order the transport delivers them)
+ * and the ghost rows (recv_idx) filled from the neighbours, with two device
+ * buffers of n_send / n_recv doubles the transport reads and writes. */
+typedef struct pmg_comm {
+    void *ctx;
+    /* sum v[0..n) over all ranks in place (host memory); 0 on success */
+    int (*allreduce_sum)(void *ctx, double *v, int n);
+    /* send_dev (n_send doubles, packed by the library) to the neighbours and
+     * fill recv_dev (n_recv doubles) with theirs; called after the library's
+     * stream is idle, must return with recv_dev written; 0 on success */
+    int (*exchange)(void *ctx, const double *send_dev, int n_send, double *recv_dev, int n_recv);
+} pmg_comm;
+int pmg_set_halo(pmg_handle h, int n_send, const int *send_idx, int n_recv, const int *recv_idx,
+                 double *send_buf_dev, double *recv_buf_dev);
+/* FGMRES over the ranks' subdomains (every rank calls it with its own handle
+ * and the same parameters): products with the neighbours' ghost values, every
+ * inner product summed over the ranks, each rank's V-cycle on its subdomain
+ * with the ghost rows held at zero as the preconditioner (overlapping additive
+ * Schwarz with multigrid inside each subdomain).  sol / rhs / stats as
+ * pmg_solve (local arrays; only the owned entries of sol are the solution). */
+int pmg_solve_dd(pmg_handle h, const pmg_comm *comm, double *sol, const double *rhs, pmg_solve_stats *stats);
+
 /* Copy the device-resident finest-level solution out. */
 int pmg_get_solution(pmg_handle h, double *sol_out);
 

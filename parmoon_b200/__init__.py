@@ -341,6 +341,23 @@ class Handle:
         """z = MG(v) on device vectors of the finest level."""
         _check(lib().pmg_vcycle(self.h, _p(v_ptr), _p(z_ptr)))
 
+    def set_halo(self, send_idx, recv_idx, send_buf_ptr, recv_buf_ptr):
+        """Halo of a subdomain's finest level (pmg_set_halo): owned rows packed for the
+        neighbours, ghost rows filled from them, device buffers of the transport."""
+        si, ri = _c_i32(send_idx), _c_i32(recv_idx)
+        _check(lib().pmg_set_halo(self.h, _i(si.size), _ptr(si), _i(ri.size), _ptr(ri), _p(send_buf_ptr),
+                                  _p(recv_buf_ptr)))
+
+    def solve_dd(self, comm, sol=None, rhs=None, raise_on_error=True):
+        """FGMRES over the ranks' subdomains (pmg_solve_dd) with a pmg_comm structure."""
+        st = SolveStats()
+        sol = None if sol is None else np.array(sol, dtype=np.float64)
+        rhs = None if rhs is None else _c_f64(rhs)
+        rc = lib().pmg_solve_dd(self.h, ctypes.byref(comm), _ptr(sol), _ptr(rhs), ctypes.byref(st))
+        if raise_on_error and rc != OK:
+            _check(rc)
+        return sol, st, rc
+
     def get_solution(self, out=None):
         x = _out_f64(out, self.sizes[-1][0])
         _check(lib().pmg_get_solution(self.h, _ptr(x)))
@@ -386,6 +403,17 @@ def struct_level(elem, n, jitter=0.0, seed=0):
     _check(lib().pmg_struct_row_colors(_i(elem), _i(n), N, _ptr(lat), _ptr(colors), ctypes.byref(ncol)))
     return dict(elem=elem, n=n, elem_dof=ed, cell_vert=cv, dof_xyz=xyz.reshape(-1, 3), dof_lat=lat, N=N.value,
                 active_bound=ab.value, n_cells=nc.value, rowptr=rp, kcol=kc, colors=colors, n_colors=ncol.value)
+
+
+def struct_csr_of(elem_dof, nloc, n_dofs, active_bound):
+    """TSquareStructure3D + Sort of any element->dof map (host builder): (rowptr, kcol)."""
+    ed = _c_i32(elem_dof)
+    rp = np.empty(n_dofs + 1, dtype=np.int32)
+    _check(lib().pmg_struct_csr(_i(ed.size // nloc), _i(nloc), _ptr(ed), _i(n_dofs), _i(active_bound), _ptr(rp), None))
+    kc = np.empty(int(rp[-1]), dtype=np.int32)
+    _check(lib().pmg_struct_csr(_i(ed.size // nloc), _i(nloc), _ptr(ed), _i(n_dofs), _i(active_bound), _ptr(rp),
+                                _ptr(kc)))
+    return rp, kc
 
 
 def struct_prolongation(elem, nc, lat_c, lat_f):

@@ -234,6 +234,12 @@ struct Handle {
   unsigned long long vgraph_ssor_kernels = 0;
   double *h_pinned = nullptr;
   size_t h_pinned_n = 0;
+  // halo of a subdomain (solve_dd): owned dofs packed for the neighbours, ghost rows
+  // filled from them; the packing buffers belong to the caller's transport
+  bool halo_set = false;
+  int halo_nsend = 0, halo_nrecv = 0;
+  DBuf<int> halo_send_idx, halo_recv_idx;
+  double *halo_send_buf = nullptr, *halo_recv_buf = nullptr;
   // time-dependent state (tcd.cu): previous rhs, start vector preset, system assembled
   DBuf<double> tcd_fold;
   bool sol_preset = false, tcd_active = false;
@@ -282,10 +288,10 @@ int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, in
 // one damped Jacobi step; tmp: a level-sized work vector other than x and f
 template <typename T>
 int sell_jacobi(cudaStream_t s, const Level &L, const T *f, T *x, T *tmp, double omega, int num_sms, bool dirichlet);
-// y_a -= A_aD v_D over the active rows' Dirichlet columns (the part of A the
-// solve copy leaves out)
+// y_a -= A_aD v_D (add: y_a += A_aD v_D) over the active rows' Dirichlet
+// columns (the part of A the solve copy leaves out)
 template <typename T>
-int dirichlet_cols(cudaStream_t s, const Level &L, const T *v, T *y);
+int dirichlet_cols(cudaStream_t s, const Level &L, const T *v, T *y, bool add = false);
 
 // ------------------------------------------------------------- solver (solver.cu)
 int coarse_factor(Handle &h);

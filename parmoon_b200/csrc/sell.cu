@@ -361,7 +361,7 @@ __global__ void k_sell_copy_dirichlet(int Na, int N, const T *__restrict__ f, T 
 template <typename T>
 __global__ void k_dirichlet_cols(int n, const int *__restrict__ rows, const int *__restrict__ beg,
                                  const int *__restrict__ rp, const int *__restrict__ kc, const double *__restrict__ a,
-                                 const T *v, T *y) {
+                                 const T *v, T *y, double sign) {
   pdl_wait();
   pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -369,20 +369,20 @@ __global__ void k_dirichlet_cols(int n, const int *__restrict__ rows, const int 
   const int r = __ldg(rows + i);
   double s = 0;
   for (int k = __ldg(beg + i), e = __ldg(rp + r + 1); k < e; k++) s += __ldg(a + k) * (double)v[__ldg(kc + k)];
-  y[r] = (T)((double)y[r] - s);
+  y[r] = (T)((double)y[r] + sign * s);
 }
 
 template <typename T>
-int dirichlet_cols(cudaStream_t s, const Level &L, const T *v, T *y) {
+int dirichlet_cols(cudaStream_t s, const Level &L, const T *v, T *y, bool add) {
   if (L.n_dd == 0) return PMG_OK;
   PMG_CUDA(launch_pdl(k_dirichlet_cols<T>, dim3((L.n_dd + 255) / 256), dim3(256), 0, s, L.n_dd,
                       (const int *)L.dd_row.p, (const int *)L.dd_beg.p, (const int *)L.rowptr.p,
-                      (const int *)L.kcol.p, (const double *)L.A.p, v, y));
+                      (const int *)L.kcol.p, (const double *)L.A.p, v, y, add ? 1.0 : -1.0));
   count_launches(1);
   return PMG_OK;
 }
-template int dirichlet_cols<float>(cudaStream_t, const Level &, const float *, float *);
-template int dirichlet_cols<double>(cudaStream_t, const Level &, const double *, double *);
+template int dirichlet_cols<float>(cudaStream_t, const Level &, const float *, float *, bool);
+template int dirichlet_cols<double>(cudaStream_t, const Level &, const double *, double *, bool);
 
 // grid of a SELL launch: one CTA per slice up to a cap, beyond which CTAs loop
 // over slices (loading the next slice's first chunk before the reduction).

@@ -842,7 +842,7 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
         vc_timed = true;
       }
       PMG_TRY(sell_spmv<double>(s, F, zi, nullptr, w, 0, h.num_sms));
-      PMG_TRY(dirichlet_cols<double>(s, F, zi, w));  // w = A z_i with the Dirichlet columns
+      PMG_TRY(dirichlet_cols<double>(s, F, zi, w, true));  // w = A z_i with the Dirichlet columns (z_D = 0 here)
       double *Hc = Hd + (size_t)i * (m + 1);
       // modified Gram-Schmidt (FgmresIte.C): h_k = w.v_k, w -= h_k v_k for
       // k = 0..i, then h_{i+1}^2 = w.w; each update fused with the next product
@@ -933,7 +933,259 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
   return status;
 }
 
+// ------------------------------------------------------- domain decomposition
+// FGMRES over a domain-decomposed finest level (the parallel path of the
+// reference: TParFECommunicator3D::CommUpdate before each product and an
+// all-reduce of every inner product, src/Parallel/ParFECommunicator3D.C:218-346,
+// src/FE/MGLevel3D.C:220-272).  Each rank's handle holds its subdomain: the
+// rows it owns (active rows, and its Dirichlet rows) plus ghost rows -- the
+// dofs of a layer of neighbouring cells -- stored as Dirichlet rows of the
+// local problem.  Per iteration:
+//   * the preconditioner is the rank's own V-cycle with the ghost rows held at
+//     zero (overlapping additive Schwarz, one subdomain per rank, multigrid
+//     inside each);
+//   * the product w = A z takes the ghost values of z from the neighbours
+//     (halo exchange) and drops the ghost rows of w;
+//   * every inner product is summed over the ranks before it is used
+//     (modified Gram-Schmidt: one sum per step, as the reference's Ddot);
+//   * the residual takes the ghost values of x from the neighbours.
+// The transport is the caller's: pmg_comm's callbacks move the packed halo
+// buffers and sum host doubles (NCCL, MPI, gloo ...).
+__global__ void k_halo_gather(int n, const int *__restrict__ idx, const double *__restrict__ x, double *__restrict__ buf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) buf[i] = x[idx[i]];
+}
+__global__ void k_halo_scatter(int n, const int *__restrict__ idx, const double *__restrict__ buf, double *__restrict__ x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[idx[i]] = buf[i];
+}
+__global__ void k_zero_rows(int n, const int *__restrict__ idx, double *__restrict__ x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[idx[i]] = 0.0;
+}
+
+static int halo_exchange(Handle &h, const pmg_comm *comm, double *x) {
+  cudaStream_t s = h.stream;
+  if (h.halo_nsend > 0) {
+    k_halo_gather<<<(h.halo_nsend + 255) / 256, 256, 0, s>>>(h.halo_nsend, h.halo_send_idx.p, x, h.halo_send_buf);
+    count_launches(1);
+    PMG_CUDA(cudaGetLastError());
+  }
+  PMG_CUDA(cudaStreamSynchronize(s));
+  if (comm->exchange(comm->ctx, h.halo_send_buf, h.halo_nsend, h.halo_recv_buf, h.halo_nrecv) != 0) {
+    set_error("solve_dd: the halo exchange callback failed");
+    return PMG_ERR_STATE;
+  }
+  if (h.halo_nrecv > 0) {
+    k_halo_scatter<<<(h.halo_nrecv + 255) / 256, 256, 0, s>>>(h.halo_nrecv, h.halo_recv_idx.p, h.halo_recv_buf, x);
+    count_launches(1);
+    PMG_CUDA(cudaGetLastError());
+  }
+  return PMG_OK;
+}
+
+static int zero_ghosts(Handle &h, double *x) {
+  if (h.halo_nrecv > 0) {
+    k_zero_rows<<<(h.halo_nrecv + 255) / 256, 256, 0, h.stream>>>(h.halo_nrecv, h.halo_recv_idx.p, x);
+    count_launches(1);
+    PMG_CUDA(cudaGetLastError());
+  }
+  return PMG_OK;
+}
+
+// the device scalar *d summed over the ranks, in place (host round trip)
+static int sum_over_ranks(Handle &h, const pmg_comm *comm, double *d, int n) {
+  double *hv = h.h_H + 128;  // the pinned scratch (256 doubles; FGMRES uses at most 62)
+  PMG_CUDA(cudaMemcpyAsync(hv, d, sizeof(double) * n, cudaMemcpyDeviceToHost, h.stream));
+  PMG_CUDA(cudaStreamSynchronize(h.stream));
+  if (comm->allreduce_sum(comm->ctx, hv, n) != 0) {
+    set_error("solve_dd: the all-reduce callback failed");
+    return PMG_ERR_STATE;
+  }
+  PMG_CUDA(cudaMemcpyAsync(d, hv, sizeof(double) * n, cudaMemcpyHostToDevice, h.stream));
+  return PMG_OK;
+}
+
+int solve_dd(Handle &h, const pmg_comm *comm, double *sol_host, const double *rhs_host, pmg_solve_stats *st) {
+  if (h.lv.empty()) { set_error("solve_dd: no levels"); return PMG_ERR_STATE; }
+  if (!comm || !comm->allreduce_sum || !comm->exchange) { set_error("solve_dd: incomplete communicator"); return PMG_ERR_ARG; }
+  if (!h.halo_set) { set_error("solve_dd: pmg_set_halo first"); return PMG_ERR_STATE; }
+  if (h.prm.smoother == PMG_SMOOTHER_LEARNED) { set_error("solve_dd: the learned smoother is not built for subdomains"); return PMG_ERR_UNSUPPORTED; }
+  PMG_CUDA(cudaEventRecord(h.ev[2], h.stream));
+  PMG_TRY(prepare_levels(h));
+  PMG_TRY(capture_vcycle(h));
+  Level &F = h.lv.back();
+  const size_t N = F.N;
+  const int m = h.prm.restart;
+  if (h.krylov_n != (int)N || h.krylov_restart != m) {
+    PMG_TRY(h.V.alloc(N * (m + 1)));
+    PMG_TRY(h.Z.alloc(N * m));
+    PMG_TRY(h.w.alloc(N));
+    PMG_TRY(h.sol.alloc(N));
+    PMG_TRY(h.rhs.alloc(N));
+    PMG_TRY(h.H.alloc((size_t)(m + 1) * (m + 1) + 64));
+    h.krylov_n = (int)N;
+    h.krylov_restart = m;
+  }
+  cudaStream_t s = h.stream;
+  if (rhs_host) PMG_CUDA(cudaMemcpyAsync(h.rhs.p, rhs_host, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  else PMG_CUDA(cudaMemcpyAsync(h.rhs.p, F.rhs.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+  if (sol_host) PMG_CUDA(cudaMemcpyAsync(h.sol.p, sol_host, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  else PMG_TRY(zero<double>(s, h.sol.p, N));
+  PMG_TRY(copy_dirichlet(s, F.Na, F.N, h.rhs.p, h.sol.p));
+  double *V = h.V.p, *Z = h.Z.p, *w = h.w.p;
+  double *Hd = h.H.p, *sc = Hd + (size_t)(m + 1) * (m + 1);
+  std::vector<double> H((size_t)(m + 1) * m, 0.0), sv(m + 1), cs(m), sn(m), y(m);
+  double *hcol = h.h_H;
+
+  auto residual = [&](double *out_vec, double &nrm) -> int {
+    PMG_TRY(halo_exchange(h, comm, h.sol.p));
+    PMG_TRY(sell_spmv<double>(s, F, h.sol.p, h.rhs.p, out_vec, 1, h.num_sms));
+    PMG_TRY(dirichlet_cols<double>(s, F, h.sol.p, out_vec));
+    PMG_TRY(zero_ghosts(h, out_vec));
+    PMG_TRY(dot(h, out_vec, out_vec, N, sc));
+    PMG_TRY(sum_over_ranks(h, comm, sc, 1));
+    PMG_CUDA(cudaMemcpyAsync(hcol, sc, sizeof(double), cudaMemcpyDeviceToHost, s));
+    PMG_CUDA(cudaStreamSynchronize(s));
+    nrm = sqrt(hcol[0]);
+    return PMG_OK;
+  };
+
+  double beta;
+  PMG_TRY(residual(V, beta));
+  const double res0 = beta;
+  double r0 = beta, res = beta;
+  int j = 1, status = PMG_ERR_NOT_CONVERGED, iters = 0;
+  const double red = h.prm.lin_red, rmin = h.prm.lin_res_min;
+  const int maxit = h.prm.lin_maxit;
+  if (!std::isfinite(beta)) { set_error("solve_dd: non-finite initial residual"); return PMG_ERR_NONFINITE; }
+  if (beta <= rmin || beta < 1e-300) status = PMG_OK;
+  while (status == PMG_ERR_NOT_CONVERGED && j <= maxit) {
+    PMG_TRY(scale_by_inv_sqrt(s, N, sc, V, V));
+    std::fill(sv.begin(), sv.end(), 0.0);
+    sv[0] = beta;
+    int i;
+    bool done = false;
+    for (i = 0; i < m && j <= maxit; i++, j++) {
+      double *vi = V + (size_t)i * N, *zi = Z + (size_t)i * N;
+      PMG_TRY(precondition(h, vi, zi, false));
+      PMG_TRY(halo_exchange(h, comm, zi));
+      PMG_TRY(sell_spmv<double>(s, F, zi, nullptr, w, 0, h.num_sms));
+      PMG_TRY(dirichlet_cols<double>(s, F, zi, w, true));  // + A_aG z_G: the neighbours' values of z
+      PMG_TRY(zero_ghosts(h, w));
+      double *Hc = Hd + (size_t)i * (m + 1);
+      PMG_TRY(dot(h, w, V, N, Hc));
+      PMG_TRY(sum_over_ranks(h, comm, Hc, 1));
+      for (int k = 0; k <= i; k++) {
+        PMG_TRY(mgs_step(h, N, Hc + k, V + (size_t)k * N, k < i ? V + (size_t)(k + 1) * N : w, w, Hc + k + 1));
+        PMG_TRY(sum_over_ranks(h, comm, Hc + k + 1, 1));
+      }
+      PMG_TRY(scale_by_inv_sqrt(s, N, Hc + i + 1, w, V + (size_t)(i + 1) * N));
+      PMG_CUDA(cudaMemcpyAsync(hcol, Hc, sizeof(double) * (i + 2), cudaMemcpyDeviceToHost, s));
+      PMG_CUDA(cudaStreamSynchronize(s));
+      for (int k = 0; k <= i; k++) H[(size_t)k * m + i] = hcol[k];
+      H[(size_t)(i + 1) * m + i] = sqrt(hcol[i + 1]);
+      for (int k = 0; k < i; k++) {
+        double t = cs[k] * H[(size_t)k * m + i] + sn[k] * H[(size_t)(k + 1) * m + i];
+        H[(size_t)(k + 1) * m + i] = -sn[k] * H[(size_t)k * m + i] + cs[k] * H[(size_t)(k + 1) * m + i];
+        H[(size_t)k * m + i] = t;
+      }
+      givens(H[(size_t)i * m + i], H[(size_t)(i + 1) * m + i], cs[i], sn[i]);
+      {
+        double t = cs[i] * H[(size_t)i * m + i] + sn[i] * H[(size_t)(i + 1) * m + i];
+        H[(size_t)(i + 1) * m + i] = 0.0;
+        H[(size_t)i * m + i] = t;
+        t = cs[i] * sv[i] + sn[i] * sv[i + 1];
+        sv[i + 1] = -sn[i] * sv[i] + cs[i] * sv[i + 1];
+        sv[i] = t;
+      }
+      res = fabs(sv[i + 1]);
+      iters = j;
+      if (!std::isfinite(res)) { status = PMG_ERR_NONFINITE; set_error("solve_dd: non-finite residual estimate"); done = true; i++; break; }
+      const double ref = h.prm.reference_restart_rule ? r0 : res0;
+      if (res < rmin || res < red * ref) { status = PMG_OK; done = true; i++; break; }
+      if (res > h.prm.div_factor * res0) { status = PMG_ERR_DIVERGED; set_error("solve_dd: diverged"); done = true; i++; break; }
+    }
+    int mm = i;
+    for (int k = mm - 1; k >= 0; k--) {
+      double t = sv[k];
+      for (int l = k + 1; l < mm; l++) t -= H[(size_t)k * m + l] * y[l];
+      y[k] = t / H[(size_t)k * m + k];
+    }
+    if (mm > 0) {
+      for (int k = 0; k < mm; k++) hcol[k] = y[k];
+      PMG_CUDA(cudaMemcpyAsync(sc + 1, hcol, sizeof(double) * mm, cudaMemcpyHostToDevice, s));
+      size_t nb = (N + 255) / 256;
+      k_lincomb<<<(unsigned)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(N, mm, sc + 1, Z, N, h.sol.p); count_launches(1);
+      PMG_CUDA(cudaGetLastError());
+      PMG_CUDA(cudaStreamSynchronize(s));
+    }
+    if (done || j > maxit) break;
+    PMG_TRY(residual(V, beta));
+    r0 = beta;
+  }
+  double res_final;
+  PMG_TRY(residual(w, res_final));  // also refreshes the ghost values of x
+  PMG_CUDA(cudaEventRecord(h.ev[3], s));
+  PMG_CUDA(cudaEventSynchronize(h.ev[3]));
+  float ms = 0;
+  PMG_CUDA(cudaEventElapsedTime(&ms, h.ev[2], h.ev[3]));
+  h.t_solve = ms * 1e-3;
+  if (sol_host) PMG_CUDA(cudaMemcpyAsync(sol_host, h.sol.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+  PMG_CUDA(cudaStreamSynchronize(s));
+  PMG_TRY(coarse_cycle_check(h));
+  if (st) {
+    st->iterations = iters;
+    st->res0 = res0;
+    st->res_final = res_final;
+    st->rel_res = res0 > 0 ? res_final / res0 : 0.0;
+    st->mean_contraction = (iters > 0 && res0 > 0 && res_final > 0) ? pow(res_final / res0, 1.0 / iters) : 0.0;
+    st->smoother_used = h.prm.smoother;
+    st->seconds = h.t_solve;
+    st->setup_seconds = 0.0;
+    st->vcycle_seconds = 0.0;
+  }
+  if (status == PMG_ERR_NOT_CONVERGED)
+    set_error("solve_dd: the iteration limit (lin_maxit) was reached before |r| <= max(lin_res_min, lin_red |r0|)");
+  return status;
+}
+
 }  // namespace pmg
+
+extern "C" int pmg_set_halo(pmg_handle hh, int n_send, const int *send_idx, int n_recv, const int *recv_idx,
+                            double *send_buf_dev, double *recv_buf_dev) {
+  pmg::Handle *h = reinterpret_cast<pmg::Handle *>(hh);
+  if (!h || h->lv.empty() || n_send < 0 || n_recv < 0 || (n_send && (!send_idx || !send_buf_dev)) ||
+      (n_recv && (!recv_idx || !recv_buf_dev))) {
+    pmg::set_error("pmg_set_halo: bad arguments");
+    return PMG_ERR_ARG;
+  }
+  pmg::Level &F = h->lv.back();
+  if (!F.has_csr) { pmg::set_error("pmg_set_halo: set the finest level's pattern first"); return PMG_ERR_STATE; }
+  for (int k = 0; k < n_send; k++)
+    if (send_idx[k] < 0 || send_idx[k] >= F.N) { pmg::set_error("pmg_set_halo: send index out of range"); return PMG_ERR_ARG; }
+  for (int k = 0; k < n_recv; k++)
+    if (recv_idx[k] < F.Na || recv_idx[k] >= F.N) {
+      pmg::set_error("pmg_set_halo: ghost rows must be rows of the local problem past active_bound");
+      return PMG_ERR_ARG;
+    }
+  PMG_TRY(h->halo_send_idx.upload(send_idx, n_send, h->stream));
+  PMG_TRY(h->halo_recv_idx.upload(recv_idx, n_recv, h->stream));
+  PMG_CUDA(cudaStreamSynchronize(h->stream));
+  h->halo_nsend = n_send;
+  h->halo_nrecv = n_recv;
+  h->halo_send_buf = send_buf_dev;
+  h->halo_recv_buf = recv_buf_dev;
+  h->halo_set = true;
+  return PMG_OK;
+}
+
+extern "C" int pmg_solve_dd(pmg_handle hh, const pmg_comm *comm, double *sol, const double *rhs,
+                            pmg_solve_stats *stats) {
+  pmg::Handle *h = reinterpret_cast<pmg::Handle *>(hh);
+  if (!h) return PMG_ERR_ARG;
+  return pmg::solve_dd(*h, comm, sol, rhs, stats);
+}
 
 extern "C" int pmg_vcycle(pmg_handle hh, const double *v_dev, double *z_dev) {
   pmg::Handle *h = reinterpret_cast<pmg::Handle *>(hh);

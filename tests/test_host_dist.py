@@ -1,11 +1,12 @@
 """Host logic of the multi-process paths on CPU (gloo, world size 2): the
 gradient average of data-parallel training of the learned smoother, the
-identical updates it leads to on every rank, and the max-over-ranks timing of
-bench.py.  No GPU."""
+identical updates it leads to on every rank, the max-over-ranks timing of
+bench.py, and the subdomains of the domain-decomposed solve.  No GPU."""
 import os
 import socket
 
 import numpy as np
+import pytest
 import torch.multiprocessing as mp
 
 import dist_workers as W
@@ -44,3 +45,23 @@ def test_data_parallel_training_and_rank_max(tmp_path):
     assert losses[-1] < losses[0]
     assert np.allclose(r[0]["mean"], 1.5) and np.allclose(r[1]["mean"], 1.5)
     assert float(r[0]["mx"]) == 1.5 and float(r[1]["mx"]) == 1.5
+
+
+@pytest.mark.parametrize("elem,n,nl", [(2, 8, 3), (1, 16, 3), (12, 8, 2)])
+def test_subdomains_partition_and_halo(tmp_path, elem, n, nl):
+    """Domain decomposition host logic (parmoon_b200.dd, gloo, 2 ranks): the
+    owned dofs of the ranks partition the global dofs, the halo exchange fills
+    every ghost row with its owner's value, and the pattern of every owned
+    active row built from the subdomain's cells equals the global row
+    (TSquareStructure3D on the subdomain holds all couplings of its owned
+    rows, so its assembly of those rows is complete)."""
+    world = 2
+    mp.start_processes(W.dd_partition, args=(world, free_port(), str(tmp_path), elem, n, nl), nprocs=world,
+                       join=True, start_method="spawn")
+    r = [np.load(os.path.join(tmp_path, f"dd{k}.npz")) for k in range(world)]
+    owned = np.concatenate([x["glob"][:int(x["n_owned"])] for x in r])
+    N = r[0]["ref"].size
+    assert np.array_equal(np.sort(owned), np.arange(N))
+    for x in r:
+        assert np.array_equal(x["x"], x["ref"][x["glob"]])  # ghosts filled from their owners
+        assert int(x["bad_rows"]) == 0
