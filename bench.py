@@ -497,6 +497,52 @@ def bench_ours(args, rank, world, dist):
     h.close()
 
 
+def bench_dd(args, rank, world, dist):
+    """--dd: the domain-decomposed solve (pmg_solve_dd) of the same problem over
+    the ranks (z-slabs, one GPU per rank, NCCL halo exchange and sums): one step
+    = assembly of every level of the rank's subdomain + the solve to 1e-10;
+    value = the slowest rank's mean step time (strong scaling: the problem is
+    the same at every rank count).  The slab count must divide the coarsest
+    level's cells per direction."""
+    import torch
+    import parmoon_b200 as P
+    from parmoon_b200 import dd
+    glob, loc = dd.local_hierarchy(P.Q2_HEX, N_CELLS, N_LEVELS, world, rank)
+    h = P.Handle(N_LEVELS, P.default_params(precision=P.PREC_FP32, restart=RESTART))
+    h.set_coefficients(P.coeff(kind=P.COEF_CONST, eps=EPS, b=B, f=F))
+    dd.load_subdomain(h, loc, dirichlet=dirichlet)
+    comm = dd.TorchComm(dist, loc[-1])
+    c = comm.struct(P.lib())
+    h.set_halo(comm.send_idx, comm.recv_idx, comm.send_buf.data_ptr(), comm.recv_buf.data_ptr())
+
+    def step():
+        h.assemble(-1, P.FORM_SUPG, copy_out=False)
+        t_asm = h.timings()[0]
+        _, st, rc = h.solve_dd(c)
+        return t_asm + st.seconds, st
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    dist.barrier()
+    times = []
+    for _ in range(args.steps):
+        t, st = step()
+        times.append(t)
+    torch.cuda.synchronize()
+    dist.barrier()
+    value = max_over_ranks(statistics.mean(times), dist)
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+                          "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+                          "scaling": "strong", "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+                          "mode": "domain-decomposed (pmg_solve_dd)",
+                          "config": {"workload": f"CD3D SUPG Q2 hexahedra {N_CELLS}^3 ({N_LEVELS} levels), "
+                                                 f"{world} z-slab subdomains", "parallelism": f"dd{world}"},
+                          "iterations": st.iterations, "rel_res_fp64": st.rel_res}))
+    h.close()
+
+
 def config_line(name, extra):
     line = {"metric": METRIC, "impl": "ours", "config_name": name, "n_gpus": 1, "dtype": "f64+f32",
             "data": "synthetic", "higher_is_better": False, "unit": "s"}
@@ -629,6 +675,8 @@ def main():
     ap.add_argument("--levels", type=int, default=5)
     ap.add_argument("--profile-kernel", choices=sorted(KERNELS), default=None,
                     help="time one kernel on the finest level only (the profiling command)")
+    ap.add_argument("--dd", action="store_true",
+                    help="domain-decomposed solve over the ranks (launch with torchrun, one GPU per rank)")
     ap.add_argument("--config", choices=["poisson_q1_32", "p2tet_lognormal_64", "tcd_q1_128_cn"], default=None,
                     help="run one of the other workloads instead of the bench line")
     args = ap.parse_args()
@@ -647,6 +695,16 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None
+    if args.dd:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        bench_dd(args, rank, world, tdist)
+        tdist.barrier()
+        tdist.destroy_process_group()
+        return
     if args.impl == "ours" and world > 1:
         import datetime
         import torch
