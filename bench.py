@@ -439,6 +439,29 @@ def bench_ours(args, rank, world, dist):
            "fp64_everywhere_rel_res": st_t.rel_res, "fp64_everywhere_status": rc_t,
            "note": "relative L2 errors of the 1e-10 solutions against the FP64-everywhere solve to 1e-14"}
 
+    # the learned-smoother FP32 V-cycle in FP64 FGMRES on the same problem: the
+    # stencil network on every level's Q2 node lattice ((2n+1)^3 nodes), the
+    # committed weights, the SSOR guard on; the timed solve includes the
+    # network's forward on every level (it runs once per assembly)
+    learned = None
+    if os.path.exists(WEIGHTS):
+        w = np.fromfile(WEIGHTS, dtype=np.float32)
+        for l, L in enumerate(levels):
+            h.set_lattice(l, 2 * L["n"] + 1, L["dof_lat"])
+        h.set_learned_weights(w)
+        h.set_params(P.default_params(precision=P.PREC_FP32, restart=RESTART, smoother=P.SMOOTHER_LEARNED))
+        h.solve()  # warm-up: graph capture
+        h.set_learned_weights(w)
+        _, stl, rcl = h.solve()
+        xl = h.get_solution()
+        learned = {"solve_s": stl.seconds, "network_and_setup_s": stl.setup_seconds, "iterations": stl.iterations,
+                   "rel_res": stl.rel_res, "status": rcl,
+                   "smoother_used": "learned" if stl.smoother_used == P.SMOOTHER_LEARNED else "ssor",
+                   "rho_plain": stl.rho_plain, "rho_learned": stl.rho_learned, "learned_cycles": stl.learned_cycles,
+                   "speedup_vs_fp64_gmg": fp64_s / stl.seconds,
+                   "err_vs_fp64_everywhere": float(np.linalg.norm(xl - xt)) / nt,
+                   "weights": os.path.relpath(WEIGHTS, os.path.dirname(os.path.abspath(__file__)))}
+
     line = None
     if rank == 0:
         cpu = None
@@ -467,6 +490,7 @@ def bench_ours(args, rank, world, dist):
             "fp64_gmg": {"solve_s": fp64_s, "iterations": fp64[0][1], "rel_res": fp64[0][2], "status": fp64[0][3],
                          "vcycle_s": fp64[0][4]},
             "err_vs_fp64": err,
+            "learned_fp32": learned,
             "setup_csr_s": {"host_builder": t_host_csr, "device_builder": c_dev.value,
                             "device_entry_total": t_dev_csr, "device_entry_install": c_inst.value,
                             "note": "finest-level CSR pattern (TSquareStructure3D + Sort), wall time; "
@@ -483,9 +507,9 @@ def bench_ours(args, rank, world, dist):
                          "launch_s": ssor["seconds"]},
             "roofline_spmv64": {"achieved": spmv64["gbs"], "frac": spmv64["gbs"] / hbm, "bytes": spmv64["bytes"]},
             "roofline_spmv32": {"achieved": spmv32["gbs"], "frac": spmv32["gbs"] / hbm, "bytes": spmv32["bytes"]},
-            "roofline_assembly": {"kernel": "k_assemble_tc<Q2,27,CONST> (reference-table contraction on the FP64 "
-                                            "tensor cores, mma.sync m8n8k4 f64; finest level, all 8 element colours, "
-                                            "matrix and rhs zeroed first)",
+            "roofline_assembly": {"kernel": "k_tc_setup<Q2,27> + k_assemble_tc16<Q2> (reference-table contraction "
+                                            "on the FP64 tensor cores, mma.sync m8n8k4 f64; finest level, all 8 "
+                                            "element colours, matrix and rhs zeroed first)",
                                   "achieved_gbs": asm["gbs"], "frac_hbm": asm["gbs"] / hbm,
                                   "achieved_tflops_fp64": asm["tflops"], "bytes": asm["bytes"], "launch_s": asm["seconds"]},
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": 2 * N * 8, "d2h_bytes_per_step": 2 * N * 8},
@@ -564,9 +588,10 @@ def run_config(name, steps):
         form, dirv, nl = P.FORM_GALERKIN, None, 4
     elif name == "p2tet_lognormal_64":
         # P2 tetrahedra: 64^3 hexahedra x 6 Kuhn tetrahedra (1,572,864 cells, 2,146,689 dofs), interior
-        # vertices jittered by up to 0.2 h, lognormal diffusion (sigma 1, correlation 0.1), b = 0, f = 1, Keast-11
+        # vertices jittered by up to 0.2 h, lognormal diffusion (sigma 1, correlation 0.1), b = 0, f = 1,
+        # the 5-point degree-3 tetrahedral rule the workload names
         levels = P.struct_hierarchy(P.P2_TET, 64, 5, jitter=0.2, seed=1)
-        mk = lambda prec: P.default_params(precision=prec)
+        mk = lambda prec: P.default_params(precision=prec, quad_rule=P.QUAD_KEAST5)
         coef = P.coeff(kind=P.COEF_LOGNORMAL, eps=1.0, f=1.0, modes=lognormal_modes(1))
         form, dirv, nl = P.FORM_GALERKIN, None, 5
     else:
@@ -637,7 +662,8 @@ def run_tcd(steps):
     h.close()
 
 
-KERNELS = {"spmv64": 0, "spmv32": 1, "ssor64": 2, "ssor32": 3, "assemble": 4, "coarse_factor": 6}
+KERNELS = {"spmv64": 0, "spmv32": 1, "ssor64": 2, "ssor32": 3, "assemble": 4, "coarse_factor": 6, "learned_fwd": 7}
+WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "parmoon_b200", "weights", "stencil_net_q1.f32")
 
 
 def profile_kernel(name):
@@ -653,6 +679,10 @@ def profile_kernel(name):
     fine = 0 if name == "coarse_factor" else N_LEVELS - 1
     if name != "assemble":
         h.assemble(fine, P.FORM_SUPG, copy_out=False)
+    if name == "learned_fwd":
+        # the Q2 dofs of the finest level form a (2n+1)^3 node lattice
+        h.set_lattice(fine, 2 * N_CELLS + 1, levels[fine]["dof_lat"])
+        h.set_learned_weights(np.fromfile(WEIGHTS, dtype=np.float32))
     sec, by, fl = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
     P._check(lib.pmg_time_kernel(h.h, KERNELS[name], fine, P.FORM_SUPG, 3, ctypes.byref(sec), ctypes.byref(by),
                                  ctypes.byref(fl)))
@@ -660,7 +690,7 @@ def profile_kernel(name):
     print(json.dumps({"kernel": name, "n_cells": N_CELLS, "levels": N_LEVELS, "level": fine, "n_dofs": levels[fine]["N"],
                       "nnz": int(levels[fine]["rowptr"][-1]), "seconds": sec.value, "bytes": by.value,
                       "flops": fl.value, "gbs": by.value / sec.value / 1e9, "hbm_frac": by.value / sec.value / 1e9 / hbm,
-                      "peak_kind": kind}))
+                      "tflops": fl.value / sec.value / 1e12, "peak_kind": kind}))
     h.close()
 
 
@@ -675,6 +705,8 @@ def main():
     ap.add_argument("--levels", type=int, default=5)
     ap.add_argument("--profile-kernel", choices=sorted(KERNELS), default=None,
                     help="time one kernel on the finest level only (the profiling command)")
+    ap.add_argument("--peaks", action="store_true",
+                    help="print the FP64 FMA, FP64 DMMA and BF16 mma.sync throughput of this GPU")
     ap.add_argument("--dd", action="store_true",
                     help="domain-decomposed solve over the ranks (launch with torchrun, one GPU per rank)")
     ap.add_argument("--config", choices=["poisson_q1_32", "p2tet_lognormal_64", "tcd_q1_128_cn"], default=None,
@@ -685,6 +717,11 @@ def main():
     N_FULL = (2 * N_CELLS + 1) ** 3
     if args.profile_kernel:
         profile_kernel(args.profile_kernel)
+        return
+    if args.peaks:
+        import parmoon_b200 as P
+        fma, dmma, hmma = P.measure_peaks()
+        print(json.dumps({"fp64_fma_tflops": fma, "fp64_dmma_tflops": dmma, "bf16_mma_sync_tflops": hmma}))
         return
     if args.config == "tcd_q1_128_cn":
         run_tcd(args.steps)

@@ -86,6 +86,17 @@ typedef struct pmg_coeff_desc {
 #define PMG_PREC_FP64         0  /* V-cycle stores level matrices and vectors in FP64 */
 #define PMG_PREC_FP32         1  /* V-cycle in FP32, outer FGMRES / true residual in FP64 */
 
+/* quadrature rules selectable through pmg_params.quad_rule (Gauss: hexahedra,
+ * Keast: tetrahedra; src/QuadFormulas/QuadFormulaHexa.C, QuadFormulaTetra.C;
+ * the 5-point degree-3 tetrahedral rule has no reference counterpart) */
+#define PMG_QUAD_AUTO     0
+#define PMG_QUAD_GAUSS2   2
+#define PMG_QUAD_GAUSS3   3
+#define PMG_QUAD_GAUSS4   4
+#define PMG_QUAD_KEAST4   104
+#define PMG_QUAD_KEAST5   105
+#define PMG_QUAD_KEAST11  111
+
 typedef struct pmg_params {
     int    smoother;           /* SC_SMOOTHER_SCALAR */
     int    pre_smooth;         /* SC_PRE_SMOOTH_SCALAR */
@@ -117,6 +128,14 @@ typedef struct pmg_params {
     int    slc_fine;           /* SC_STEP_LENGTH_CONTROL_FINE_SCALAR: step-length control on the finest level
                                   (TMultiGrid3D::Cycle, src/FE/MultiGrid3D.C:517-523, 655-663;
                                   TMGLevel3D::StepLengthControl, src/FE/MGLevel3D.C:908-961) */
+    int    quad_rule;          /* 0 (default): the reference's rule for the element (problem_linear above);
+                                  else one of PMG_QUAD_* for the element's shape (PMG_ERR_UNSUPPORTED at
+                                  assembly otherwise) */
+    int    learned_guard_off;  /* 0 (default): with PMG_SMOOTHER_LEARNED the solve measures the plain SSOR
+                                  V-cycle's contraction over the first 2 cycles, then runs the learned
+                                  smoother and hands back to SSOR as soon as its measured per-cycle
+                                  contraction exceeds the plain one; 1: the learned smoother runs in every
+                                  cycle (for measuring it alone) */
 } pmg_params;
 
 typedef struct pmg_solve_stats {
@@ -129,6 +148,11 @@ typedef struct pmg_solve_stats {
     double seconds;            /* device time of the solve (CUDA events) */
     double setup_seconds;      /* of which per-solve set-up: SELL values, coarsest factorisation, graph capture */
     double vcycle_seconds;     /* device time of the first preconditioner application (one V-cycle) */
+    double rho_plain;          /* learned smoother: the plain SSOR cycles' measured contraction per cycle (0 if
+                                  not measured) */
+    double rho_learned;        /* learned smoother: its measured contraction per cycle over the cycles it ran
+                                  (0 if it ran fewer than 2) */
+    int    learned_cycles;     /* V-cycles that used the learned smoother */
 } pmg_solve_stats;
 
 typedef struct pmg_handle_s *pmg_handle;
@@ -396,12 +420,22 @@ int pmg_last_timings(pmg_handle h, double *assemble_s, double *solve_s, double *
 #define PMG_KERNEL_ASSEMBLE  4
 #define PMG_KERNEL_CSR_SPMV64 5
 #define PMG_KERNEL_COARSE_FACTOR 6  /* LU + inverse of the coarsest level (level must be 0) */
+#define PMG_KERNEL_LEARNED_FWD 7    /* the stencil network's forward on the level's lattice (features, three
+                                       tensor-core convolutions, stencil); flops = 2 x 27 x (27*32 + 32*32 +
+                                       32*27) per lattice node; needs weights and a lattice */
 int pmg_time_kernel(pmg_handle h, int kernel, int level, int form, int reps,
                     double *seconds_per_launch, double *bytes_per_launch, double *flops_per_launch);
 
 /* Number of kernel launches this library has issued in the process (graph
  * replays count every kernel node of the graph). */
 int pmg_launch_count(unsigned long long *n);
+
+/* Throughput of the arithmetic paths the kernels use, measured on the current
+ * device by register-only probe kernels (8 blocks of 256 threads per SM, one
+ * timed launch after a warm-up): FP64 FMA on the CUDA cores, FP64
+ * mma.sync.m8n8k4 (DMMA) and BF16 mma.sync.m16n8k16 with FP32 accumulation,
+ * in TFLOP/s.  Diagnostic only; no handle needed. */
+int pmg_measure_peaks(double *fp64_fma_tflops, double *fp64_dmma_tflops, double *bf16_mma_sync_tflops);
 
 #ifdef __cplusplus
 }

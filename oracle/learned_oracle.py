@@ -6,7 +6,8 @@ checker of the device kernels in parmoon_b200/csrc/learned.cu:
 
   features  F[k][L] = a(i, nb_k(i)) / a(i, i) for active rows i at node L
   network   three 3x3x3 convolutions with zero padding, 27 -> 32 (ReLU) -> 32
-            (ReLU) -> 27; parameters flat [W1 b1 W2 b2 W3 b3], W[c_out][c_in][27]
+            (ReLU) -> 27; parameters flat [W1 b1 W2 b2 W3 b3], W[c_out][c_in][27];
+            the device rounds weights and every layer's input to BF16
   stencil   W_k(L) = out3[k][L] / a(i, i)  (0 on Dirichlet nodes)
   loss      |A (e - S r)|^2 / |r|^2 for one pair (e, r = A e), S r = sum_k W_k r(nb_k)
 """
@@ -85,12 +86,18 @@ def features(n1, rowptr, kcol, A, Na, dof_lat):
     return F, dscale
 
 
-def forward(theta, F, dscale):
+def forward(theta, F, dscale, act_bf16=True):
+    """The network on the feature lattice.  act_bf16: every layer's input is
+    rounded to BF16 as the device stores it (the features, and the ReLU
+    outputs of the hidden layers); False gives the unrounded function whose
+    gradient the finite-difference test pins."""
+    rnd = bf16_round if act_bf16 else (lambda x: x)
     W1, b1, W2, b2, W3, b3 = unpack(theta)
+    F = rnd(F)
     z1 = conv(F, W1, b1)
-    a1 = np.maximum(z1, 0)
+    a1 = rnd(np.maximum(z1, 0))
     z2 = conv(a1, W2, b2)
-    a2 = np.maximum(z2, 0)
+    a2 = rnd(np.maximum(z2, 0))
     out3 = conv(a2, W3, b3)
     Wst = out3 * dscale[None]
     return Wst, (F, z1, a1, z2, a2, out3)
@@ -109,11 +116,14 @@ def apply_stencil(Wst, rl):
     return c
 
 
-def loss_and_grad(theta, n1, rowptr, kcol, A, Na, dof_lat, e, r):
-    """Returns (loss, dloss/dtheta) for one pair (e, r)."""
+def loss_and_grad(theta, n1, rowptr, kcol, A, Na, dof_lat, e, r, act_bf16=True):
+    """Returns (loss, dloss/dtheta) for one pair (e, r).  With act_bf16 the
+    forward rounds the layer inputs to BF16 and the gradient passes the
+    rounding as the identity (the weight gradients use the rounded inputs),
+    as the device's backward does."""
     N = rowptr.size - 1
     F, dscale = features(n1, rowptr, kcol, A, Na, dof_lat)
-    Wst, (F_, z1, a1, z2, a2, out3) = forward(theta, F, dscale)
+    Wst, (F, z1, a1, z2, a2, out3) = forward(theta, F, dscale, act_bf16)
     rl = to_lattice(r, dof_lat, n1)
     cl = apply_stencil(Wst, rl).reshape(-1)
     c = cl[dof_lat]
@@ -143,9 +153,9 @@ def loss_and_grad(theta, n1, rowptr, kcol, A, Na, dof_lat, e, r):
     return loss, g
 
 
-def stencil(theta, n1, rowptr, kcol, A, Na, dof_lat):
+def stencil(theta, n1, rowptr, kcol, A, Na, dof_lat, act_bf16=True):
     F, dscale = features(n1, rowptr, kcol, A, Na, dof_lat)
-    Wst, _ = forward(theta, F, dscale)
+    Wst, _ = forward(theta, F, dscale, act_bf16)
     return Wst  # [27, k, j, i] == channel-major lattice order
 
 

@@ -28,6 +28,7 @@ COEF_CONST, COEF_SINE_RHS, COEF_LOGNORMAL, COEF_CURL_FOURIER, COEF_ROTATING, COE
 SMOOTHER_JACOBI, SMOOTHER_SOR, SMOOTHER_SSOR, SMOOTHER_LEARNED = 1, 2, 3, 30
 COARSE_JACOBI, COARSE_SOR, COARSE_SSOR, COARSE_DIRECT = 1, 2, 3, 17
 PREC_FP64, PREC_FP32 = 0, 1
+QUAD_AUTO, QUAD_GAUSS2, QUAD_GAUSS3, QUAD_GAUSS4, QUAD_KEAST4, QUAD_KEAST5, QUAD_KEAST11 = 0, 2, 3, 4, 104, 105, 111
 
 _i, _d, _p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
@@ -38,7 +39,8 @@ class Params(ctypes.Structure):
                 ("lin_red", _d), ("lin_res_min", _d), ("lin_maxit", _i), ("restart", _i), ("div_factor", _d),
                 ("precision", _i), ("sdfem_type", _i), ("poly_degree", _i), ("delta0", _d),
                 ("reference_restart_rule", _i), ("problem_linear", _i), ("learned_steps", _i),
-                ("assembly_kernel", _i), ("slc_all", _i), ("slc_fine", _i)]
+                ("assembly_kernel", _i), ("slc_all", _i), ("slc_fine", _i), ("quad_rule", _i),
+                ("learned_guard_off", _i)]
 
 
 class CoeffDesc(ctypes.Structure):
@@ -48,7 +50,8 @@ class CoeffDesc(ctypes.Structure):
 
 class SolveStats(ctypes.Structure):
     _fields_ = [("iterations", _i), ("res0", _d), ("res_final", _d), ("rel_res", _d), ("mean_contraction", _d),
-                ("smoother_used", _i), ("seconds", _d), ("setup_seconds", _d), ("vcycle_seconds", _d)]
+                ("smoother_used", _i), ("seconds", _d), ("setup_seconds", _d), ("vcycle_seconds", _d),
+                ("rho_plain", _d), ("rho_learned", _d), ("learned_cycles", _i)]
 
 
 class PmgError(RuntimeError):
@@ -375,6 +378,13 @@ class Handle:
         a, s, k = _d(), _d(), _d()
         _check(lib().pmg_last_timings(self.h, ctypes.byref(a), ctypes.byref(s), ctypes.byref(k)))
         return a.value, s.value, k.value
+
+
+def measure_peaks():
+    """(FP64 FMA, FP64 DMMA, BF16 mma.sync) throughput in TFLOP/s on the current device."""
+    v = [ctypes.c_double() for _ in range(3)]
+    _check(lib().pmg_measure_peaks(*[ctypes.byref(x) for x in v]))
+    return tuple(x.value for x in v)
 
 
 def learned_num_params():

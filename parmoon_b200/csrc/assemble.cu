@@ -43,13 +43,23 @@ __device__ __forceinline__ void coeff_eval(const CoefDev &C, double x, double y,
       break;
     case PMG_COEF_LOGNORMAL: {
       // cos(2 pi k.x + phi) as cospi(2 k.x + phi / pi): the reduction of an
-      // argument in units of pi is exact, so no general range reduction
-      double g = 0;
-      for (int m = 0; m < C.n_modes; m++) {
+      // argument in units of pi is exact, so no general range reduction.
+      // Four partial sums keep four independent cospi chains in flight (the
+      // FP64 pipe is latency-bound with one); g = (g0 + g1) + (g2 + g3).
+      double g0 = 0, g1 = 0, g2 = 0, g3 = 0;
+      auto term = [&](int m) {
         const double *M = C.modes + 8 * m;
-        g += M[3] * cospi(2.0 * (M[0] * x + M[1] * y + M[2] * z) + M[4] * (1.0 / PI));
+        return M[3] * cospi(2.0 * (M[0] * x + M[1] * y + M[2] * z) + M[4] * (1.0 / PI));
+      };
+      int m = 0;
+      for (; m + 4 <= C.n_modes; m += 4) {
+        g0 += term(m);
+        g1 += term(m + 1);
+        g2 += term(m + 2);
+        g3 += term(m + 3);
       }
-      c[0] = C.eps * exp(g);
+      for (; m < C.n_modes; m++) g0 += term(m);
+      c[0] = C.eps * exp((g0 + g1) + (g2 + g3));
       break;
     }
     case PMG_COEF_CURL_FOURIER: {
@@ -911,7 +921,11 @@ static TableCache g_tab[4];
 
 // quadrature rule of the reference (TFEDatabase3D::GetOrig, FEDatabase3D.C:1203-1309):
 // degree N_terms * polynomial degree with N_terms = 2 (INTERNAL_PROBLEM_LINEAR) or 3
-static int rule_for(int elem, int problem_linear) {
+static int rule_for(int elem, int problem_linear, int quad_rule = PMG_QUAD_AUTO) {
+  if (quad_rule != PMG_QUAD_AUTO) {
+    const bool hex_rule = quad_rule < 100;
+    return hex_rule == elem_is_hex(elem) ? quad_rule : -2;
+  }
   switch (elem) {
     case PMG_ELEM_Q1_HEX: return problem_linear ? RULE_GAUSS2 : RULE_GAUSS3;
     case PMG_ELEM_Q2_HEX: return problem_linear ? RULE_GAUSS3 : RULE_GAUSS4;
@@ -1127,7 +1141,11 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
   }
   if (!L.slot.p) PMG_TRY(build_slot_map(h, L));
   TableCache *T = nullptr;
-  const int rule = rule_for(L.elem, h.prm.problem_linear);
+  const int rule = rule_for(L.elem, h.prm.problem_linear, h.prm.quad_rule);
+  if (rule == -2) {
+    set_error("assemble: quad_rule does not fit the element's shape");
+    return PMG_ERR_UNSUPPORTED;
+  }
   if (rule < 0) {
     set_error("assemble: the degree-6 tetrahedral rule (P2 with INTERNAL_PROBLEM_LINEAR = 0) is not built");
     return PMG_ERR_UNSUPPORTED;
@@ -1181,7 +1199,10 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
       case PMG_ELEM_Q2_HEX * 1000 + 27: return launch_assemble_tc16<PMG_ELEM_Q2_HEX, 27>(h, L, a, tf, T->rtab.p);
       case PMG_ELEM_Q2_HEX * 1000 + 64: return launch_assemble_tc16<PMG_ELEM_Q2_HEX, 64>(h, L, a, tf, T->rtab.p);
       case PMG_ELEM_P1_TET * 1000 + 4: return launch_assemble_tc16<PMG_ELEM_P1_TET, 4>(h, L, a, tf, T->rtab.p);
+      case PMG_ELEM_P1_TET * 1000 + 5: return launch_assemble_tc16<PMG_ELEM_P1_TET, 5>(h, L, a, tf, T->rtab.p);
       case PMG_ELEM_P1_TET * 1000 + 11: return launch_assemble_tc16<PMG_ELEM_P1_TET, 11>(h, L, a, tf, T->rtab.p);
+      case PMG_ELEM_P2_TET * 1000 + 4: return launch_assemble_tc16<PMG_ELEM_P2_TET, 4>(h, L, a, tf, T->rtab.p);
+      case PMG_ELEM_P2_TET * 1000 + 5: return launch_assemble_tc16<PMG_ELEM_P2_TET, 5>(h, L, a, tf, T->rtab.p);
       case PMG_ELEM_P2_TET * 1000 + 11: return launch_assemble_tc16<PMG_ELEM_P2_TET, 11>(h, L, a, tf, T->rtab.p);
       default: break;
     }
@@ -1192,7 +1213,10 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
       case PMG_ELEM_Q1_HEX * 1000 + 8: PMG_TC(PMG_ELEM_Q1_HEX, 8, true);
       case PMG_ELEM_Q1_HEX * 1000 + 27: PMG_TC(PMG_ELEM_Q1_HEX, 27, true);
       case PMG_ELEM_P1_TET * 1000 + 4: PMG_TC(PMG_ELEM_P1_TET, 4, true);
+      case PMG_ELEM_P1_TET * 1000 + 5: PMG_TC(PMG_ELEM_P1_TET, 5, true);
       case PMG_ELEM_P1_TET * 1000 + 11: PMG_TC(PMG_ELEM_P1_TET, 11, true);
+      case PMG_ELEM_P2_TET * 1000 + 4: PMG_TC(PMG_ELEM_P2_TET, 4, true);
+      case PMG_ELEM_P2_TET * 1000 + 5: PMG_TC(PMG_ELEM_P2_TET, 5, true);
       case PMG_ELEM_P2_TET * 1000 + 11: PMG_TC(PMG_ELEM_P2_TET, 11, true);
       default: break;
     }
@@ -1217,7 +1241,10 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
     case PMG_ELEM_Q2_HEX * 1000 + 27: PMG_TRY((launch_assemble<PMG_ELEM_Q2_HEX, 27>(h, L, a))); break;
     case PMG_ELEM_Q2_HEX * 1000 + 64: PMG_TRY((launch_assemble<PMG_ELEM_Q2_HEX, 64>(h, L, a))); break;
     case PMG_ELEM_P1_TET * 1000 + 4: PMG_TRY((launch_assemble<PMG_ELEM_P1_TET, 4>(h, L, a))); break;
+    case PMG_ELEM_P1_TET * 1000 + 5: PMG_TRY((launch_assemble<PMG_ELEM_P1_TET, 5>(h, L, a))); break;
     case PMG_ELEM_P1_TET * 1000 + 11: PMG_TRY((launch_assemble<PMG_ELEM_P1_TET, 11>(h, L, a))); break;
+    case PMG_ELEM_P2_TET * 1000 + 4: PMG_TRY((launch_assemble<PMG_ELEM_P2_TET, 4>(h, L, a))); break;
+    case PMG_ELEM_P2_TET * 1000 + 5: PMG_TRY((launch_assemble<PMG_ELEM_P2_TET, 5>(h, L, a))); break;
     case PMG_ELEM_P2_TET * 1000 + 11: PMG_TRY((launch_assemble<PMG_ELEM_P2_TET, 11>(h, L, a))); break;
     default: set_error("assemble: no kernel for this element / quadrature rule"); return PMG_ERR_UNSUPPORTED;
   }
@@ -1257,9 +1284,10 @@ extern "C" int pmg_quad_points(pmg_handle hh, int level, int *nq, double *xyz) {
     set_error("pmg_quad_points: call pmg_set_level_mesh first");
     return PMG_ERR_STATE;
   }
-  const int rule = rule_for(L.elem, h->prm.problem_linear);
+  const int rule = rule_for(L.elem, h->prm.problem_linear, h->prm.quad_rule);
   if (rule < 0) {
-    set_error("pmg_quad_points: the degree-6 tetrahedral rule is not built");
+    set_error(rule == -2 ? "pmg_quad_points: quad_rule does not fit the element's shape"
+                         : "pmg_quad_points: the degree-6 tetrahedral rule is not built");
     return PMG_ERR_UNSUPPORTED;
   }
   QuadRule q = make_rule(rule);

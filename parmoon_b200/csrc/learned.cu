@@ -10,12 +10,18 @@
 // smoother costs two streaming passes per step.
 //
 // Network: three 3x3x3 convolutions with zero padding on the lattice,
-// 27 -> 32 (ReLU) -> 32 (ReLU) -> 27 channels, weights stored in BF16 and
-// expanded to FP32 in shared memory, FP32 accumulation.  Training (forward,
-// backward, Adam) runs on the device through the pmg_learned_* entry points.
+// 27 -> 32 (ReLU) -> 32 (ReLU) -> 27 channels, BF16 weights and BF16
+// activations (every layer's input is rounded to BF16), FP32 accumulation.
+// The forward runs on the tensor cores as an implicit GEMM per brick of the
+// lattice (mma.sync m16n8k16 BF16: rows = nodes, columns = output channels,
+// reduction = 27 offsets x 32 input channels); the backward (data and weight
+// gradients) and Adam run on FP32 CUDA cores.  Training runs on the device
+// through the pmg_learned_* entry points.
 //
-// Lattice order: node L = i + n1 (j + n1 k); arrays of C channels are
-// channel-major (c * NL + L).  Offsets: k = (di+1) + 3 (dj+1) + 9 (dk+1).
+// Lattice order: node L = i + n1 (j + n1 k).  The forward's activations are
+// node-major BF16 with the channels padded to 32 (L * 32 + c); the FP32
+// arrays of the backward are channel-major (c * NL + L).  Offsets:
+// k = (di+1) + 3 (dj+1) + 9 (dk+1).
 #include "pmg_internal.h"
 #include <cuda_bf16.h>
 #include <cmath>
@@ -38,16 +44,18 @@ __device__ __forceinline__ int lat_nb(int L, int k, int n1) {
 }
 
 // ------------------------------------------------------------- features
-// feat[k][L] = a(i, nb_k(i)) / a(i,i) for an active row i at node L (0 elsewhere);
-// dscale[L] = 1 / a(i,i) for active rows, 0 for Dirichlet rows
+// feature k of node L = a(i, nb_k(i)) / a(i,i) for an active row i at node L
+// (0 elsewhere), rounded to BF16: xf[L * 32 + k] (channels 27..31 stay 0) and,
+// when feat != NULL (training), the same values FP32 channel-major;
+// dscale[L] = 1 / a(i,i) for active rows, 0 for Dirichlet rows.  The caller
+// zeroes xf (and feat).
 __global__ void k_features(int N, int Na, int n1, const int *__restrict__ rp, const int *__restrict__ kc,
-                           const double *__restrict__ a, const int *__restrict__ dof_lat, float *__restrict__ feat,
-                           float *__restrict__ dscale) {
+                           const double *__restrict__ a, const int *__restrict__ dof_lat, __nv_bfloat16 *__restrict__ xf,
+                           float *__restrict__ feat, float *__restrict__ dscale) {
   const int NL = n1 * n1 * n1;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= N) return;
   const int L = dof_lat[r];
-  for (int k = 0; k < 27; k++) feat[(size_t)k * NL + L] = 0.0f;
   if (r >= Na) { dscale[L] = 0.0f; return; }
   double diag = 1.0;
   for (int p = rp[r]; p < rp[r + 1]; p++) if (kc[p] == r) diag = a[p];
@@ -57,45 +65,172 @@ __global__ void k_features(int N, int Na, int n1, const int *__restrict__ rp, co
     const int di = Lc % n1 - i, dj = (Lc / n1) % n1 - j, dk = Lc / (n1 * n1) - kk;
     if (di < -1 || di > 1 || dj < -1 || dj > 1 || dk < -1 || dk > 1) continue;  // not on a 27-point stencil
     const int k = (di + 1) + 3 * (dj + 1) + 9 * (dk + 1);
-    feat[(size_t)k * NL + L] = (float)(a[p] / diag);
+    const __nv_bfloat16 v = __float2bfloat16((float)(a[p] / diag));
+    xf[(size_t)L * 32 + k] = v;
+    if (feat) feat[(size_t)k * NL + L] = __bfloat162float(v);
   }
   dscale[L] = (float)(1.0 / diag);
 }
 
-// ------------------------------------------------------------- convolution
-// out[co][L] = b[co] + sum_{ci,k} w[co][ci][k] in[ci][nb_k(L)]  (ReLU optional;
-// pre-activation kept in zout for the backward pass when non-NULL)
-template <int CIN, int COUT>
-__global__ void __launch_bounds__(128) k_conv_fwd(int n1, const float *__restrict__ in, const __nv_bfloat16 *__restrict__ w,
-                                                  const __nv_bfloat16 *__restrict__ bias, float *__restrict__ out,
-                                                  float *__restrict__ zout, int relu) {
-  extern __shared__ float sw[];  // [ci][k][co] FP32
-  const int NL = n1 * n1 * n1;
-  for (int t = threadIdx.x; t < COUT * CIN * 27; t += blockDim.x) {
-    const int co = t / (CIN * 27), rem = t % (CIN * 27);  // source layout [co][ci][k]
-    const int ci = rem / 27, k = rem % 27;
-    sw[(ci * 27 + k) * COUT + co] = __bfloat162float(w[t]);
+// Weights of one layer, [co][ci][27] BF16, repacked for the tensor-core
+// forward as [k][co][ci] with both channel counts padded to 32 by zeros.
+__global__ void k_pack_weights(int cin, int cout, const __nv_bfloat16 *__restrict__ w, __nv_bfloat16 *__restrict__ wpk) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 27 * 32 * 32) return;
+  const int k = t >> 10, co = (t >> 5) & 31, ci = t & 31;
+  wpk[t] = (co < cout && ci < cin) ? w[((size_t)co * cin + ci) * 27 + k] : __float2bfloat16(0.0f);
+}
+
+// ------------------------------------------------------------- tensor-core convolution
+// One CTA (8 warps) owns a brick of CONV_BX x CONV_BY x CONV_BZ output nodes at
+// a time (persistent over the bricks).  Shared memory holds the packed weights
+// of the layer (27 x 32 x 32 BF16, loaded once) and the brick's input with a
+// one-node halo (18 x 10 x 4 nodes x 64 bytes, zero outside the lattice).
+// Warp w computes the nodes x = 0..15, y = w, z = 0..1 (two m16 tiles) for all
+// 32 output channels (four n8 tiles): per offset and 16-channel chunk two
+// ldmatrix.x4 for the activations, two for the weights and eight mma.
+// Rows of 64 bytes are stored with their four 16-byte chunks permuted
+// (chunk ^ ((row >> 1) & 3)), so the eight rows of one 8x8 ldmatrix read hit
+// distinct banks.
+constexpr int CONV_BX = 16, CONV_BY = 8, CONV_BZ = 2;
+constexpr int CONV_HX = CONV_BX + 2, CONV_HY = CONV_BY + 2, CONV_HZ = CONV_BZ + 2;
+constexpr int CONV_HALO = CONV_HX * CONV_HY * CONV_HZ;  // 720 nodes
+constexpr int CONV_WROWS = 27 * 32;                     // weight rows [k][co]
+constexpr int CONV_SMEM = (CONV_HALO + CONV_WROWS) * 64;  // 101,376 bytes: two CTAs per SM
+
+__device__ __forceinline__ unsigned swz(int row, int chunk) {
+  return (unsigned)(row * 64 + ((chunk ^ ((row >> 1) & 3)) << 4));
+}
+
+__device__ __forceinline__ void ldsm_x4(unsigned addr, unsigned (&r)[4]) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(addr));
+}
+
+// D += A (16x16, row) B (16x8, col), BF16 inputs, FP32 accumulators
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// LAST = false: out = ReLU(conv + b) as BF16 node-major into xo; with a_cm /
+//   z_cm (training) also the rounded activation and the pre-activation, FP32
+//   channel-major.
+// LAST = true: the stencil W[co][L] = (conv + b)[co] * dscale[L], co < cout.
+template <bool LAST>
+__global__ void __launch_bounds__(256, 2)
+    k_conv_tc(int n1, int cout, const __nv_bfloat16 *__restrict__ xi, const __nv_bfloat16 *__restrict__ wpk,
+              const __nv_bfloat16 *__restrict__ bias, __nv_bfloat16 *__restrict__ xo, float *__restrict__ a_cm,
+              float *__restrict__ z_cm, const float *__restrict__ dscale, float *__restrict__ Wst) {
+  extern __shared__ __align__(128) unsigned char conv_sm[];
+  const unsigned s_halo = (unsigned)__cvta_generic_to_shared(conv_sm);
+  const unsigned s_w = s_halo + CONV_HALO * 64;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const size_t NL = (size_t)n1 * n1 * n1;
+  // weights: 864 rows x 4 chunks
+  for (int t = tid; t < CONV_WROWS * 4; t += blockDim.x) {
+    const int row = t >> 2, ch = t & 3;
+    const uint4 v = __ldg(reinterpret_cast<const uint4 *>(wpk) + t);
+    *reinterpret_cast<uint4 *>(conv_sm + CONV_HALO * 64 + swz(row, ch)) = v;
   }
-  __syncthreads();
-  const int L = blockIdx.x * blockDim.x + threadIdx.x;
-  if (L >= NL) return;
-  float acc[COUT];
+  float bv[4][2];
 #pragma unroll
-  for (int co = 0; co < COUT; co++) acc[co] = __bfloat162float(bias[co]);
-  for (int k = 0; k < 27; k++) {
-    const int nb = lat_nb(L, k, n1);
-    if (nb < 0) continue;
-    for (int ci = 0; ci < CIN; ci++) {
-      const float v = in[(size_t)ci * NL + nb];
-      const float *wr = sw + (ci * 27 + k) * COUT;
+  for (int nt = 0; nt < 4; nt++)
 #pragma unroll
-      for (int co = 0; co < COUT; co++) acc[co] += wr[co] * v;
+    for (int e = 0; e < 2; e++) {
+      const int co = nt * 8 + 2 * (lane & 3) + e;
+      bv[nt][e] = co < cout ? __bfloat162float(bias[co]) : 0.0f;
     }
-  }
+  const int nbx = (n1 + CONV_BX - 1) / CONV_BX, nby = (n1 + CONV_BY - 1) / CONV_BY, nbz = (n1 + CONV_BZ - 1) / CONV_BZ;
+  const int nbricks = nbx * nby * nbz;
+  // per-lane ldmatrix rows: A (activations) row within the m16 tile and chunk half;
+  // B (weights) output channel within a pair of n8 tiles and chunk half
+  const int a_row = (lane & 7) + 8 * ((lane >> 3) & 1), a_half = lane >> 4;
+  const int b_co = 8 * (lane >> 4) + (lane & 7), b_half = (lane >> 3) & 1;
+  for (int br = blockIdx.x; br < nbricks; br += gridDim.x) {
+    const int bx = br % nbx, by = (br / nbx) % nby, bz = br / (nbx * nby);
+    const int x0 = bx * CONV_BX, y0 = by * CONV_BY, z0 = bz * CONV_BZ;
+    __syncthreads();  // the previous brick's reads of the halo are done
+    for (int t = tid; t < CONV_HALO * 4; t += blockDim.x) {
+      const int node = t >> 2, ch = t & 3;
+      const int hx = node % CONV_HX, hy = (node / CONV_HX) % CONV_HY, hz = node / (CONV_HX * CONV_HY);
+      const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 - 1 + hz;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (gx >= 0 && gy >= 0 && gz >= 0 && gx < n1 && gy < n1 && gz < n1) {
+        const size_t L = (size_t)gx + (size_t)n1 * ((size_t)gy + (size_t)n1 * gz);
+        v = __ldg(reinterpret_cast<const uint4 *>(xi + L * 32) + ch);
+      }
+      *reinterpret_cast<uint4 *>(conv_sm + swz(node, ch)) = v;
+    }
+    __syncthreads();
+    float acc[2][4][4];
 #pragma unroll
-  for (int co = 0; co < COUT; co++) {
-    if (zout) zout[(size_t)co * NL + L] = acc[co];
-    out[(size_t)co * NL + L] = relu ? fmaxf(acc[co], 0.0f) : acc[co];
+    for (int m = 0; m < 2; m++)
+#pragma unroll
+      for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) acc[m][nt][e] = 0.0f;
+#pragma unroll 3
+    for (int k = 0; k < 27; k++) {
+      const int dx = k % 3, dy = (k / 3) % 3, dz = k / 9;
+#pragma unroll
+      for (int kc = 0; kc < 2; kc++) {
+        unsigned a[2][4], b[2][4];
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+          const int row = (a_row + dx) + CONV_HX * ((warp + dy) + CONV_HY * (m + dz));
+          ldsm_x4(s_halo + swz(row, 2 * kc + a_half), a[m]);
+        }
+#pragma unroll
+        for (int p = 0; p < 2; p++) {
+          const int row = k * 32 + 16 * p + b_co;
+          ldsm_x4(s_w + swz(row, 2 * kc + b_half), b[p]);
+        }
+#pragma unroll
+        for (int m = 0; m < 2; m++)
+#pragma unroll
+          for (int p = 0; p < 2; p++) {
+            mma_bf16(acc[m][2 * p], a[m], b[p][0], b[p][1]);
+            mma_bf16(acc[m][2 * p + 1], a[m], b[p][2], b[p][3]);
+          }
+      }
+    }
+    // epilogue: c0,c1 = (row g, channels 2q, 2q+1), c2,c3 = (row g+8, ...)
+    const int g = lane >> 2, q = lane & 3;
+    const int gy = y0 + warp;
+#pragma unroll
+    for (int m = 0; m < 2; m++) {
+      const int gz = z0 + m;
+#pragma unroll
+      for (int hrow = 0; hrow < 2; hrow++) {
+        const int gx = x0 + g + 8 * hrow;
+        if (gx >= n1 || gy >= n1 || gz >= n1) continue;
+        const size_t L = (size_t)gx + (size_t)n1 * ((size_t)gy + (size_t)n1 * gz);
+        const float ds = LAST ? dscale[L] : 0.0f;
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) {
+          const int co = nt * 8 + 2 * q;
+          const float v0 = acc[m][nt][2 * hrow] + bv[nt][0], v1 = acc[m][nt][2 * hrow + 1] + bv[nt][1];
+          if (LAST) {
+            if (co < cout) Wst[(size_t)co * NL + L] = v0 * ds;
+            if (co + 1 < cout) Wst[(size_t)(co + 1) * NL + L] = v1 * ds;
+          } else {
+            const __nv_bfloat162 r = __floats2bfloat162_rn(fmaxf(v0, 0.0f), fmaxf(v1, 0.0f));
+            *reinterpret_cast<__nv_bfloat162 *>(xo + L * 32 + co) = r;
+            if (a_cm) {
+              a_cm[(size_t)co * NL + L] = __low2float(r);
+              a_cm[(size_t)(co + 1) * NL + L] = __high2float(r);
+              z_cm[(size_t)co * NL + L] = v0;
+              z_cm[(size_t)(co + 1) * NL + L] = v1;
+            }
+          }
+        }
+      }
+    }
   }
 }
 
@@ -180,15 +315,6 @@ __global__ void k_relu_bwd(size_t n, const float *__restrict__ z, float *__restr
     if (!(z[i] > 0.0f)) g[i] = 0.0f;
 }
 
-// W[k][L] = out3[k][L] * dscale[L]  (zero on Dirichlet nodes)
-__global__ void k_stencil_scale(int NL, const float *__restrict__ out3, const float *__restrict__ dscale,
-                                float *__restrict__ W) {
-  const int L = blockIdx.x * blockDim.x + threadIdx.x;
-  if (L >= NL) return;
-  const float s = dscale[L];
-  for (int k = 0; k < 27; k++) W[(size_t)k * NL + L] = out3[(size_t)k * NL + L] * s;
-}
-
 // ------------------------------------------------------------- smoothing step
 // x_i += omega sum_k W_k(L_i) r_{dof(nb_k(L_i))} on active dofs (dof order vectors)
 template <typename T>
@@ -228,38 +354,60 @@ static int conv_smem(int cin, int cout) { return cin * cout * 27 * (int)sizeof(f
 static int set_conv_attrs() {
   static bool done = false;
   if (done) return PMG_OK;
-  PMG_CUDA(cudaFuncSetAttribute(k_conv_fwd<NET_C0, NET_C1>, cudaFuncAttributeMaxDynamicSharedMemorySize, conv_smem(NET_C0, NET_C1)));
-  PMG_CUDA(cudaFuncSetAttribute(k_conv_fwd<NET_C1, NET_C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, conv_smem(NET_C1, NET_C2)));
-  PMG_CUDA(cudaFuncSetAttribute(k_conv_fwd<NET_C2, NET_C3>, cudaFuncAttributeMaxDynamicSharedMemorySize, conv_smem(NET_C2, NET_C3)));
+  PMG_CUDA(cudaFuncSetAttribute(k_conv_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, CONV_SMEM));
+  PMG_CUDA(cudaFuncSetAttribute(k_conv_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, CONV_SMEM));
   PMG_CUDA(cudaFuncSetAttribute(k_conv_bwd_data<NET_C1, NET_C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, conv_smem(NET_C1, NET_C2)));
   PMG_CUDA(cudaFuncSetAttribute(k_conv_bwd_data<NET_C2, NET_C3>, cudaFuncAttributeMaxDynamicSharedMemorySize, conv_smem(NET_C2, NET_C3)));
   done = true;
   return PMG_OK;
 }
 
-// forward pass on one level: features -> W (stencil) ; keeps activations in S
-static int net_forward(cudaStream_t s, Level &L, const __nv_bfloat16 *wb, NetScratch &S) {
+// persistent grid of the tensor-core convolution: two CTAs per SM, at most one per brick
+static int conv_grid(int n1, int num_sms) {
+  const long nb = (long)((n1 + CONV_BX - 1) / CONV_BX) * ((n1 + CONV_BY - 1) / CONV_BY) * ((n1 + CONV_BZ - 1) / CONV_BZ);
+  return (int)std::min<long>(nb, 2L * num_sms);
+}
+
+// forward pass on one level: features -> W (stencil, L.lw_stencil); with
+// train, the FP32 channel-major layer inputs and pre-activations stay in S
+static int net_forward(cudaStream_t s, int num_sms, Level &L, const __nv_bfloat16 *wb, NetScratch &S, bool train) {
   const int n1 = L.lat_n[0], NL = n1 * n1 * n1;
   PMG_TRY(set_conv_attrs());
-  PMG_TRY(S.alloc(NL, NET_C0, NET_C1, NET_C2, NET_C3));
-  PMG_CUDA(cudaMemsetAsync(S.feat.p, 0, sizeof(float) * NET_C0 * (size_t)NL, s));
+  PMG_TRY(S.alloc(NL, NET_C0, NET_C1, NET_C2, train));
+  __nv_bfloat16 *xa = reinterpret_cast<__nv_bfloat16 *>(S.xa.p), *xb = reinterpret_cast<__nv_bfloat16 *>(S.xb.p);
+  __nv_bfloat16 *wpk = reinterpret_cast<__nv_bfloat16 *>(S.wpk.p);
+  const int WPK = 27 * 32 * 32;
+  k_pack_weights<<<WPK / 256, 256, 0, s>>>(NET_C0, NET_C1, wb + NET_OFF_W1, wpk);
+  k_pack_weights<<<WPK / 256, 256, 0, s>>>(NET_C1, NET_C2, wb + NET_OFF_W2, wpk + WPK);
+  k_pack_weights<<<WPK / 256, 256, 0, s>>>(NET_C2, NET_C3, wb + NET_OFF_W3, wpk + 2 * WPK);
+  PMG_CUDA(cudaMemsetAsync(xa, 0, sizeof(__nv_bfloat16) * 32 * (size_t)NL, s));
   PMG_CUDA(cudaMemsetAsync(S.dscale.p, 0, sizeof(float) * (size_t)NL, s));
-  k_features<<<(L.N + 255) / 256, 256, 0, s>>>(L.N, L.Na, n1, L.rowptr.p, L.kcol.p, L.A.p, L.dof_ijk.p, S.feat.p,
-                                                S.dscale.p);
-  const int g = (NL + 127) / 128;
-  k_conv_fwd<NET_C0, NET_C1><<<g, 128, conv_smem(NET_C0, NET_C1), s>>>(n1, S.feat.p, wb + NET_OFF_W1, wb + NET_OFF_B1,
-                                                                       S.a1.p, S.z1.p, 1);
-  k_conv_fwd<NET_C1, NET_C2><<<g, 128, conv_smem(NET_C1, NET_C2), s>>>(n1, S.a1.p, wb + NET_OFF_W2, wb + NET_OFF_B2,
-                                                                       S.a2.p, S.z2.p, 1);
-  k_conv_fwd<NET_C2, NET_C3><<<g, 128, conv_smem(NET_C2, NET_C3), s>>>(n1, S.a2.p, wb + NET_OFF_W3, wb + NET_OFF_B3,
-                                                                       S.out3.p, nullptr, 0);
+  if (train) PMG_CUDA(cudaMemsetAsync(S.feat.p, 0, sizeof(float) * NET_C0 * (size_t)NL, s));
+  k_features<<<(L.N + 255) / 256, 256, 0, s>>>(L.N, L.Na, n1, L.rowptr.p, L.kcol.p, L.A.p, L.dof_ijk.p, xa,
+                                                train ? S.feat.p : nullptr, S.dscale.p);
   PMG_TRY(L.lw_stencil.alloc((size_t)27 * NL));
-  k_stencil_scale<<<(NL + 255) / 256, 256, 0, s>>>(NL, S.out3.p, S.dscale.p, L.lw_stencil.p);
-  count_launches(5);
+  const int g = conv_grid(n1, num_sms);
+  k_conv_tc<false><<<g, 256, CONV_SMEM, s>>>(n1, NET_C1, xa, wpk, wb + NET_OFF_B1, xb, train ? S.a1.p : nullptr,
+                                              train ? S.z1.p : nullptr, nullptr, nullptr);
+  k_conv_tc<false><<<g, 256, CONV_SMEM, s>>>(n1, NET_C2, xb, wpk + WPK, wb + NET_OFF_B2, xa, train ? S.a2.p : nullptr,
+                                              train ? S.z2.p : nullptr, nullptr, nullptr);
+  k_conv_tc<true><<<g, 256, CONV_SMEM, s>>>(n1, NET_C3, xa, wpk + 2 * WPK, wb + NET_OFF_B3, nullptr, nullptr, nullptr,
+                                             S.dscale.p, L.lw_stencil.p);
+  count_launches(7);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
 }
 
+
+int learned_forward(Handle &h, Level &L) {
+  if (!h.has_learned || L.lat_n[0] <= 0) {
+    set_error("learned smoother: the forward needs weights and a lattice");
+    return PMG_ERR_STATE;
+  }
+  PMG_TRY(net_forward(h.stream, h.num_sms, L, reinterpret_cast<const __nv_bfloat16 *>(h.lw_bf16.p), h.net_scratch, false));
+  L.lw_fresh = true;
+  return PMG_OK;
+}
 
 // network -> stencil on every level that has a lattice (after assembly)
 int learned_prepare(Handle &h) {
@@ -273,8 +421,7 @@ int learned_prepare(Handle &h) {
       return PMG_ERR_STATE;
     }
     if (L.lw_fresh) continue;
-    PMG_TRY(net_forward(h.stream, L, reinterpret_cast<const __nv_bfloat16 *>(h.lw_bf16.p), h.net_scratch));
-    L.lw_fresh = true;
+    PMG_TRY(learned_forward(h, L));
   }
   return PMG_OK;
 }
@@ -465,7 +612,7 @@ int pmg_learned_train_step(pmg_handle hh, int level, int n_samples, const double
     PMG_TRY(L.tpos.upload(tp.data(), tp.size(), s));
   }
   NetScratch &S = h->net_scratch;
-  PMG_TRY(net_forward(s, L, reinterpret_cast<const __nv_bfloat16 *>(h->lw_bf16.p), S));
+  PMG_TRY(net_forward(s, h->num_sms, L, reinterpret_cast<const __nv_bfloat16 *>(h->lw_bf16.p), S, true));
   PMG_TRY(h->lw_grad.alloc(NET_NPARAM));
   PMG_TRY(h->lw_m.alloc(NET_NPARAM));
   PMG_TRY(h->lw_v.alloc(NET_NPARAM));

@@ -79,6 +79,11 @@ static int validate_params(const pmg_params *p) {
   if (p->reference_restart_rule != 0 && p->reference_restart_rule != 1) return bad("reference_restart_rule must be 0 or 1");
   if ((p->slc_all != 0 && p->slc_all != 1) || (p->slc_fine != 0 && p->slc_fine != 1)) return bad("slc_all / slc_fine must be 0 or 1");
   if (p->learned_steps < 0 || p->learned_steps > 64) return bad("learned_steps must be in [0, 64]");
+  if (p->learned_guard_off != 0 && p->learned_guard_off != 1) return bad("learned_guard_off must be 0 or 1");
+  if (p->quad_rule != PMG_QUAD_AUTO && p->quad_rule != PMG_QUAD_GAUSS2 && p->quad_rule != PMG_QUAD_GAUSS3 &&
+      p->quad_rule != PMG_QUAD_GAUSS4 && p->quad_rule != PMG_QUAD_KEAST4 && p->quad_rule != PMG_QUAD_KEAST5 &&
+      p->quad_rule != PMG_QUAD_KEAST11)
+    return bad("quad_rule must be 0 or one of PMG_QUAD_*");
   if (p->poly_degree < 0) return bad("poly_degree must be >= 0");
   const double pos[] = {p->smooth_omega, p->div_factor};
   for (double v : pos)
@@ -695,6 +700,7 @@ int pmg_time_kernel(pmg_handle hh, int kernel, int level, int form, int reps, do
       case PMG_KERNEL_CSR_SPMV64: return spmv<double>(s, L, L.A.p, x64.p, y64.p);
       case PMG_KERNEL_ASSEMBLE: return assemble_level(*h, L, form, L.A.p, true, L.rhs.p);
       case PMG_KERNEL_COARSE_FACTOR: return coarse_factor(*h);
+      case PMG_KERNEL_LEARNED_FWD: return learned_forward(*h, L);
       default: set_error("pmg_time_kernel: unknown kernel"); return PMG_ERR_ARG;
     }
   };
@@ -724,6 +730,16 @@ int pmg_time_kernel(pmg_handle hh, int kernel, int level, int form, int reps, do
     // LU (2/3 n^3) and inverse (4/3 n^3) flops; the dense matrix is read and written
     by = 2.0 * 8.0 * N * N;
     fl = 2.0 * N * N * N;
+  } else if (kernel == PMG_KERNEL_LEARNED_FWD) {
+    if (!h->has_learned || L.lat_n[0] <= 0) {
+      set_error("pmg_time_kernel: the learned forward needs weights and the level's lattice");
+      return PMG_ERR_STATE;
+    }
+    // per lattice node: the CSR row (12 B per entry), three BF16 layer inputs and
+    // outputs (64 B each way), the FP32 stencil (27 x 4 B)
+    const double NL = (double)L.lat_n[0] * L.lat_n[0] * L.lat_n[0];
+    by = 12.0 * nnz + NL * (3 * 128.0 + 108.0);
+    fl = 2.0 * 27 * (27 * 32 + 32 * 32 + 32 * 27) * NL;
   } else {
     // coloured scatter per element: n_loc^2 (4 slot + 8 read + 8 write) + n_loc (4 dof + 16 rhs) + vertices
     const double nl = L.nloc, nv = L.nvert;

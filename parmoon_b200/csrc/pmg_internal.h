@@ -162,20 +162,27 @@ struct Level {
   DBuf<double> sell_val64, sell_invd64;
 };
 
-// activations of the stencil network on one lattice (learned.cu)
+// Activations of the stencil network.  The tensor-core forward reads and
+// writes node-major BF16 (32 channels = 64 bytes per lattice node, two
+// ping-pong buffers); training also keeps FP32 channel-major copies of every
+// layer's input (the BF16-rounded values) and pre-activations for the
+// backward kernels.
 struct NetScratch {
-  DBuf<float> feat, a1, z1, a2, z2, out3, dscale;
-  int NL = 0;
-  int alloc(int nl, int c0, int c1, int c2, int c3) {
-    if (nl == NL) return PMG_OK;
-    PMG_TRY(feat.alloc((size_t)c0 * nl));
-    PMG_TRY(a1.alloc((size_t)c1 * nl));
-    PMG_TRY(z1.alloc((size_t)c1 * nl));
-    PMG_TRY(a2.alloc((size_t)c2 * nl));
-    PMG_TRY(z2.alloc((size_t)c2 * nl));
-    PMG_TRY(out3.alloc((size_t)c3 * nl));
-    PMG_TRY(dscale.alloc(nl));
-    NL = nl;
+  DBuf<uint16_t> xa, xb, wpk;
+  DBuf<float> feat, a1, z1, a2, z2, dscale;
+  // grow-only: the levels of a hierarchy share the buffers of the largest
+  int alloc(int nl, int c0, int c1, int c2, bool train) {
+    PMG_TRY(xa.reserve((size_t)32 * nl));
+    PMG_TRY(xb.reserve((size_t)32 * nl));
+    PMG_TRY(dscale.reserve(nl));
+    PMG_TRY(wpk.reserve((size_t)3 * 27 * 32 * 32));
+    if (train) {
+      PMG_TRY(feat.reserve((size_t)c0 * nl));
+      PMG_TRY(a1.reserve((size_t)c1 * nl));
+      PMG_TRY(z1.reserve((size_t)c1 * nl));
+      PMG_TRY(a2.reserve((size_t)c2 * nl));
+      PMG_TRY(z2.reserve((size_t)c2 * nl));
+    }
     return PMG_OK;
   }
 };
@@ -300,6 +307,8 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
 // ------------------------------------------------------------- learned smoother (learned.cu)
 int learned_num_params();
 int learned_prepare(Handle &h);
+// the network's forward on one level (stencil into L.lw_stencil)
+int learned_forward(Handle &h, Level &L);
 template <typename T>
 int learned_smooth(cudaStream_t s, const Level &L, const T *r, T *x, double omega);
 

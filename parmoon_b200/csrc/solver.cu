@@ -812,10 +812,12 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
   };
 
   // learned smoother guard: 0 = calibrating with SSOR, 1 = learned, 2 = SSOR took over
+  // (without the guard the learned smoother runs from the first cycle on)
   const bool learned = h.prm.smoother == PMG_SMOOTHER_LEARNED;
+  const bool guarded = learned && !h.prm.learned_guard_off;
   const int kCalib = 2;
-  int guard_phase = learned ? 0 : 2, learned_start = 0;
-  double rho_plain = 0.0;
+  int guard_phase = learned ? (guarded ? 0 : 1) : 2, learned_start = 0, learned_cycles = 0;
+  double rho_plain = 0.0, rho_learned = 0.0;
   std::vector<double> res_hist;
   double beta;
   PMG_TRY(residual(V, beta));
@@ -837,6 +839,7 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
       double *vi = V + (size_t)i * N, *zi = Z + (size_t)i * N;
       if (!vc_timed) PMG_CUDA(cudaEventRecord(h.ev[7], s));
       PMG_TRY(precondition(h, vi, zi, guard_phase == 1));
+      if (guard_phase == 1) learned_cycles++;
       if (!vc_timed) {
         PMG_CUDA(cudaEventRecord(h.ev[8], s));
         vc_timed = true;
@@ -871,15 +874,15 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
       res = fabs(sv[i + 1]);
       iters = j;
       res_hist.push_back(res);
-      if (guard_phase == 0 && learned && j == kCalib) {
+      if (guard_phase == 0 && j == kCalib) {
         // per-cycle contraction of the plain SSOR V-cycle over the first cycles
         rho_plain = pow(res / res_hist[0], 1.0 / kCalib);
         guard_phase = 1;
         learned_start = j;
       } else if (guard_phase == 1 && j - learned_start >= 2) {
         const int nl = j - learned_start;
-        const double rho_l = pow(res / res_hist[learned_start], 1.0 / nl);
-        if (rho_l > rho_plain) guard_phase = 2;  // the plain SSOR smoother takes over
+        rho_learned = pow(res / res_hist[learned_start], 1.0 / nl);
+        if (guarded && rho_learned > rho_plain) guard_phase = 2;  // the plain SSOR smoother takes over
       }
       if (!std::isfinite(res)) { status = PMG_ERR_NONFINITE; set_error("solve: non-finite residual estimate"); done = true; i++; break; }
       double ref = h.prm.reference_restart_rule ? r0 : res0;
@@ -922,6 +925,9 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
     st->rel_res = res0 > 0 ? res_final / res0 : 0.0;
     st->mean_contraction = (iters > 0 && res0 > 0 && res_final > 0) ? pow(res_final / res0, 1.0 / iters) : 0.0;
     st->smoother_used = learned ? (guard_phase == 1 ? PMG_SMOOTHER_LEARNED : PMG_SMOOTHER_SSOR) : h.prm.smoother;
+    st->rho_plain = rho_plain;
+    st->rho_learned = rho_learned;
+    st->learned_cycles = learned_cycles;
     st->seconds = h.t_solve;
     float a = 0, b = 0;
     st->setup_seconds = cudaEventElapsedTime(&a, h.ev[2], h.ev[6]) == cudaSuccess ? a * 1e-3 : 0.0;
@@ -1144,6 +1150,8 @@ int solve_dd(Handle &h, const pmg_comm *comm, double *sol_host, const double *rh
     st->seconds = h.t_solve;
     st->setup_seconds = 0.0;
     st->vcycle_seconds = 0.0;
+    st->rho_plain = st->rho_learned = 0.0;
+    st->learned_cycles = 0;
   }
   if (status == PMG_ERR_NOT_CONVERGED)
     set_error("solve_dd: the iteration limit (lin_maxit) was reached before |r| <= max(lin_res_min, lin_red |r0|)");

@@ -43,3 +43,48 @@ def test_reference_matrix_kernel_equals_point_kernel(pmg, elem, form, kind, jitt
             A0, r0 = out[path][l]
             assert np.max(np.abs(A0 - A1) / rowmax) <= 1e-13, path
             assert np.max(np.abs(r0 - r1)) <= 1e-13 * max(1.0, np.max(np.abs(r1))), path
+
+
+@pytest.mark.parametrize("elem,form,kind", [("P2_TET", "GALERKIN", "LOGNORMAL"), ("P2_TET", "SUPG", "CONST"),
+                                            ("P1_TET", "SUPG", "LOGNORMAL"), ("P1_TET", "GALERKIN", "CONST")])
+def test_five_point_tet_rule_matches_oracle(pmg, elem, form, kind):
+    """quad_rule = PMG_QUAD_KEAST5, the 5-point degree-3 rule the P2 lognormal
+    workload names, on every kernel path against the oracle's assembly with the
+    same rule (1e-12 of the row's largest entry)."""
+    from oracle import cd3d as O
+    from parmoon_b200.configs import lognormal_modes
+    et = getattr(pmg, elem)
+    fm = getattr(pmg, "FORM_" + form)
+    levels = pmg.struct_hierarchy(et, 4, 2, jitter=0.2, seed=11)
+    if kind == "LOGNORMAL":
+        kw = dict(kind=pmg.COEF_LOGNORMAL, eps=1e-2, f=2.0, modes=lognormal_modes(5))
+    else:
+        kw = dict(kind=pmg.COEF_CONST, eps=1e-3, b=(1.0, -0.5, 0.25), c=0.3, f=2.0)
+    F = levels[-1]
+    dv = F["dof_xyz"][F["active_bound"]:] @ np.array([1.0, 2.0, -1.0])
+    ok = {"kind": kw["kind"], "eps": kw["eps"], "b": kw.get("b", (0, 0, 0)), "c": kw.get("c", 0.0), "f": kw["f"],
+          "modes": kw.get("modes")}
+    Ao, ro = O.assemble(getattr(O, elem[:2]), F["elem_dof"], F["cell_vert"], F["N"], F["active_bound"],
+                        F["rowptr"], F["kcol"], getattr(O, "FORM_" + form), O.make_coeff(**ok), quad=105,
+                        dir_values=dv)
+    rows = np.repeat(np.arange(F["N"]), np.diff(F["rowptr"]))
+    rowmax = np.maximum.reduceat(np.abs(Ao), F["rowptr"][:-1])[rows]
+    for path in (0, 1, 2):
+        h = pmg.Handle(2, pmg.default_params(assembly_kernel=path, quad_rule=pmg.QUAD_KEAST5))
+        h.set_coefficients(pmg.coeff(**kw))
+        pmg.load_hierarchy(h, levels, dirichlet=lambda x, y, z: x + 2 * y - z)
+        h.assemble(-1, fm, copy_out=False)
+        A, r = h.get_matrix(1), h.get_rhs(1)
+        h.close()
+        assert np.max(np.abs(A - Ao) / rowmax) <= 1e-12, path
+        assert np.max(np.abs(r - ro)) <= 1e-12 * max(1.0, np.max(np.abs(ro))), path
+
+
+def test_quad_rule_must_fit_the_element(pmg):
+    levels = pmg.struct_hierarchy(pmg.Q1_HEX, 2, 1)
+    h = pmg.Handle(1, pmg.default_params(quad_rule=pmg.QUAD_KEAST5))
+    pmg.load_hierarchy(h, levels)
+    with pytest.raises(pmg.PmgError) as e:
+        h.assemble(-1, pmg.FORM_GALERKIN, copy_out=False)
+    assert e.value.code == pmg.ERR_UNSUPPORTED
+    h.close()

@@ -32,12 +32,12 @@ def test_learned_oracle_gradient_matches_finite_differences():
     Ad = np.zeros((N, N))
     Ad[np.repeat(np.arange(N), np.diff(rp)), kc] = A
     r = Ad @ e
-    loss, g = LO.loss_and_grad(theta, n1, rp, kc, A, Na, m["dof_lat"], e, r)
+    loss, g = LO.loss_and_grad(theta, n1, rp, kc, A, Na, m["dof_lat"], e, r, act_bf16=False)
     for trial in range(4):
         d = rng.standard_normal(theta.size)
         h = 1e-6
-        lp, _ = LO.loss_and_grad(theta + h * d, n1, rp, kc, A, Na, m["dof_lat"], e, r)
-        lm, _ = LO.loss_and_grad(theta - h * d, n1, rp, kc, A, Na, m["dof_lat"], e, r)
+        lp, _ = LO.loss_and_grad(theta + h * d, n1, rp, kc, A, Na, m["dof_lat"], e, r, act_bf16=False)
+        lm, _ = LO.loss_and_grad(theta - h * d, n1, rp, kc, A, Na, m["dof_lat"], e, r, act_bf16=False)
         fd = (lp - lm) / (2 * h)
         assert abs(fd - g @ d) <= 1e-6 * max(1.0, abs(fd)), (trial, fd, g @ d)
 
