@@ -39,6 +39,10 @@ extern "C" {
  * [-1,1]^3, tetrahedra follow the reference vertex/edge numbering. */
 #define PMG_ELEM_Q1_HEX   1   /*  8 local dofs */
 #define PMG_ELEM_Q2_HEX   2   /* 27 local dofs */
+#define PMG_ELEM_NQ1_HEX  3   /*  6 local dofs: the non-conforming rotated trilinear element N_Q1
+                                 (include/FE3D/BF_N_H_Q1_3D.h, point-value nodal functionals at the
+                                 face midpoints, NF_N_H_Q1_3D.h) of the non-conforming levels of
+                                 SC_MG_TYPE_SCALAR = 1 */
 #define PMG_ELEM_P1_TET  11   /*  4 local dofs */
 #define PMG_ELEM_P2_TET  12   /* 10 local dofs */
 

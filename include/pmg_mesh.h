@@ -22,7 +22,10 @@ int pmg_struct_sizes(int elem_type, int n, int *n_cells, int *n_dofs, int *nloc)
 
 /* Build the level (caller allocates): elem_dof n_cells x nloc, cell_vert
  * n_cells x 8 x 3 (tetrahedra use the first 4 vertex slots), dof_xyz N x 3,
- * dof_lat N (lattice index i + n1 (j + n1 k), n1 = degree n + 1).
+ * dof_lat N (lattice index i + n1 (j + n1 k), n1 = degree n + 1; for N_Q1,
+ * whose dofs are the 3 n^2 (n+1) faces, the face's index instead: x faces,
+ * then y faces, then z faces, each i + (n_i+1)(j + ...) as the builder
+ * documents).
  * jitter > 0 perturbs interior vertices by U(-jitter h, jitter h) per
  * coordinate (seeded; meaningful for tetrahedra, whose maps stay affine). */
 int pmg_struct_build(int elem_type, int n, double jitter, unsigned long long seed, int *elem_dof,
@@ -47,6 +50,22 @@ int pmg_struct_prolongation(int elem_type, int nc, const int *lat_c, int n_coars
 int pmg_nested_prolongation(int elem_type, int n_coarse_cells, const int *c_elem_dof, const double *c_cell_vert,
                             int n_coarse, int n_fine, const double *f_dof_xyz, const int *f_dof_cell,
                             int *p_row_ptr, int *p_col, double *p_val);
+
+/* Prolongation as Prolongate applies it for any pair of spaces on nested
+ * meshes (MGComponents3D.C:208-488, GetProlongationMatrix3D, FEDatabase3D.C:
+ * 1656-1815): every fine cell K takes the coarse function of its parent cell
+ * f_parent[K] (the cell itself when both spaces live on one mesh) at the
+ * fine element's nodal points -- point values at the Lagrange nodes, at the
+ * face midpoints for N_Q1 -- and every fine dof gets the mean over the fine
+ * cells that hold it.  For conforming nested spaces all those values agree;
+ * for N_Q1 a fine face on a coarse face takes the mean of the two parents'
+ * values, and N_Q1 -> Q1 on one mesh averages the cells around a vertex.
+ * Both meshes in the pmg_set_level_mesh layout (8 vertex slots per cell,
+ * affine cells); p_col == NULL: counts only. */
+int pmg_cell_prolongation(int c_elem_type, int n_coarse_cells, const int *c_elem_dof, const double *c_cell_vert,
+                          int n_coarse, int f_elem_type, int n_fine_cells, const int *f_elem_dof,
+                          const double *f_cell_vert, const int *f_parent, int n_fine, int *p_row_ptr, int *p_col,
+                          double *p_val);
 
 /* Lattice colouring for the multicolour SSOR: (i mod m, j mod m, k mod m),
  * m = degree + 1; no two coupled dofs share a colour. */

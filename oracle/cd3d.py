@@ -15,6 +15,7 @@ SRC = os.path.join(HERE, "cd3d_oracle.c")
 LIB = os.path.join(HERE, "_build", "libcd3d_oracle.so")
 
 Q1, Q2, P1, P2 = 1, 2, 11, 12
+NQ1 = 3  # the non-conforming N_Q1 hexahedron (face-midpoint values)
 FORM_GALERKIN, FORM_SUPG, FORM_MASS, FORM_MASS_SUPG, FORM_STIFF_SUPG = 1, 2, 3, 4, 5
 COEF_CONST, COEF_SINE_RHS, COEF_LOGNORMAL, COEF_CURL_FOURIER, COEF_ROTATING, COEF_AMC = range(6)
 
@@ -63,14 +64,14 @@ def _ptr(a):
 
 
 def nloc_of(elem):
-    return {Q1: 8, Q2: 27, P1: 4, P2: 10}[elem]
+    return {Q1: 8, Q2: 27, NQ1: 6, P1: 4, P2: 10}[elem]
 
 
 def default_quad(elem, linear=True):
     """Rule the reference picks with INTERNAL_PROBLEM_LINEAR=1 (linear) or 0."""
     if elem == Q1:
         return 2 if linear else 3
-    if elem == Q2:
+    if elem in (Q2, NQ1):
         return 3 if linear else 4
     if elem == P1:
         return 104 if linear else 111
@@ -264,4 +265,23 @@ def errors(elem, elem_dof, cell_vert, sol, quad, exact_kind, t=0.0):
                           _ptr(np.ascontiguousarray(sol, dtype=np.float64)), _i(quad), _i(exact_kind), _d(t), _ptr(out))
     if rc != 0:
         raise RuntimeError("orc_errors failed")
+    return out
+
+
+def cell_transfer(mode, c_elem, c_elem_dof, c_cell_vert, n_coarse, f_elem, f_elem_dof, f_cell_vert, f_parent,
+                  n_fine, vec):
+    """Prolongate (mode 0: coarse -> fine) or DefectRestriction (mode 1: fine -> coarse)
+    restated operationally for any pair of spaces on nested meshes (cell averaging)."""
+    ced = np.ascontiguousarray(c_elem_dof, dtype=np.int32)
+    fed = np.ascontiguousarray(f_elem_dof, dtype=np.int32)
+    ccv = np.ascontiguousarray(c_cell_vert, dtype=np.float64)
+    fcv = np.ascontiguousarray(f_cell_vert, dtype=np.float64)
+    par = np.ascontiguousarray(f_parent, dtype=np.int32)
+    v = np.ascontiguousarray(vec, dtype=np.float64)
+    out = np.zeros(n_fine if mode == 0 else n_coarse)
+    rc = lib().orc_cell_transfer(_i(mode), _i(c_elem), _i(ced.size // nloc_of(c_elem)), _ptr(ced), _ptr(ccv),
+                                 _i(n_coarse), _i(f_elem), _i(fed.size // nloc_of(f_elem)), _ptr(fed), _ptr(fcv),
+                                 _ptr(par), _i(n_fine), _ptr(v), _ptr(out))
+    if rc != 0:
+        raise RuntimeError(f"orc_cell_transfer failed: {rc}")
     return out

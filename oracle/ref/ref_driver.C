@@ -24,7 +24,8 @@
 //   problem(laplace|cdsupg|cdgal) eps(1) b1 b2 b3 (0) linear_quad(1)
 //   disc(1=Galerkin,2=SUPG) restart(20) red(1e-10) maxit(1000) smoother(3)
 //   pre(2) post(2) coarse_smoother(3) coarse_maxit(10) dump(1) solve(1)
-//   omega(1) slc_all(0) slc_fine(0) dump_solution(0)
+//   omega(1) slc_all(0) slc_fine(0) dump_solution(0) mg_type(0: one space of
+//   `order` per level; 1: N_Q1 / N_P1 on every mesh + `order` on the finest)
 //   repeat(0) warmup(0) start_file (timing mode of the benchmark)
 //   tau, endtime (tcd3d) geo(Wuerfel|SixTetras) order 12 = P2 on tetrahedra
 #include <Domain.h>
@@ -315,12 +316,18 @@ static int run_cd3d()
   for (int i = 0; i < coarse_steps; i++) Domain->RegRefineAll();
 
   char Name[] = "u", Desc[] = "u";
+  // mg_type=1 (SC_MG_TYPE_SCALAR = 1, CD3D_ParMooN.C:258-313): the
+  // non-conforming N_Q1 / N_P1 space (order -1) on every geometric level,
+  // then the conforming space of `order` on the finest mesh as one more level
+  const int mg_type = (int)optd("mg_type", 0), geo_levels = levels;
+  if (mg_type) levels = geo_levels + 1;
   std::vector<Level> L(levels);
+  TCollection *coll = NULL;
   for (int i = 0; i < levels; i++)
   {
-    if (i) Domain->RegRefineAll();
-    TCollection *coll = Domain->GetCollection(It_Finest, 0);
-    L[i].space = new TFESpace3D(coll, Name, Desc, BoundCondFn, order);
+    if (i && i < geo_levels) Domain->RegRefineAll();
+    if (i < geo_levels) coll = Domain->GetCollection(It_Finest, 0);
+    L[i].space = new TFESpace3D(coll, Name, Desc, BoundCondFn, (mg_type && i < geo_levels) ? -1 : order);
     L[i].N = L[i].space->GetN_DegreesOfFreedom();
     L[i].sol = new double[L[i].N]();
     L[i].rhs = new double[L[i].N]();
@@ -454,6 +461,24 @@ static int run_cd3d()
   bool do_dump = optd("dump", 1) != 0;
   if (do_dump)
     for (int i = 0; i < levels; i++) dump_level(i, L[i]);
+  // parent of every cell of level i in level i-1's collection (the cell
+  // itself when both levels share the mesh): what Prolongate walks
+  if (do_dump)
+    for (int i = 1; i < levels; i++)
+    {
+      TCollection *cc = L[i - 1].space->GetCollection(), *fc = L[i].space->GetCollection();
+      int ncc = cc->GetN_Cells(), nfc = fc->GetN_Cells();
+      for (int c = 0; c < ncc; c++) cc->GetCell(c)->SetClipBoard(c);
+      std::vector<int> par(nfc);
+      for (int c = 0; c < nfc; c++)
+      {
+        TBaseCell *cell = fc->GetCell(c);
+        par[c] = cc == fc ? c : cell->GetParent()->GetClipBoard();
+      }
+      char k[64];
+      snprintf(k, sizeof k, "L%d_parent", i);
+      dump(k, par.data(), nfc, "i4");
+    }
   for (int i = 0; i < levels; i++)
   {
     char k[64];

@@ -23,6 +23,9 @@ ERR = {-1: "ARG", -2: "CUDA", -3: "STATE", -4: "NOT_CONVERGED", -5: "DIVERGED", 
 (ERR_ARG, ERR_CUDA, ERR_STATE, ERR_NOT_CONVERGED, ERR_DIVERGED, ERR_SLOT, ERR_NONFINITE, ERR_SINGULAR,
  ERR_UNSUPPORTED) = range(-1, -10, -1)
 Q1_HEX, Q2_HEX, P1_TET, P2_TET = 1, 2, 11, 12
+NQ1_HEX = 3  # non-conforming N_Q1 (levels of SC_MG_TYPE_SCALAR = 1)
+NLOC = {Q1_HEX: 8, Q2_HEX: 27, NQ1_HEX: 6, P1_TET: 4, P2_TET: 10}
+HEX_ELEMS = (Q1_HEX, Q2_HEX, NQ1_HEX)
 FORM_GALERKIN, FORM_SUPG, FORM_MASS, FORM_MASS_SUPG, FORM_STIFF_SUPG = 1, 2, 3, 4, 5
 COEF_CONST, COEF_SINE_RHS, COEF_LOGNORMAL, COEF_CURL_FOURIER, COEF_ROTATING, COEF_AMC, COEF_TABLE = range(7)
 SMOOTHER_JACOBI, SMOOTHER_SOR, SMOOTHER_SSOR, SMOOTHER_LEARNED = 1, 2, 3, 30
@@ -156,7 +159,7 @@ class Handle:
 
     def set_level_mesh(self, level, elem_type, elem_dof, cell_vert, brick=False):
         elem_dof, cell_vert = _c_i32(elem_dof), _c_f64(cell_vert)
-        nloc = {Q1_HEX: 8, Q2_HEX: 27, P1_TET: 4, P2_TET: 10}[elem_type]
+        nloc = NLOC[elem_type]
         n_cells = elem_dof.size // nloc
         if cell_vert.size != n_cells * 24:
             raise ValueError("cell_vert must hold 8 vertex slots x 3 coordinates per cell")
@@ -408,9 +411,10 @@ def struct_level(elem, n, jitter=0.0, seed=0):
     _check(lib().pmg_struct_csr(_i(nc.value), _i(nl.value), _ptr(ed), N, ab, _ptr(rp), None))
     kc = np.empty(int(rp[-1]), dtype=np.int32)
     _check(lib().pmg_struct_csr(_i(nc.value), _i(nl.value), _ptr(ed), N, ab, _ptr(rp), _ptr(kc)))
-    colors = np.empty(N.value, dtype=np.int32)
-    ncol = _i()
-    _check(lib().pmg_struct_row_colors(_i(elem), _i(n), N, _ptr(lat), _ptr(colors), ctypes.byref(ncol)))
+    colors, ncol = None, _i(0)
+    if elem != NQ1_HEX:  # N_Q1 has no node lattice: the library colours its rows greedily
+        colors = np.empty(N.value, dtype=np.int32)
+        _check(lib().pmg_struct_row_colors(_i(elem), _i(n), N, _ptr(lat), _ptr(colors), ctypes.byref(ncol)))
     return dict(elem=elem, n=n, elem_dof=ed, cell_vert=cv, dof_xyz=xyz.reshape(-1, 3), dof_lat=lat, N=N.value,
                 active_bound=ab.value, n_cells=nc.value, rowptr=rp, kcol=kc, colors=colors, n_colors=ncol.value)
 
@@ -444,7 +448,7 @@ def nested_prolongation(elem, c_elem_dof, c_cell_vert, n_coarse, f_dof_xyz, f_do
     ed, cv = _c_i32(c_elem_dof), _c_f64(c_cell_vert)
     xyz, fc = _c_f64(f_dof_xyz), _c_i32(f_dof_cell)
     nf = fc.size
-    nloc = {Q1_HEX: 8, Q2_HEX: 27, P1_TET: 4, P2_TET: 10}[elem]
+    nloc = NLOC[elem]
     ncc = ed.size // nloc
     rp = np.empty(nf + 1, dtype=np.int32)
     args = (_i(elem), _i(ncc), _ptr(ed), _ptr(cv), _i(n_coarse), _i(nf), _ptr(xyz), _ptr(fc))
@@ -453,6 +457,52 @@ def nested_prolongation(elem, c_elem_dof, c_cell_vert, n_coarse, f_dof_xyz, f_do
     val = np.empty(int(rp[-1]), dtype=np.float64)
     _check(lib().pmg_nested_prolongation(*args, _ptr(rp), _ptr(col), _ptr(val)))
     return rp, col, val
+
+
+def cell_prolongation(c_elem, c_elem_dof, c_cell_vert, n_coarse, f_elem, f_elem_dof, f_cell_vert, f_parent, n_fine):
+    """Prolongate's operator for any pair of spaces on nested meshes (cell averaging,
+    pmg_cell_prolongation): CSR (rp, col, val) of n_fine x n_coarse."""
+    ced, ccv = _c_i32(c_elem_dof), _c_f64(c_cell_vert)
+    fed, fcv, par = _c_i32(f_elem_dof), _c_f64(f_cell_vert), _c_i32(f_parent)
+    args = (_i(c_elem), _i(ced.size // NLOC[c_elem]), _ptr(ced), _ptr(ccv), _i(n_coarse), _i(f_elem),
+            _i(fed.size // NLOC[f_elem]), _ptr(fed), _ptr(fcv), _ptr(par), _i(n_fine))
+    rp = np.empty(n_fine + 1, dtype=np.int32)
+    _check(lib().pmg_cell_prolongation(*args, _ptr(rp), None, None))
+    col = np.empty(int(rp[-1]), dtype=np.int32)
+    val = np.empty(int(rp[-1]), dtype=np.float64)
+    _check(lib().pmg_cell_prolongation(*args, _ptr(rp), _ptr(col), _ptr(val)))
+    return rp, col, val
+
+
+def struct_parents(n):
+    """Parent (in the (n/2)^3 mesh) of every cell of the structured n^3 hexahedral mesh."""
+    i = np.arange(n ** 3)
+    x, y, z = i % n, (i // n) % n, i // (n * n)
+    m = n // 2
+    return (x // 2 + m * (y // 2 + m * (z // 2))).astype(np.int32)
+
+
+def mdml_hierarchy(elem, n_fine, n_geo):
+    """The SC_MG_TYPE_SCALAR = 1 hierarchy of the unit cube (CD3D_ParMooN.C:258-313):
+    N_Q1 on each of the n_geo meshes (n_fine >> (n_geo-1) .. n_fine cells per
+    direction), then `elem` (Q1 or Q2) on the finest mesh as one more level.
+    Transfers by cell averaging (Prolongate): N_Q1 -> N_Q1 between meshes, N_Q1 ->
+    elem on the finest mesh."""
+    levels = []
+    for g in range(n_geo):
+        n = n_fine >> (n_geo - 1 - g)
+        L = struct_level(NQ1_HEX, n)
+        if g > 0:
+            C = levels[-1]
+            L["P"] = cell_prolongation(NQ1_HEX, C["elem_dof"], C["cell_vert"], C["N"], NQ1_HEX, L["elem_dof"],
+                                       L["cell_vert"], struct_parents(n), L["N"])
+        levels.append(L)
+    F = struct_level(elem, n_fine)
+    C = levels[-1]
+    F["P"] = cell_prolongation(NQ1_HEX, C["elem_dof"], C["cell_vert"], C["N"], elem, F["elem_dof"], F["cell_vert"],
+                               np.arange(n_fine ** 3, dtype=np.int32), F["N"])
+    levels.append(F)
+    return levels
 
 
 def struct_hierarchy(elem, n_fine, n_levels, jitter=0.0, seed=0):
@@ -473,8 +523,8 @@ def load_hierarchy(handle, levels, dirichlet=None, lattice_colors=True):
     dirichlet: function (x, y, z) -> values on the Dirichlet dofs (default 0)."""
     for l, L in enumerate(levels):
         handle.set_level_csr(l, L["rowptr"], L["kcol"], L["active_bound"])
-        handle.set_level_mesh(l, L["elem"], L["elem_dof"], L["cell_vert"], brick=L["elem"] in (Q1_HEX, Q2_HEX))
-        if lattice_colors:
+        handle.set_level_mesh(l, L["elem"], L["elem_dof"], L["cell_vert"], brick=L["elem"] in HEX_ELEMS)
+        if lattice_colors and L.get("colors") is not None:
             handle.set_row_colors(l, L["colors"], L["n_colors"])
         if l > 0:
             rp, col, val = L["P"]

@@ -187,6 +187,7 @@ __device__ double hk_convection(bool hex, bool brick, const double *cv, const do
 template <int E> struct ET;
 template <> struct ET<PMG_ELEM_Q1_HEX> { static constexpr int NLOC = 8, NV = 8; static constexpr bool HEX = true; };
 template <> struct ET<PMG_ELEM_Q2_HEX> { static constexpr int NLOC = 27, NV = 8; static constexpr bool HEX = true; };
+template <> struct ET<PMG_ELEM_NQ1_HEX> { static constexpr int NLOC = 6, NV = 8; static constexpr bool HEX = true; };
 template <> struct ET<PMG_ELEM_P1_TET> { static constexpr int NLOC = 4, NV = 4; static constexpr bool HEX = false; };
 template <> struct ET<PMG_ELEM_P2_TET> { static constexpr int NLOC = 10, NV = 4; static constexpr bool HEX = false; };
 
@@ -917,7 +918,7 @@ static std::vector<double> tc_fragments(int nn, int kd, const std::function<doub
       }
   return f;
 }
-static TableCache g_tab[4];
+static TableCache g_tab[5];
 
 // quadrature rule of the reference (TFEDatabase3D::GetOrig, FEDatabase3D.C:1203-1309):
 // degree N_terms * polynomial degree with N_terms = 2 (INTERNAL_PROBLEM_LINEAR) or 3
@@ -928,14 +929,16 @@ static int rule_for(int elem, int problem_linear, int quad_rule = PMG_QUAD_AUTO)
   }
   switch (elem) {
     case PMG_ELEM_Q1_HEX: return problem_linear ? RULE_GAUSS2 : RULE_GAUSS3;
-    case PMG_ELEM_Q2_HEX: return problem_linear ? RULE_GAUSS3 : RULE_GAUSS4;
+    case PMG_ELEM_Q2_HEX:
+    case PMG_ELEM_NQ1_HEX: return problem_linear ? RULE_GAUSS3 : RULE_GAUSS4;
     case PMG_ELEM_P1_TET: return problem_linear ? RULE_KEAST4 : RULE_KEAST11;
     default: return problem_linear ? RULE_KEAST11 : -1;  // P5Tetra (degree 6) is not built
   }
 }
 
 static int get_tables(int elem, int rule, TableCache *&out) {
-  int slot = elem == PMG_ELEM_Q1_HEX ? 0 : elem == PMG_ELEM_Q2_HEX ? 1 : elem == PMG_ELEM_P1_TET ? 2 : 3;
+  int slot = elem == PMG_ELEM_Q1_HEX ? 0 : elem == PMG_ELEM_Q2_HEX ? 1 : elem == PMG_ELEM_P1_TET ? 2
+           : elem == PMG_ELEM_P2_TET ? 3 : 4;
   TableCache &T = g_tab[slot];
   if (T.elem != elem || T.rule != rule) {
     QuadRule q = make_rule(rule);
@@ -1198,6 +1201,9 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
       case PMG_ELEM_Q1_HEX * 1000 + 27: return launch_assemble_tc16<PMG_ELEM_Q1_HEX, 27>(h, L, a, tf, T->rtab.p);
       case PMG_ELEM_Q2_HEX * 1000 + 27: return launch_assemble_tc16<PMG_ELEM_Q2_HEX, 27>(h, L, a, tf, T->rtab.p);
       case PMG_ELEM_Q2_HEX * 1000 + 64: return launch_assemble_tc16<PMG_ELEM_Q2_HEX, 64>(h, L, a, tf, T->rtab.p);
+      case PMG_ELEM_NQ1_HEX * 1000 + 8: return launch_assemble_tc16<PMG_ELEM_NQ1_HEX, 8>(h, L, a, tf, T->rtab.p);
+      case PMG_ELEM_NQ1_HEX * 1000 + 27: return launch_assemble_tc16<PMG_ELEM_NQ1_HEX, 27>(h, L, a, tf, T->rtab.p);
+      case PMG_ELEM_NQ1_HEX * 1000 + 64: return launch_assemble_tc16<PMG_ELEM_NQ1_HEX, 64>(h, L, a, tf, T->rtab.p);
       case PMG_ELEM_P1_TET * 1000 + 4: return launch_assemble_tc16<PMG_ELEM_P1_TET, 4>(h, L, a, tf, T->rtab.p);
       case PMG_ELEM_P1_TET * 1000 + 5: return launch_assemble_tc16<PMG_ELEM_P1_TET, 5>(h, L, a, tf, T->rtab.p);
       case PMG_ELEM_P1_TET * 1000 + 11: return launch_assemble_tc16<PMG_ELEM_P1_TET, 11>(h, L, a, tf, T->rtab.p);
@@ -1229,6 +1235,9 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
       case PMG_ELEM_Q1_HEX * 1000 + 27: return launch_assemble_cc<PMG_ELEM_Q1_HEX, 27>(h, L, a, st);
       case PMG_ELEM_Q2_HEX * 1000 + 27: return launch_assemble_cc<PMG_ELEM_Q2_HEX, 27>(h, L, a, st);
       case PMG_ELEM_Q2_HEX * 1000 + 64: return launch_assemble_cc<PMG_ELEM_Q2_HEX, 64>(h, L, a, st);
+      case PMG_ELEM_NQ1_HEX * 1000 + 8: return launch_assemble_cc<PMG_ELEM_NQ1_HEX, 8>(h, L, a, st);
+      case PMG_ELEM_NQ1_HEX * 1000 + 27: return launch_assemble_cc<PMG_ELEM_NQ1_HEX, 27>(h, L, a, st);
+      case PMG_ELEM_NQ1_HEX * 1000 + 64: return launch_assemble_cc<PMG_ELEM_NQ1_HEX, 64>(h, L, a, st);
       case PMG_ELEM_P1_TET * 1000 + 4: return launch_assemble_cc<PMG_ELEM_P1_TET, 4>(h, L, a, st);
       case PMG_ELEM_P1_TET * 1000 + 11: return launch_assemble_cc<PMG_ELEM_P1_TET, 11>(h, L, a, st);
       case PMG_ELEM_P2_TET * 1000 + 11: return launch_assemble_cc<PMG_ELEM_P2_TET, 11>(h, L, a, st);
@@ -1240,6 +1249,9 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
     case PMG_ELEM_Q1_HEX * 1000 + 27: PMG_TRY((launch_assemble<PMG_ELEM_Q1_HEX, 27>(h, L, a))); break;
     case PMG_ELEM_Q2_HEX * 1000 + 27: PMG_TRY((launch_assemble<PMG_ELEM_Q2_HEX, 27>(h, L, a))); break;
     case PMG_ELEM_Q2_HEX * 1000 + 64: PMG_TRY((launch_assemble<PMG_ELEM_Q2_HEX, 64>(h, L, a))); break;
+    case PMG_ELEM_NQ1_HEX * 1000 + 8: PMG_TRY((launch_assemble<PMG_ELEM_NQ1_HEX, 8>(h, L, a))); break;
+    case PMG_ELEM_NQ1_HEX * 1000 + 27: PMG_TRY((launch_assemble<PMG_ELEM_NQ1_HEX, 27>(h, L, a))); break;
+    case PMG_ELEM_NQ1_HEX * 1000 + 64: PMG_TRY((launch_assemble<PMG_ELEM_NQ1_HEX, 64>(h, L, a))); break;
     case PMG_ELEM_P1_TET * 1000 + 4: PMG_TRY((launch_assemble<PMG_ELEM_P1_TET, 4>(h, L, a))); break;
     case PMG_ELEM_P1_TET * 1000 + 5: PMG_TRY((launch_assemble<PMG_ELEM_P1_TET, 5>(h, L, a))); break;
     case PMG_ELEM_P1_TET * 1000 + 11: PMG_TRY((launch_assemble<PMG_ELEM_P1_TET, 11>(h, L, a))); break;

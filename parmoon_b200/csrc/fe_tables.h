@@ -60,13 +60,39 @@ inline QuadRule make_rule(int rule) {
   return q;
 }
 
-inline int elem_nloc(int e) { return e == PMG_ELEM_Q1_HEX ? 8 : e == PMG_ELEM_Q2_HEX ? 27 : e == PMG_ELEM_P1_TET ? 4 : 10; }
-inline bool elem_is_hex(int e) { return e == PMG_ELEM_Q1_HEX || e == PMG_ELEM_Q2_HEX; }
-inline int elem_degree(int e) { return (e == PMG_ELEM_Q2_HEX || e == PMG_ELEM_P2_TET) ? 2 : 1; }
+inline int elem_nloc(int e) {
+  return e == PMG_ELEM_Q1_HEX ? 8 : e == PMG_ELEM_Q2_HEX ? 27 : e == PMG_ELEM_NQ1_HEX ? 6 : e == PMG_ELEM_P1_TET ? 4 : 10;
+}
+inline bool elem_is_hex(int e) { return e == PMG_ELEM_Q1_HEX || e == PMG_ELEM_Q2_HEX || e == PMG_ELEM_NQ1_HEX; }
+// polynomial degree the quadrature rule is chosen from (GetOrig: N_terms x degree);
+// N_Q1's basis holds xi^2 terms, so its rules are Q2's
+inline int elem_degree(int e) { return (e == PMG_ELEM_Q2_HEX || e == PMG_ELEM_P2_TET || e == PMG_ELEM_NQ1_HEX) ? 2 : 1; }
+
+// N_Q1 on [-1,1]^3: local dof f sits at the midpoint of face f, faces in the
+// order zeta = -1, eta = -1, xi = +1, eta = +1, xi = -1, zeta = +1
+// (NF_N_H_Q1_3D.h).  phi_f = 1/6 + s_f t_f / 2 + (t_f^2 - (u^2 + v^2) / 2) / 3
+// with t_f the coordinate normal to face f, s_f = +-1 its side and u, v the
+// other two coordinates: 1 at its own face midpoint, 0 at the other five.
+constexpr int NQ1_AXIS[6] = {2, 1, 0, 1, 0, 2};
+constexpr double NQ1_SIDE[6] = {-1, -1, 1, 1, -1, 1};
 
 // value and reference gradient of every local basis function at (x,y,z):
 // out[l*4 + 0..2] = d/dxi, d/deta, d/dzeta ; out[l*4 + 3] = value
 inline void basis_eval(int e, double x, double y, double z, double *out) {
+  if (e == PMG_ELEM_NQ1_HEX) {
+    const double c[3] = {x, y, z};
+    for (int f = 0; f < 6; f++) {
+      const int a = NQ1_AXIS[f];
+      const double s = NQ1_SIDE[f], t = c[a];
+      double others = 0.0;
+      for (int d = 0; d < 3; d++)
+        if (d != a) others += c[d] * c[d];
+      out[f * 4 + 3] = 1.0 / 6.0 + 0.5 * s * t + (t * t - 0.5 * others) / 3.0;
+      for (int d = 0; d < 3; d++)
+        out[f * 4 + d] = d == a ? 0.5 * s + 2.0 * t / 3.0 : -c[d] / 3.0;
+    }
+    return;
+  }
   if (elem_is_hex(e)) {
     int p = elem_degree(e), n = p + 1;
     auto lag = [p](double s, double *v, double *d) {

@@ -14,10 +14,64 @@
 namespace {
 
 int degree_of(int e) { return (e == PMG_ELEM_Q2_HEX || e == PMG_ELEM_P2_TET) ? 2 : 1; }
-bool is_hex(int e) { return e == PMG_ELEM_Q1_HEX || e == PMG_ELEM_Q2_HEX; }
+bool is_hex(int e) { return e == PMG_ELEM_Q1_HEX || e == PMG_ELEM_Q2_HEX || e == PMG_ELEM_NQ1_HEX; }
 int nloc_of(int e) { return pmg::elem_nloc(e); }
 bool valid_elem(int e) {
-  return e == PMG_ELEM_Q1_HEX || e == PMG_ELEM_Q2_HEX || e == PMG_ELEM_P1_TET || e == PMG_ELEM_P2_TET;
+  return e == PMG_ELEM_Q1_HEX || e == PMG_ELEM_Q2_HEX || e == PMG_ELEM_NQ1_HEX || e == PMG_ELEM_P1_TET ||
+         e == PMG_ELEM_P2_TET;
+}
+
+// N_Q1 on the n^3 cube: one dof per face.  Faces normal to x are (i, j+1/2,
+// k+1/2) with i = 0..n (id i + (n+1)(j + n k)), then the y faces
+// (i+1/2, j, k+1/2) and the z faces (i+1/2, j+1/2, k) in the same pattern;
+// interior faces are numbered first (in id order), the boundary faces after.
+// Cell (i, j, k) takes its faces in N_Q1's local order: z = k (zeta = -1),
+// y = j, x = i+1, y = j+1, x = i, z = k+1.
+int build_nq1(int n, int *elem_dof, double *cell_vert, double *dof_xyz, int *face_id, int *active_bound) {
+  const long nf1 = (long)(n + 1) * n * n, N = 3 * nf1;
+  auto fx = [&](int i, int j, int k) { return (long)i + (n + 1) * ((long)j + (long)n * k); };
+  auto fy = [&](int i, int j, int k) { return nf1 + i + (long)n * ((long)j + (long)(n + 1) * k); };
+  auto fz = [&](int i, int j, int k) { return 2 * nf1 + i + (long)n * ((long)j + (long)n * k); };
+  auto boundary = [&](long f) {
+    const int dir = (int)(f / nf1);
+    const long r = f % nf1;
+    // the coordinate along the face normal runs 0..n
+    const long t = dir == 0 ? r % (n + 1) : dir == 1 ? (r / n) % (n + 1) : r / ((long)n * n);
+    return t == 0 || t == n;
+  };
+  std::vector<int> num(N);
+  int a = 0;
+  for (long f = 0; f < N; f++)
+    if (!boundary(f)) num[f] = a++;
+  *active_bound = a;
+  int b = a;
+  for (long f = 0; f < N; f++)
+    if (boundary(f)) num[f] = b++;
+  const double h = 1.0 / n;
+  for (long f = 0; f < N; f++) {
+    const int dir = (int)(f / nf1);
+    const long r = f % nf1;
+    double x, y, z;
+    if (dir == 0) { x = (r % (n + 1)) * h; y = ((r / (n + 1)) % n + 0.5) * h; z = (r / ((long)(n + 1) * n) + 0.5) * h; }
+    else if (dir == 1) { x = (r % n + 0.5) * h; y = ((r / n) % (n + 1)) * h; z = (r / ((long)n * (n + 1)) + 0.5) * h; }
+    else { x = (r % n + 0.5) * h; y = ((r / n) % n + 0.5) * h; z = (r / ((long)n * n)) * h; }
+    const int d = num[f];
+    face_id[d] = (int)f;
+    dof_xyz[3 * (size_t)d] = x; dof_xyz[3 * (size_t)d + 1] = y; dof_xyz[3 * (size_t)d + 2] = z;
+  }
+  static const int hoff[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+  size_t c = 0;
+  for (int k = 0; k < n; k++)
+    for (int j = 0; j < n; j++)
+      for (int i = 0; i < n; i++, c++) {
+        double *cv = cell_vert + c * 24;
+        for (int v = 0; v < 8; v++) {
+          cv[3 * v] = (i + hoff[v][0]) * h; cv[3 * v + 1] = (j + hoff[v][1]) * h; cv[3 * v + 2] = (k + hoff[v][2]) * h;
+        }
+        const long f[6] = {fz(i, j, k), fy(i, j, k), fx(i + 1, j, k), fy(i, j + 1, k), fx(i, j, k), fz(i, j, k + 1)};
+        for (int l = 0; l < 6; l++) elem_dof[c * 6 + l] = num[f[l]];
+      }
+  return PMG_OK;
 }
 
 // reference coordinates of the local nodes, in units of the element's lattice
@@ -64,6 +118,12 @@ extern "C" {
 
 int pmg_struct_sizes(int e, int n, int *n_cells, int *n_dofs, int *nloc) {
   if (!valid_elem(e) || n < 1 || !n_cells || !n_dofs || !nloc) return PMG_ERR_ARG;
+  if (e == PMG_ELEM_NQ1_HEX) {
+    *n_cells = n * n * n;
+    *n_dofs = 3 * n * n * (n + 1);
+    *nloc = 6;
+    return PMG_OK;
+  }
   long n1 = (long)degree_of(e) * n + 1;
   *n_cells = is_hex(e) ? n * n * n : 6 * n * n * n;
   *n_dofs = (int)(n1 * n1 * n1);
@@ -74,6 +134,10 @@ int pmg_struct_sizes(int e, int n, int *n_cells, int *n_dofs, int *nloc) {
 int pmg_struct_build(int e, int n, double jitter, unsigned long long seed, int *elem_dof, double *cell_vert,
                      double *dof_xyz, int *dof_lat, int *active_bound) {
   if (!valid_elem(e) || n < 1 || !elem_dof || !cell_vert || !dof_xyz || !dof_lat || !active_bound) return PMG_ERR_ARG;
+  if (e == PMG_ELEM_NQ1_HEX) {
+    if (jitter != 0.0) return PMG_ERR_UNSUPPORTED;  // affine bricks only
+    return build_nq1(n, elem_dof, cell_vert, dof_xyz, dof_lat, active_bound);
+  }
   const int p = degree_of(e), n1 = p * n + 1, nv1 = n + 1;
   const long N = (long)n1 * n1 * n1;
   std::vector<int> num(N);
@@ -224,6 +288,7 @@ int pmg_struct_csr(int n_cells, int nloc, const int *ed, int N, int Na, int *rp,
 int pmg_struct_prolongation(int e, int nc, const int *lat_c, int Nc, const int *lat_f, int Nf, int *prp, int *pcol,
                             double *pval) {
   if (!valid_elem(e) || nc < 1 || !lat_c || !lat_f || !prp) return PMG_ERR_ARG;
+  if (e == PMG_ELEM_NQ1_HEX) return PMG_ERR_UNSUPPORTED;  // no node lattice: pmg_cell_prolongation
   const int p = degree_of(e), n1c = p * nc + 1, n1f = 2 * p * nc + 1;
   std::vector<int> inv((size_t)n1c * n1c * n1c, -1);
   for (int d = 0; d < Nc; d++) inv[lat_c[d]] = d;
@@ -364,8 +429,106 @@ int pmg_nested_prolongation(int e, int n_coarse_cells, const int *c_elem_dof, co
   return PMG_OK;
 }
 
+int pmg_cell_prolongation(int ce, int n_coarse_cells, const int *c_elem_dof, const double *c_cell_vert, int Nc,
+                          int fe, int n_fine_cells, const int *f_elem_dof, const double *f_cell_vert,
+                          const int *f_parent, int Nf, int *prp, int *pcol, double *pval) {
+  if (!valid_elem(ce) || !valid_elem(fe) || is_hex(ce) != is_hex(fe) || n_coarse_cells < 1 || n_fine_cells < 1 ||
+      !c_elem_dof || !c_cell_vert || !f_elem_dof || !f_cell_vert || !f_parent || Nc < 1 || Nf < 1 || !prp)
+    return PMG_ERR_ARG;
+  const bool hex = is_hex(ce);
+  const int nlc = nloc_of(ce), nlf = nloc_of(fe);
+  // the fine element's nodal points on its reference cell
+  std::vector<double> fnode((size_t)nlf * 3);
+  for (int k = 0; k < nlf; k++) {
+    double *q = &fnode[(size_t)k * 3];
+    if (fe == PMG_ELEM_NQ1_HEX) {
+      q[0] = q[1] = q[2] = 0.0;
+      q[pmg::NQ1_AXIS[k]] = pmg::NQ1_SIDE[k];
+    } else {
+      int r[3];
+      local_node(fe, k, r);
+      const int p = degree_of(fe);
+      for (int d = 0; d < 3; d++) q[d] = hex ? -1.0 + 2.0 * r[d] / p : (double)r[d] / p;
+    }
+  }
+  // affine map of a cell (8 vertex slots) and its inverse
+  auto map_of = [&](const double *v, double *J, double *x0) {
+    for (int d = 0; d < 3; d++) {
+      if (hex) {
+        J[d * 3 + 0] = (v[3 + d] - v[d]) * 0.5;
+        J[d * 3 + 1] = (v[9 + d] - v[d]) * 0.5;
+        J[d * 3 + 2] = (v[12 + d] - v[d]) * 0.5;
+        x0[d] = (v[3 + d] + v[9 + d] + v[12 + d] - v[d]) * 0.5;
+      } else {
+        J[d * 3 + 0] = v[3 + d] - v[d];
+        J[d * 3 + 1] = v[6 + d] - v[d];
+        J[d * 3 + 2] = v[9 + d] - v[d];
+        x0[d] = v[d];
+      }
+    }
+  };
+  std::vector<std::vector<std::pair<int, double>>> rows(Nf);
+  std::vector<int> count(Nf, 0);
+  double tab[27 * 4];
+  for (int K = 0; K < n_fine_cells; K++) {
+    const int c = f_parent[K];
+    if (c < 0 || c >= n_coarse_cells) return PMG_ERR_ARG;
+    double Jf[9], xf[3], Jc[9], xc[3], Ji[9];
+    map_of(f_cell_vert + (size_t)K * 24, Jf, xf);
+    map_of(c_cell_vert + (size_t)c * 24, Jc, xc);
+    const double det = Jc[0] * (Jc[4] * Jc[8] - Jc[5] * Jc[7]) - Jc[1] * (Jc[3] * Jc[8] - Jc[5] * Jc[6]) +
+                       Jc[2] * (Jc[3] * Jc[7] - Jc[4] * Jc[6]);
+    if (!(std::fabs(det) > 0)) return PMG_ERR_ARG;
+    Ji[0] = (Jc[4] * Jc[8] - Jc[5] * Jc[7]) / det; Ji[1] = (Jc[2] * Jc[7] - Jc[1] * Jc[8]) / det;
+    Ji[2] = (Jc[1] * Jc[5] - Jc[2] * Jc[4]) / det; Ji[3] = (Jc[5] * Jc[6] - Jc[3] * Jc[8]) / det;
+    Ji[4] = (Jc[0] * Jc[8] - Jc[2] * Jc[6]) / det; Ji[5] = (Jc[2] * Jc[3] - Jc[0] * Jc[5]) / det;
+    Ji[6] = (Jc[3] * Jc[7] - Jc[4] * Jc[6]) / det; Ji[7] = (Jc[1] * Jc[6] - Jc[0] * Jc[7]) / det;
+    Ji[8] = (Jc[0] * Jc[4] - Jc[1] * Jc[3]) / det;
+    for (int k = 0; k < nlf; k++) {
+      const int d = f_elem_dof[(size_t)K * nlf + k];
+      if (d < 0 || d >= Nf) return PMG_ERR_ARG;
+      const double *q = &fnode[(size_t)k * 3];
+      double x[3], ref[3];
+      for (int t = 0; t < 3; t++) x[t] = xf[t] + Jf[t * 3] * q[0] + Jf[t * 3 + 1] * q[1] + Jf[t * 3 + 2] * q[2] - xc[t];
+      for (int t = 0; t < 3; t++) ref[t] = Ji[t * 3] * x[0] + Ji[t * 3 + 1] * x[1] + Ji[t * 3 + 2] * x[2];
+      pmg::basis_eval(ce, ref[0], ref[1], ref[2], tab);
+      count[d]++;
+      for (int l = 0; l < nlc; l++) {
+        const double w = tab[l * 4 + 3];
+        if (std::fabs(w) < 1e-12) continue;
+        const int col = c_elem_dof[(size_t)c * nlc + l];
+        if (col < 0 || col >= Nc) return PMG_ERR_ARG;
+        rows[d].push_back({col, w});
+      }
+    }
+  }
+  prp[0] = 0;
+  for (int r = 0; r < Nf; r++) {
+    auto &v = rows[r];
+    std::sort(v.begin(), v.end(), [](const std::pair<int, double> &a, const std::pair<int, double> &b) {
+      return a.first < b.first;
+    });
+    int m = 0;
+    for (size_t t = 0; t < v.size();) {
+      const int col = v[t].first;
+      double sum = 0.0;
+      for (; t < v.size() && v[t].first == col; t++) sum += v[t].second;
+      sum /= count[r] > 0 ? count[r] : 1;
+      if (std::fabs(sum) <= 1e-15) continue;
+      if (pcol) {
+        pcol[prp[r] + m] = col;
+        pval[prp[r] + m] = sum;
+      }
+      m++;
+    }
+    prp[r + 1] = prp[r] + m;
+  }
+  return PMG_OK;
+}
+
 int pmg_struct_row_colors(int e, int n, int N, const int *lat, int *colors, int *n_colors) {
   if (!valid_elem(e) || !lat || !colors || !n_colors) return PMG_ERR_ARG;
+  if (e == PMG_ELEM_NQ1_HEX) return PMG_ERR_UNSUPPORTED;  // no node lattice: greedy row colours
   const int p = degree_of(e), n1 = p * n + 1, m = p + 1;
   for (int d = 0; d < N; d++) {
     int L = lat[d], i = L % n1, j = (L / n1) % n1, k = L / (n1 * n1);

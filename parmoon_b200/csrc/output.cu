@@ -69,6 +69,10 @@ extern "C" int pmg_write_vtk(pmg_handle hh, int level, const double *values, con
     set_error("pmg_write_vtk: the level has no mesh (pmg_set_level_mesh)");
     return PMG_ERR_STATE;
   }
+  if (L.elem == PMG_ELEM_NQ1_HEX) {
+    set_error("pmg_write_vtk: N_Q1 has no nodes at the cell corners (write the conforming level)");
+    return PMG_ERR_UNSUPPORTED;
+  }
   const double *u = nullptr;
   DBuf<double> du;
   if (values) {

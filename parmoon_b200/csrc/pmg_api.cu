@@ -263,8 +263,8 @@ int pmg_set_level_mesh(pmg_handle hh, int level, int elem_type, int n_cells, con
   Handle *h = H(hh);
   PMG_TRY(check_level(h, level));
   Level &L = h->lv[level];
-  if (elem_type != PMG_ELEM_Q1_HEX && elem_type != PMG_ELEM_Q2_HEX && elem_type != PMG_ELEM_P1_TET &&
-      elem_type != PMG_ELEM_P2_TET) {
+  if (elem_type != PMG_ELEM_Q1_HEX && elem_type != PMG_ELEM_Q2_HEX && elem_type != PMG_ELEM_NQ1_HEX &&
+      elem_type != PMG_ELEM_P1_TET && elem_type != PMG_ELEM_P2_TET) {
     set_error("pmg_set_level_mesh: unknown element type");
     return PMG_ERR_ARG;
   }
@@ -744,7 +744,8 @@ int pmg_time_kernel(pmg_handle hh, int kernel, int level, int form, int reps, do
     // coloured scatter per element: n_loc^2 (4 slot + 8 read + 8 write) + n_loc (4 dof + 16 rhs) + vertices
     const double nl = L.nloc, nv = L.nvert;
     by = L.n_cells * (nl * nl * 20 + nl * 20 + nv * 4 + nv * 24);
-    const double nq = L.elem == PMG_ELEM_Q1_HEX ? 8 : L.elem == PMG_ELEM_Q2_HEX ? 27 : L.elem == PMG_ELEM_P1_TET ? 4 : 11;
+    const double nq = L.elem == PMG_ELEM_Q1_HEX ? 8 : (L.elem == PMG_ELEM_Q2_HEX || L.elem == PMG_ELEM_NQ1_HEX) ? 27
+                    : L.elem == PMG_ELEM_P1_TET ? 4 : 11;
     fl = L.n_cells * (nq * nl * nl * 8 + nq * nl * 32);  // 4 FMA per (q,i,j) + D_q u_j (16 FMA per q,j)
   }
   PMG_TRY(run());  // warm-up

@@ -382,6 +382,10 @@ extern "C" int pmg_build_transfer(pmg_handle hh, int level, int n_fine, const do
     set_error("pmg_build_transfer: needs the fine level's pattern and the coarse level's pattern and mesh");
     return PMG_ERR_STATE;
   }
+  if (C.elem == PMG_ELEM_NQ1_HEX || L.elem == PMG_ELEM_NQ1_HEX) {
+    set_error("pmg_build_transfer: conforming nested spaces only (N_Q1 levels: pmg_cell_prolongation)");
+    return PMG_ERR_UNSUPPORTED;
+  }
   // the coarse cells sit on the device in colour order: caller index -> position
   std::vector<int> pos(C.n_cells), cpos(n_fine);
   for (int k = 0; k < C.n_cells; k++) pos[C.cell_order[k]] = k;

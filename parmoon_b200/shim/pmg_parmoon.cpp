@@ -81,6 +81,7 @@ void TPmgSystemCD3D::setup(BoundValueFunct3D *BoundValue) {
   dirichlet.assign(N_Levels, DirichletNodes());
   std::vector<std::vector<int>> ed_lv(N_Levels);
   std::vector<std::vector<double>> cv_lv(N_Levels);
+  std::vector<int> elem_lv(N_Levels, 0);
   for (int i = 0; i < N_Levels && status == PMG_OK; i++) {
     TFESpace3D *sp = FeSpaces[i];
     TCollection *coll = sp->GetCollection();
@@ -92,8 +93,11 @@ void TPmgSystemCD3D::setup(BoundValueFunct3D *BoundValue) {
     int *gn = sp->GetGlobalNumbers(), *bi = sp->GetBeginIndex();
     const int nloc = bi[1] - bi[0];
     const int nv = coll->GetCell(0)->GetN_Vertices();
-    const int elem = nv == 8 ? (nloc == 8 ? PMG_ELEM_Q1_HEX : PMG_ELEM_Q2_HEX)
+    // Q1 / Q2 / N_Q1 (the non-conforming levels of SC_MG_TYPE_SCALAR = 1) on
+    // hexahedra, P1 / P2 on tetrahedra
+    const int elem = nv == 8 ? (nloc == 8 ? PMG_ELEM_Q1_HEX : nloc == 6 ? PMG_ELEM_NQ1_HEX : PMG_ELEM_Q2_HEX)
                              : (nloc == 4 ? PMG_ELEM_P1_TET : PMG_ELEM_P2_TET);
+    elem_lv[i] = elem;
     std::vector<int> &ed = ed_lv[i];
     std::vector<double> &cv = cv_lv[i];
     ed.resize((size_t)nc * nloc);
@@ -155,18 +159,36 @@ void TPmgSystemCD3D::setup(BoundValueFunct3D *BoundValue) {
       saved[c] = ccoll->GetCell(c)->GetClipBoard();
       ccoll->GetCell(c)->SetClipBoard(c);
     }
-    std::vector<int> owner(N, -1);
+    // the coarse cell of every fine cell: its parent, or the cell itself when
+    // both spaces live on one mesh (the conforming level above the N_Q1 levels)
+    const bool same_mesh = ccoll == coll;
+    std::vector<int> owner(N, -1), par(nc, -1);
     for (int c = 0; c < nc; c++) {
-      TBaseCell *parent = coll->GetCell(c)->GetParent();
+      TBaseCell *parent = same_mesh ? coll->GetCell(c) : coll->GetCell(c)->GetParent();
       const int pc = parent ? parent->GetClipBoard() : -1;
       if (pc < 0 || pc >= ncc || ccoll->GetCell(pc) != parent) {
         check(PMG_ERR_ARG, "levels are not nested (fine cell without a parent on the coarser level)");
         break;
       }
+      par[c] = pc;
       for (int l = 0; l < nloc; l++) owner[ed[(size_t)c * nloc + l]] = pc;
     }
     for (int c = 0; c < ncc; c++) ccoll->GetCell(c)->SetClipBoard(saved[c]);
     if (status != PMG_OK) continue;
+    if (elem_lv[i - 1] != elem || elem == PMG_ELEM_NQ1_HEX) {
+      // different spaces, or the non-conforming N_Q1: Prolongate's cell average
+      std::vector<int> prp(N + 1);
+      check(pmg_cell_prolongation(elem_lv[i - 1], ncc, ed_lv[i - 1].data(), cv_lv[i - 1].data(), Nc, elem, nc,
+                                  ed.data(), cv.data(), par.data(), N, prp.data(), nullptr, nullptr),
+            "pmg_cell_prolongation");
+      std::vector<int> pcol(prp[N]);
+      std::vector<double> pval(prp[N]);
+      check(pmg_cell_prolongation(elem_lv[i - 1], ncc, ed_lv[i - 1].data(), cv_lv[i - 1].data(), Nc, elem, nc,
+                                  ed.data(), cv.data(), par.data(), N, prp.data(), pcol.data(), pval.data()),
+            "pmg_cell_prolongation");
+      check(pmg_set_transfer(h, i, N, Nc, prp.data(), pcol.data(), pval.data()), "pmg_set_transfer");
+      continue;
+    }
     std::vector<double> xyz((size_t)3 * N);
     for (int d = 0; d < N; d++) { xyz[3 * d] = X[d]; xyz[3 * d + 1] = Y[d]; xyz[3 * d + 2] = Z[d]; }
     std::vector<int> prp(N + 1);

@@ -8,6 +8,7 @@ that binary on small cases and packs its dumps into ``<case>.npz``:
 
   L<l>_{rowptr,kcol,entries,rhs,elem_dof,cell_vert,dof_xyz}  per level
   L<l>_{N,active_bound,n_cells,n_loc}                         per level
+  L<l>_parent                                                  parent cells (l >= 1)
   T<l>_{coarse_in,fine_in,prolongated,restricted}             transfer probes
   solution, solve_iterations, res0, res_final                 FGMRES + GMG solve
   params                                                      the driver options
@@ -53,6 +54,13 @@ CASES = {
     "c1_poisson_q1_32": ("cd3d", dict(order=1, levels=4, coarse_steps=2, problem="laplace", dump=0,
                                       dump_solution=1, **TIGHT)),
     "tcd3d_amc": ("tcd3d", dict(order=1, levels=3, coarse_steps=2, endtime=0.5)),
+    # SC_MG_TYPE_SCALAR = 1: N_Q1 on the 2^3, 4^3, 8^3 meshes, then the conforming
+    # space on the 8^3 mesh (4 multigrid levels); L<l>_parent = Prolongate's parent cells
+    "mdml_q1_laplace": ("cd3d", dict(order=1, levels=3, coarse_steps=1, problem="laplace", mg_type=1, **TIGHT)),
+    "mdml_q1_supg": ("cd3d", dict(order=1, levels=3, coarse_steps=1, problem="cdsupg", eps=1e-3, b1=1, b2=0.5,
+                                  b3=0.25, mg_type=1, **TIGHT)),
+    "mdml_q2_supg": ("cd3d", dict(order=2, levels=2, coarse_steps=1, problem="cdsupg", eps=1e-6, b1=1, b2=0.5,
+                                  b3=0.25, mg_type=1, **TIGHT)),
 }
 
 

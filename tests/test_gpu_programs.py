@@ -50,22 +50,27 @@ def run_program(exe, workdir, dat):
 
 # (the unmodified CD3D main program crashes in the reference's own mesh set-up on
 # SixTetras.GEO, CPU build included, so tetrahedra are covered by test_gpu_dropin)
-@pytest.mark.parametrize("geo,order,levels,steps", [("Wuerfel", 1, 3, 2), ("Wuerfel", 2, 3, 1),
-                                                     ("Wuerfel", 1, 4, 2)])
-def test_cd3d_program_on_device_matches_reference(tmp_path, geo, order, levels, steps):
+@pytest.mark.parametrize("geo,order,levels,steps,mg_type", [("Wuerfel", 1, 3, 2, 0), ("Wuerfel", 2, 3, 1, 0),
+                                                             ("Wuerfel", 1, 4, 2, 0), ("Wuerfel", 1, 3, 2, 1),
+                                                             ("Wuerfel", 2, 3, 1, 1)])
+def test_cd3d_program_on_device_matches_reference(tmp_path, geo, order, levels, steps, mg_type):
+    """mg_type 1: SC_MG_TYPE_SCALAR = 1, N_Q1 levels under the conforming one."""
     dat = str(tmp_path / "cd3d.dat")
     write_dat(dat, geo, ANSATZ_ORDER=order, LEVELS=levels, UNIFORM_STEPS=steps, SC_LIN_RED_FACTOR_SCALAR=1e-10,
-              SC_LIN_RES_NORM_MIN_SCALAR=0)
+              SC_LIN_RES_NORM_MIN_SCALAR=0, SC_MG_TYPE_SCALAR=mg_type)
     l2r, h1r = run_program("cd3d_program_ref", str(tmp_path / "ref"), dat)
     l2p, h1p = run_program("cd3d_program_pmg", str(tmp_path / "pmg"), dat)
     assert np.allclose(l2p, l2r, rtol=2e-6, atol=0) and np.allclose(h1p, h1r, rtol=2e-6, atol=0), (l2r, l2p, h1r, h1p)
 
 
-def test_tcd3d_program_on_device_reproduces_recorded_log(tmp_path):
+@pytest.mark.parametrize("mg_type", [0, 1])
+def test_tcd3d_program_on_device_reproduces_recorded_log(tmp_path, mg_type):
+    """mg_type 1 is the multilevel type of the recorded run (SC_MG_TYPE_SCALAR = 1:
+    an N_Q1 level on every mesh under the Q1 level, tcd3d_GMG.out:388-396)."""
     dat = str(tmp_path / "tcd3d.dat")
     write_dat(dat, "Wuerfel", ANSATZ_ORDER=1, LEVELS=3, UNIFORM_STEPS=2, SC_LIN_RED_FACTOR_SCALAR=0.0,
               SC_LIN_RES_NORM_MIN_SCALAR=1e-13, TIME_DISC=2, STARTTIME=0, ENDTIME=0.5,
-              TIMESTEPLENGTH=0.1082532, STEPS_PER_IMAGE=100)
+              TIMESTEPLENGTH=0.1082532, STEPS_PER_IMAGE=100, SC_MG_TYPE_SCALAR=mg_type)
     l2r, h1r = run_program("tcd3d_program_ref", str(tmp_path / "ref"), dat)
     l2p, h1p = run_program("tcd3d_program_pmg", str(tmp_path / "pmg"), dat)
     assert l2p.size == l2r.size == 6
