@@ -544,181 +544,21 @@ __global__ void __launch_bounds__(ASMC_WARPS * 32, 2) k_assemble_cc(AsmArgs a, c
 // DIFF (pure diffusion, eps varying in space: b = 0, c = 0): k = (q, p) with p
 //   over the 6 entries of the symmetric K = Ji Ji^T, d = w_q |det J| eps(x_q) K_p,
 //   T[m][(q,p)] = u_ia u_ja (p = aa) or u_ia u_jb + u_ib u_ja (p = ab, a < b).
-// A warp takes 8 cells.  Per 8 x 8 output block (8 entries x 8 cells) the
-// mma chain runs over the k steps of 4: the A operand (8 entries x 4 k) comes
-// from T in shared memory, stored per (entry block, k step) as the 32 lane
-// values of the fragment; the B operand (4 k x 8 cells) from the warp's
-// staged d.  Lane l ends with entries m = 8t + l/4 of cells 2(l%4), 2(l%4)+1
-// and adds them into the CSR through the slot map with L2 reductions (cells
-// of one colour share no row, so no two adds of a launch meet).  Slot loads
-// of the next batch go out before the current batch's mma chains.  The sums
-// equal the per-point ones up to rounding order.
+// d is computed per cell beforehand (k_tc_setup, k_tc_setup_diff).  A warp
+// takes 8 cells.  Per 8 x 8 output block (8 entries x 8 cells) the mma chain
+// runs over the k steps of 4: the A operand (8 entries x 4 k) comes from T in
+// shared memory, stored per (entry block, k step) as the 32 lane values of the
+// fragment; the B operand (4 k x 8 cells) from the cells' d.  Lane l ends with
+// entries m = 8t + l/4 of cells 2(l%4), 2(l%4)+1 and adds them into the CSR
+// through the slot map with L2 reductions (cells of one colour share no row,
+// so no two adds of a launch meet).  Slot loads of the next batch go out
+// before the current batch's mma chains.  The sums equal the per-point ones
+// up to rounding order.
 
 __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b) {
   asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
       : "+d"(c0), "+d"(c1)
       : "d"(a), "d"(b));
-}
-
-template <int E, int NQ, bool DIFF>
-struct TcShape {
-  static constexpr int NLOC = ET<E>::NLOC, NN = NLOC * NLOC, MT = (NN + 7) / 8;
-  static constexpr int KD = DIFF ? 6 * NQ : 16, KS = (KD + 3) / 4, KP = 4 * KS;
-  static constexpr int CW = DIFF ? 23 : 17;            // per cell: J 9, x0 3, |det J|, delta, bh 3 (, K 6)
-  static constexpr int WARP_DOUBLES = KP * 8 + 8 * NQ + 8 * CW;  // d staging, rhs weights, cell data
-  static constexpr size_t TABLE_DOUBLES = (size_t)MT * KS * 32;
-};
-
-// Up to 16 warps per block (fewer when the tables leave less shared memory);
-// 8 entry blocks per batch (slot loads in flight per lane: 2 x TC_MB).  A
-// 1024-thread variant (64 registers, 4 blocks per batch) spilled and was
-// measured slower on the P2 lognormal 64^3 level (7.24 against 6.77 ms).
-template <int E, int NQ, bool DIFF>
-__global__ void __launch_bounds__(512, 1) k_assemble_tc(AsmArgs a, const double *__restrict__ tfrag) {
-  constexpr int TC_MB = 8;
-  using S = TcShape<E, NQ, DIFF>;
-  constexpr int NLOC = S::NLOC, NN = S::NN, MT = S::MT, KS = S::KS, KP = S::KP, KD = S::KD, CW = S::CW;
-  constexpr int NV = ET<E>::NV;
-  constexpr bool HEX = ET<E>::HEX;
-  extern __shared__ double sm[];
-  double *sT = sm;
-  for (int k = threadIdx.x; k < (int)S::TABLE_DOUBLES; k += blockDim.x) sT[k] = tfrag[k];
-  // Fourier modes of the coefficient field next to the table
-  double *sM = sm + S::TABLE_DOUBLES;
-  for (int k = threadIdx.x; k < 8 * a.coef.n_modes; k += blockDim.x) sM[k] = a.coef.modes[k];
-  __syncthreads();
-  if (a.coef.n_modes > 0) a.coef.modes = sM;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  double *Bs = sm + S::TABLE_DOUBLES + 8 * (size_t)a.coef.n_modes + (size_t)warp * S::WARP_DOUBLES;  // d[k][cell]
-  double *RW = Bs + KP * 8;                                                // w_q |det J| f(x_q), [cell][q]
-  double *Cs = RW + 8 * NQ;                                                // [cell][CW]
-  const bool supg = !DIFF && (a.form == PMG_FORM_SUPG || a.form == PMG_FORM_MASS_SUPG || a.form == PMG_FORM_STIFF_SUPG);
-  const int row = lane >> 2, c0 = 2 * (lane & 3);
-
-  for (int base = (blockIdx.x * nwarps + warp) * 8; base < a.n_elems; base += gridDim.x * nwarps * 8) {
-    const int ne = min(8, a.n_elems - base);
-    // 1) cell geometry and (CONST) the 16 coefficients of each cell
-    if (lane < 8) {
-      double *cw = Cs + lane * CW;
-      if (lane < ne) {
-        const int e = base + lane;
-        const double *cv = a.cell_vert + (size_t)e * NV * 3;
-        double J[9], x0[3], Ji[9], K[9], adet;
-        cell_map<HEX>(cv, J, x0, Ji, adet, K);
-        double delta = 0.0, bh[3] = {0.0, 0.0, 0.0};
-        if (!DIFF) {
-          const double *q0 = a.qtab;
-          double c[7];
-          coeff_eval(a.coef, x0[0] + J[0] * q0[1] + J[1] * q0[2] + J[2] * q0[3],
-                     x0[1] + J[3] * q0[1] + J[4] * q0[2] + J[5] * q0[3],
-                     x0[2] + J[6] * q0[1] + J[7] * q0[2] + J[8] * q0[3], c);
-          const double hconv = supg ? hk_convection(HEX, a.brick != 0, cv, Ji, c[1], c[2], c[3]) : 0.0;
-          delta = supg ? sdfem_delta(hconv, c[0], c[1], c[2], c[3], a.poly, a.delta0) : 0.0;
-#pragma unroll
-          for (int p = 0; p < 3; p++) bh[p] = Ji[p * 3 + 0] * c[1] + Ji[p * 3 + 1] * c[2] + Ji[p * 3 + 2] * c[3];
-          double D[16];
-          form_matrix(a.form, supg, c, K, bh, delta, D);
-#pragma unroll
-          for (int k = 0; k < 16; k++) Bs[k * 8 + lane] = D[k] * adet;
-        }
-#pragma unroll
-        for (int k = 0; k < 9; k++) cw[k] = J[k];
-        cw[9] = x0[0]; cw[10] = x0[1]; cw[11] = x0[2];
-        cw[12] = adet;
-        cw[13] = delta;
-        cw[14] = bh[0]; cw[15] = bh[1]; cw[16] = bh[2];
-        if (DIFF) { cw[17] = K[0]; cw[18] = K[4]; cw[19] = K[8]; cw[20] = K[1]; cw[21] = K[2]; cw[22] = K[5]; }
-      } else {
-        if (!DIFF)
-#pragma unroll
-          for (int k = 0; k < 16; k++) Bs[k * 8 + lane] = 0.0;
-        cw[12] = 0.0;
-      }
-    }
-    __syncwarp();
-    // 2) per cell and quadrature point: the rhs weights and (DIFF) the coefficients
-    for (int pq = lane; pq < 8 * NQ; pq += 32) {
-      const int c = pq / NQ, q = pq - c * NQ;
-      const double *cw = Cs + c * CW;
-      double fw = 0.0, ew = 0.0;
-      if (c < ne) {
-        const double *qq = a.qtab + q * 4;
-        const double X = cw[9] + cw[0] * qq[1] + cw[1] * qq[2] + cw[2] * qq[3];
-        const double Y = cw[10] + cw[3] * qq[1] + cw[4] * qq[2] + cw[5] * qq[3];
-        const double Z = cw[11] + cw[6] * qq[1] + cw[7] * qq[2] + cw[8] * qq[3];
-        double cf[7];
-        coeff_eval(a.coef, X, Y, Z, cf);
-        const double w = qq[0] * cw[12];
-        fw = w * cf[5];
-        ew = w * cf[0];
-      }
-      RW[c * NQ + q] = fw;
-      if (DIFF)
-#pragma unroll
-        for (int p = 0; p < 6; p++) Bs[(q * 6 + p) * 8 + c] = c < ne ? ew * cw[(17 + p) % CW] : 0.0;
-    }
-    for (int k = KD * 8 + lane; k < KP * 8; k += 32) Bs[k] = 0.0;  // padded k rows
-    __syncwarp();
-    // 3) rhs: f_i = sum_q w_q |det J| f(x_q) (u_i3(q) + delta bh . u_i(q))
-    if (a.rhs)
-      for (int ci = lane; ci < 8 * NLOC; ci += 32) {
-        const int c = ci / NLOC, i = ci - c * NLOC;
-        if (c >= ne) continue;
-        const int di = __ldg(a.elem_dof + (size_t)(base + c) * NLOC + i);
-        if (di >= a.Na) continue;
-        const double *cw = Cs + c * CW;
-        double r = 0.0;
-        for (int q = 0; q < NQ; q++) {
-          const double *u = a.utab + ((size_t)q * NLOC + i) * 4;
-          r += RW[c * NQ + q] * (__ldg(u + 3) + cw[13] * (cw[14] * __ldg(u) + cw[15] * __ldg(u + 1) + cw[16] * __ldg(u + 2)));
-        }
-        atomicAdd(a.rhs + di, r);
-      }
-    // 4) the local matrices, 8 entries x 8 cells per mma chain, and the scatter
-    auto load_slots = [&](int t0, int (&sl)[TC_MB][2]) {
-#pragma unroll
-      for (int b = 0; b < TC_MB; b++) {
-        const int m = 8 * (t0 + b) + row;
-#pragma unroll
-        for (int u = 0; u < 2; u++)
-          sl[b][u] = (t0 + b < MT && m < NN && c0 + u < ne) ? __ldg(a.slot + (size_t)(base + c0 + u) * NN + m) : -1;
-      }
-    };
-    int slc[TC_MB][2], sln[TC_MB][2];
-    load_slots(0, slc);
-    for (int t0 = 0; t0 < MT; t0 += TC_MB) {
-      if (t0 + TC_MB < MT) load_slots(t0 + TC_MB, sln);
-      double acc[TC_MB][2];
-#pragma unroll
-      for (int b = 0; b < TC_MB; b++) {
-        acc[b][0] = 0.0;
-        acc[b][1] = 0.0;
-        if (t0 + b < MT) {
-          const double *tb = sT + (size_t)(t0 + b) * KS * 32 + lane;
-#pragma unroll 4
-          for (int s = 0; s < KS; s++) dmma_8x8x4(acc[b][0], acc[b][1], tb[s * 32], Bs[(4 * s + (lane & 3)) * 8 + row]);
-        }
-      }
-      // the adds are reductions performed at L2 (no value comes back, so no
-      // load latency per entry); the cells of one launch share no row, so each
-      // entry gets at most one add per launch and the sum order is the launch
-      // order, the same on every run
-#pragma unroll
-      for (int b = 0; b < TC_MB; b++)
-#pragma unroll
-        for (int u = 0; u < 2; u++) {
-          const int q = slc[b][u];
-          if (q >= 0) scatter_entry(a.entries, q, acc[b][u]);
-          else if (q <= -3) a.entries[-3 - q] = 1.0;  // Dirichlet row: unit diagonal (AssembleMat3D.C:840-848)
-        }
-#pragma unroll
-      for (int b = 0; b < TC_MB; b++) {
-        slc[b][0] = sln[b][0];
-        slc[b][1] = sln[b][1];
-      }
-    }
-    __syncwarp();
-  }
 }
 
 // --- space-constant coefficients: per-cell set-up, then the contraction ----
@@ -783,22 +623,67 @@ __global__ void __launch_bounds__(128) k_tc_setup(AsmArgs a, double *__restrict_
   }
 }
 
-template <int E>
+// Pure diffusion with a coefficient eps(x) (b = 0, c = 0): one thread per
+// cell evaluates eps at the cell's NQ quadrature points (all lanes busy, the
+// Fourier modes of the field read through the cache) and stores
+// d[(q, p)] = w_q |det J| eps(x_q) K_p (K = Ji Ji^T, p over 00 11 22 01 02 12,
+// zero-padded to 4 KS) and the local rhs r_i = sum_q w_q |det J| f(x_q) u_i(q);
+// k_assemble_tc16<E, KS> then contracts with the per-point table on DMMA.
+template <int E, int NQ>
+__global__ void __launch_bounds__(128) k_tc_setup_diff(AsmArgs a, double *__restrict__ dbuf, double *__restrict__ rbuf) {
+  constexpr int NLOC = ET<E>::NLOC, NV = ET<E>::NV, KD = 6 * NQ, KP = 4 * ((KD + 3) / 4);
+  constexpr bool HEX = ET<E>::HEX;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= a.n_elems) return;
+  const double *cv = a.cell_vert + (size_t)e * NV * 3;
+  double J[9], x0[3], Ji[9], K[9], adet;
+  cell_map<HEX>(cv, J, x0, Ji, adet, K);
+  const double Kp[6] = {K[0], K[4], K[8], K[1], K[2], K[5]};
+  double *d = dbuf + (size_t)e * KP;
+  double fw[NQ];
+  for (int q = 0; q < NQ; q++) {
+    const double *qq = a.qtab + q * 4;
+    double cf[7];
+    coeff_eval(a.coef, x0[0] + J[0] * qq[1] + J[1] * qq[2] + J[2] * qq[3], x0[1] + J[3] * qq[1] + J[4] * qq[2] + J[5] * qq[3],
+               x0[2] + J[6] * qq[1] + J[7] * qq[2] + J[8] * qq[3], cf);
+    const double w = qq[0] * adet, ew = w * cf[0];
+    fw[q] = w * cf[5];
+#pragma unroll
+    for (int p = 0; p < 6; p++) d[q * 6 + p] = ew * Kp[p];
+  }
+  for (int k = KD; k < KP; k++) d[k] = 0.0;
+  if (!rbuf) return;
+  double *r = rbuf + (size_t)e * NLOC;
+  for (int i = 0; i < NLOC; i++) {
+    double acc = 0.0;
+    for (int q = 0; q < NQ; q++) acc += fw[q] * __ldg(a.utab + ((size_t)q * NLOC + i) * 4 + 3);
+    r[i] = acc;
+  }
+}
+
+// KS k-steps of 4: KS = 4 for space-constant coefficients (d = the 16
+// coefficients of D), KS = ceil(6 NQ / 4) for pure diffusion (d = the 6
+// entries of w_q |det J| eps(x_q) K per quadrature point, zero-padded)
+template <int E, int KS>
 __global__ void __launch_bounds__(512, 2) k_assemble_tc16(AsmArgs a, const double *__restrict__ tfrag,
                                                           const double *__restrict__ dbuf,
                                                           const double *__restrict__ rbuf) {
-  constexpr int NLOC = ET<E>::NLOC, NN = NLOC * NLOC, MT = (NN + 7) / 8, MB = 4;
+  constexpr int NLOC = ET<E>::NLOC, NN = NLOC * NLOC, MT = (NN + 7) / 8, MB = 4, KP = 4 * KS;
   extern __shared__ double sT[];
-  for (int k = threadIdx.x; k < MT * 4 * 32; k += blockDim.x) sT[k] = tfrag[k];
+  for (int k = threadIdx.x; k < MT * KS * 32; k += blockDim.x) sT[k] = tfrag[k];
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   const int row = lane >> 2, c0 = 2 * (lane & 3);
   for (int base = (blockIdx.x * nwarps + warp) * 8; base < a.n_elems; base += gridDim.x * nwarps * 8) {
     const int ne = min(8, a.n_elems - base);
-    // B fragments: d[cell row][4 s + lane % 4]
-    double bf[4];
+    // B fragments: d[cell row][4 s + lane % 4]; held in registers for KS = 4,
+    // re-read through L1 per entry block for the longer diffusion rows (the
+    // 64-register budget of two 512-thread blocks per SM)
+    constexpr bool REG = KS <= 4;
+    const double *drow = dbuf + (size_t)(base + (row < ne ? row : 0)) * KP + (lane & 3);
+    double bf[REG ? KS : 1];
 #pragma unroll
-    for (int s = 0; s < 4; s++) bf[s] = row < ne ? __ldg(dbuf + (size_t)(base + row) * 16 + 4 * s + (lane & 3)) : 0.0;
+    for (int s = 0; s < (REG ? KS : 1); s++) bf[s] = row < ne ? __ldg(drow + 4 * s) : 0.0;
     auto load_slots = [&](int t0, int (&sl)[MB][2]) {
 #pragma unroll
       for (int b = 0; b < MB; b++) {
@@ -818,9 +703,10 @@ __global__ void __launch_bounds__(512, 2) k_assemble_tc16(AsmArgs a, const doubl
         acc[b][0] = 0.0;
         acc[b][1] = 0.0;
         if (t0 + b < MT) {
-          const double *tb = sT + (size_t)(t0 + b) * 4 * 32 + lane;
+          const double *tb = sT + (size_t)(t0 + b) * KS * 32 + lane;
 #pragma unroll
-          for (int s = 0; s < 4; s++) dmma_8x8x4(acc[b][0], acc[b][1], tb[s * 32], bf[s]);
+          for (int s = 0; s < KS; s++)
+            dmma_8x8x4(acc[b][0], acc[b][1], tb[s * 32], REG ? bf[REG ? s : 0] : (row < ne ? __ldg(drow + 4 * s) : 0.0));
         }
       }
       // L2 reductions (no value returned): the cells of one launch share no
@@ -1047,55 +933,36 @@ static int launch_assemble_cc(Handle &h, Level &L, AsmArgs a, const double *stab
   return PMG_OK;
 }
 
-// warps per block of k_assemble_tc (0: the table does not leave room for 4)
-template <int E, int NQ, bool DIFF>
-static int tc_warps(int n_modes) {
-  using S = TcShape<E, NQ, DIFF>;
-  const long avail = 227L * 1024 / 8 - (long)S::TABLE_DOUBLES - 8L * n_modes;
-  const long w = std::min(16L, avail / S::WARP_DOUBLES);
-  return w >= 4 ? (int)w : 0;
-}
-
-template <int E, int NQ, bool DIFF>
-static int launch_assemble_tc(Handle &h, Level &L, AsmArgs a, const double *tfrag) {
-  using S = TcShape<E, NQ, DIFF>;
-  const int WARPS = tc_warps<E, NQ, DIFF>(a.coef.n_modes);
-  const size_t smem = sizeof(double) * (S::TABLE_DOUBLES + 8 * (size_t)a.coef.n_modes + (size_t)WARPS * S::WARP_DOUBLES);
-  auto kern = k_assemble_tc<E, NQ, DIFF>;
+// the per-colour contraction launches over the per-cell data in h.tc_dbuf / h.tc_rbuf
+template <int E, int KS>
+static int launch_contract(Handle &h, Level &L, AsmArgs a, const double *tfrag) {
+  constexpr int NLOC = ET<E>::NLOC, NN = NLOC * NLOC, MT = (NN + 7) / 8, WARPS = 16;
+  const size_t smem = sizeof(double) * (size_t)MT * KS * 32;
   static bool attr_set = false;
   if (!attr_set) {
-    PMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    PMG_CUDA(cudaFuncSetAttribute(k_assemble_tc16<E, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr_set = true;
   }
-  h.asm_path = DIFF ? 1 : 0;
-  h.asm_kd = S::KD;
-  const int *ed0 = a.elem_dof;
-  const double *cv0 = a.cell_vert;
-  const int *sl0 = a.slot;
   for (size_t c = 0; c + 1 < L.ecolor_ptr.size(); c++) {
     const int beg = L.ecolor_ptr[c], n = L.ecolor_ptr[c + 1] - beg;
     if (n <= 0) continue;
     AsmArgs b = a;
     b.n_elems = n;
-    b.elem_dof = ed0 + (size_t)beg * S::NLOC;
-    b.cell_vert = cv0 + (size_t)beg * ET<E>::NV * 3;
-    b.slot = sl0 + (size_t)beg * S::NN;
-    const int blocks = std::min((n + WARPS * 8 - 1) / (WARPS * 8), h.num_sms);
-    kern<<<blocks, WARPS * 32, smem, h.stream>>>(b, tfrag); count_launches(1);
+    b.elem_dof = a.elem_dof + (size_t)beg * NLOC;
+    b.slot = a.slot + (size_t)beg * NN;
+    const int blocks = std::min((n + WARPS * 8 - 1) / (WARPS * 8), 2 * h.num_sms);
+    k_assemble_tc16<E, KS><<<blocks, WARPS * 32, smem, h.stream>>>(b, tfrag, h.tc_dbuf.p + (size_t)beg * 4 * KS,
+                                                                   h.tc_rbuf.p + (size_t)beg * NLOC);
+    count_launches(1);
     PMG_CUDA(cudaGetLastError());
   }
   return PMG_OK;
 }
 
+// space-constant coefficients: d = |det J| D (16 per cell), then the contraction
 template <int E, int NQ>
 static int launch_assemble_tc16(Handle &h, Level &L, AsmArgs a, const double *tfrag, const double *rtab) {
-  constexpr int NLOC = ET<E>::NLOC, NN = NLOC * NLOC, MT = (NN + 7) / 8, WARPS = 16;
-  const size_t smem = sizeof(double) * (size_t)MT * 4 * 32;
-  static bool attr_set = false;
-  if (!attr_set) {
-    PMG_CUDA(cudaFuncSetAttribute(k_assemble_tc16<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set = true;
-  }
+  constexpr int NLOC = ET<E>::NLOC;
   h.asm_path = 0;
   h.asm_kd = 16;
   PMG_TRY(h.tc_dbuf.reserve((size_t)L.n_cells * 16));
@@ -1106,20 +973,23 @@ static int launch_assemble_tc16(Handle &h, Level &L, AsmArgs a, const double *tf
                                                                      rtab);
   count_launches(1);
   PMG_CUDA(cudaGetLastError());
-  for (size_t c = 0; c + 1 < L.ecolor_ptr.size(); c++) {
-    const int beg = L.ecolor_ptr[c], n = L.ecolor_ptr[c + 1] - beg;
-    if (n <= 0) continue;
-    AsmArgs b = a;
-    b.n_elems = n;
-    b.elem_dof = a.elem_dof + (size_t)beg * NLOC;
-    b.slot = a.slot + (size_t)beg * NN;
-    const int blocks = std::min((n + WARPS * 8 - 1) / (WARPS * 8), 2 * h.num_sms);
-    k_assemble_tc16<E><<<blocks, WARPS * 32, smem, h.stream>>>(b, tfrag, h.tc_dbuf.p + (size_t)beg * 16,
-                                                               h.tc_rbuf.p + (size_t)beg * NLOC);
-    count_launches(1);
-    PMG_CUDA(cudaGetLastError());
-  }
-  return PMG_OK;
+  return launch_contract<E, 4>(h, L, a, tfrag);
+}
+
+// pure diffusion with eps(x): per-point coefficients per cell, then the contraction
+template <int E, int NQ>
+static int launch_assemble_diff(Handle &h, Level &L, AsmArgs a, const double *tfrag) {
+  constexpr int NLOC = ET<E>::NLOC, KS = (6 * NQ + 3) / 4;
+  h.asm_path = 1;
+  h.asm_kd = 6 * NQ;
+  PMG_TRY(h.tc_dbuf.reserve((size_t)L.n_cells * 4 * KS));
+  PMG_TRY(h.tc_rbuf.reserve((size_t)L.n_cells * NLOC));
+  AsmArgs all = a;
+  all.n_elems = L.n_cells;
+  k_tc_setup_diff<E, NQ><<<(L.n_cells + 127) / 128, 128, 0, h.stream>>>(all, h.tc_dbuf.p, a.rhs ? h.tc_rbuf.p : nullptr);
+  count_launches(1);
+  PMG_CUDA(cudaGetLastError());
+  return launch_contract<E, KS>(h, L, a, tfrag);
 }
 
 // coefficient kinds whose eps, b and c are constant in space
@@ -1191,9 +1061,6 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
                               h.coeff.b[2] == 0.0 && h.coeff.c == 0.0 && form != PMG_FORM_MASS &&
                               form != PMG_FORM_MASS_SUPG;
   const int nm = h.coeff.n_modes;
-#define PMG_TC(E_, NQ_, DIFF_) \
-  if (tc_warps<E_, NQ_, DIFF_>(nm)) return launch_assemble_tc<E_, NQ_, DIFF_>(h, L, a, tf); \
-  break
   if (h.prm.assembly_kernel == 0 && constant_matrix_coefficients(h.coeff.kind)) {
     const double *tf = T->tc_const.p;
     switch (L.elem * 1000 + T->nq) {
@@ -1216,18 +1083,17 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
   if (h.prm.assembly_kernel == 0 && pure_diffusion) {
     const double *tf = T->tc_diff.p;
     switch (L.elem * 1000 + T->nq) {
-      case PMG_ELEM_Q1_HEX * 1000 + 8: PMG_TC(PMG_ELEM_Q1_HEX, 8, true);
-      case PMG_ELEM_Q1_HEX * 1000 + 27: PMG_TC(PMG_ELEM_Q1_HEX, 27, true);
-      case PMG_ELEM_P1_TET * 1000 + 4: PMG_TC(PMG_ELEM_P1_TET, 4, true);
-      case PMG_ELEM_P1_TET * 1000 + 5: PMG_TC(PMG_ELEM_P1_TET, 5, true);
-      case PMG_ELEM_P1_TET * 1000 + 11: PMG_TC(PMG_ELEM_P1_TET, 11, true);
-      case PMG_ELEM_P2_TET * 1000 + 4: PMG_TC(PMG_ELEM_P2_TET, 4, true);
-      case PMG_ELEM_P2_TET * 1000 + 5: PMG_TC(PMG_ELEM_P2_TET, 5, true);
-      case PMG_ELEM_P2_TET * 1000 + 11: PMG_TC(PMG_ELEM_P2_TET, 11, true);
+      case PMG_ELEM_Q1_HEX * 1000 + 8: return launch_assemble_diff<PMG_ELEM_Q1_HEX, 8>(h, L, a, tf);
+      case PMG_ELEM_Q1_HEX * 1000 + 27: return launch_assemble_diff<PMG_ELEM_Q1_HEX, 27>(h, L, a, tf);
+      case PMG_ELEM_P1_TET * 1000 + 4: return launch_assemble_diff<PMG_ELEM_P1_TET, 4>(h, L, a, tf);
+      case PMG_ELEM_P1_TET * 1000 + 5: return launch_assemble_diff<PMG_ELEM_P1_TET, 5>(h, L, a, tf);
+      case PMG_ELEM_P1_TET * 1000 + 11: return launch_assemble_diff<PMG_ELEM_P1_TET, 11>(h, L, a, tf);
+      case PMG_ELEM_P2_TET * 1000 + 4: return launch_assemble_diff<PMG_ELEM_P2_TET, 4>(h, L, a, tf);
+      case PMG_ELEM_P2_TET * 1000 + 5: return launch_assemble_diff<PMG_ELEM_P2_TET, 5>(h, L, a, tf);
+      case PMG_ELEM_P2_TET * 1000 + 11: return launch_assemble_diff<PMG_ELEM_P2_TET, 11>(h, L, a, tf);
       default: break;
     }
   }
-#undef PMG_TC
   if (h.prm.assembly_kernel == 2 && constant_matrix_coefficients(h.coeff.kind)) {
     const double *st = T->stab.p;
     switch (L.elem * 1000 + T->nq) {
