@@ -307,7 +307,8 @@ __global__ void __launch_bounds__(ASM_WARPS * 32, 2) k_assemble(AsmArgs a) {
   double *G = sG + (size_t)(warp * GPW + (lane_used ? grp : 0)) * GS;
   const bool supg = (a.form == PMG_FORM_SUPG || a.form == PMG_FORM_MASS_SUPG || a.form == PMG_FORM_STIFF_SUPG);
 
-  for (int base = (blockIdx.x * ASM_WARPS + warp) * GPW; base < a.n_elems; base += gridDim.x * ASM_WARPS * GPW) {
+  const int nw = blockDim.x >> 5;  // ASM_WARPS, or fewer when the per-element scratch is large
+  for (int base = (blockIdx.x * nw + warp) * GPW; base < a.n_elems; base += gridDim.x * nw * GPW) {
     const int e = base + grp;
     const bool valid = lane_used && e < a.n_elems;
     if (valid) {
@@ -874,14 +875,23 @@ static int get_tables(int elem, int rule, TableCache *&out) {
 template <int E, int NQ>
 static int launch_assemble(Handle &h, Level &L, AsmArgs a) {
   constexpr int NLOC = ET<E>::NLOC, GPW = 32 / NLOC;
-  size_t smem = sizeof(double) * ((size_t)NQ * NLOC * 4 + NQ * 4 + (size_t)ASM_WARPS * GPW * NQ * 20);
+  // warps per block: ASM_WARPS, fewer when the per-element scratch (NQ x 20
+  // doubles per element) would not fit the 227 KB of shared memory (N_Q1 with
+  // Gauss4: 5 elements per warp x 64 points)
+  const size_t fixed = (size_t)NQ * NLOC * 4 + NQ * 4, per_warp = (size_t)GPW * NQ * 20;
+  const int warps = (int)std::min<size_t>(ASM_WARPS, (227 * 1024 / sizeof(double) - fixed) / per_warp);
+  if (warps < 1) {
+    set_error("assemble: the quadrature rule does not fit the per-point kernel's shared memory");
+    return PMG_ERR_UNSUPPORTED;
+  }
+  size_t smem = sizeof(double) * (fixed + (size_t)warps * per_warp);
   static bool attr_set = false;
   if (!attr_set) {
-    PMG_CUDA(cudaFuncSetAttribute(k_assemble<E, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PMG_CUDA(cudaFuncSetAttribute(k_assemble<E, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
     attr_set = true;
   }
   h.asm_path = 3;
-  int per_block = ASM_WARPS * GPW;
+  int per_block = warps * GPW;
   const int *ed0 = a.elem_dof;
   const double *cv0 = a.cell_vert;
   const int *sl0 = a.slot;
@@ -897,7 +907,7 @@ static int launch_assemble(Handle &h, Level &L, AsmArgs a) {
     int blocks = (n + per_block - 1) / per_block;
     int cap = h.num_sms * 8;
     if (blocks > cap) blocks = cap;
-    k_assemble<E, NQ><<<blocks, ASM_WARPS * 32, smem, h.stream>>>(b); count_launches(1);
+    k_assemble<E, NQ><<<blocks, warps * 32, smem, h.stream>>>(b); count_launches(1);
     PMG_CUDA(cudaGetLastError());
   }
   return PMG_OK;

@@ -17,7 +17,8 @@ pytestmark = pytest.mark.gpu
     ("Q1_HEX", "MASS_SUPG", "CONST", 0.0, 1), ("P2_TET", "SUPG", "CONST", 0.2, 1), ("P1_TET", "GALERKIN", "AMC", 0.2, 1),
     ("Q2_HEX", "MASS", "AMC", 0.0, 1), ("P2_TET", "STIFF_SUPG", "CONST", 0.2, 1), ("Q1_HEX", "GALERKIN", "CONST", 0.0, 0),
     ("P2_TET", "GALERKIN", "LOGNORMAL", 0.2, 1), ("Q1_HEX", "GALERKIN", "LOGNORMAL", 0.0, 1),
-    ("P1_TET", "SUPG", "LOGNORMAL", 0.2, 0), ("Q1_HEX", "GALERKIN", "LOGNORMAL", 0.0, 0)])
+    ("P1_TET", "SUPG", "LOGNORMAL", 0.2, 0), ("Q1_HEX", "GALERKIN", "LOGNORMAL", 0.0, 0),
+    ("NQ1_HEX", "SUPG", "CONST", 0.0, 1), ("NQ1_HEX", "SUPG", "CONST", 0.0, 0), ("NQ1_HEX", "GALERKIN", "SINE_RHS", 0.0, 0)])
 def test_reference_matrix_kernel_equals_point_kernel(pmg, elem, form, kind, jitter, linear):
     from parmoon_b200.configs import lognormal_modes
     et = getattr(pmg, elem)
