@@ -107,3 +107,10 @@ def test_all_dirichlet_coarsest_level_and_one_level_hierarchy(pmg):
     _, st, rc = h1.solve()
     assert rc == 0 and st.iterations <= 2 and st.rel_res <= 1e-10
     h1.close()
+
+
+def test_peak_probes_report_positive_throughput(pmg):
+    """pmg_measure_peaks (the denominators of the DMMA and BF16 rooflines) runs
+    its three probes and reports finite, positive TFLOP/s."""
+    fma, dmma, hmma = pmg.measure_peaks()
+    assert all(np.isfinite(v) and v > 1.0 for v in (fma, dmma, hmma)), (fma, dmma, hmma)
