@@ -273,6 +273,28 @@ int pmg_set_level_mesh(pmg_handle hh, int level, int elem_type, int n_cells, con
   if (!L.has_csr) { set_error("pmg_set_level_mesh: call pmg_set_level_csr first"); return PMG_ERR_STATE; }
   for (size_t k = 0; k < (size_t)n_cells * nloc; k++)
     if (elem_dof[k] < 0 || elem_dof[k] >= L.N) { set_error("pmg_set_level_mesh: dof index out of range"); return PMG_ERR_ARG; }
+  if (nv == 8) {
+    // the kernels map hexahedra affinely (HexaAffin): every cell must be a
+    // parallelepiped, v2 = v1 + v3 - v0, v5 = v1 + v4 - v0, v7 = v3 + v4 - v0,
+    // v6 = v1 + v3 + v4 - 2 v0 (the trilinear map of HexaTrilinear is not built)
+    for (int e = 0; e < n_cells; e++) {
+      const double *v = cell_vert + (size_t)e * 24;
+      double diam = 0.0, dev = 0.0;
+      for (int d = 0; d < 3; d++) {
+        const double a = v[3 + d] - v[d], b = v[9 + d] - v[d], c = v[12 + d] - v[d];
+        diam = std::max(diam, std::fabs(a) + std::fabs(b) + std::fabs(c));
+        dev = std::max(dev, std::fabs(v[6 + d] - (v[3 + d] + v[9 + d] - v[d])));
+        dev = std::max(dev, std::fabs(v[15 + d] - (v[3 + d] + v[12 + d] - v[d])));
+        dev = std::max(dev, std::fabs(v[21 + d] - (v[9 + d] + v[12 + d] - v[d])));
+        dev = std::max(dev, std::fabs(v[18 + d] - (v[3 + d] + v[9 + d] + v[12 + d] - 2 * v[d])));
+      }
+      if (!(dev <= 1e-10 * diam)) {
+        set_error("pmg_set_level_mesh: cell " + std::to_string(e) +
+                  " is a hexahedron that is not a parallelepiped (the trilinear map, HexaTrilinear, is not built)");
+        return PMG_ERR_UNSUPPORTED;
+      }
+    }
+  }
   int ncol = 0;
   std::vector<int> color = color_cells(n_cells, nloc, elem_dof, L.N, ncol);
   // colour-sorted copies

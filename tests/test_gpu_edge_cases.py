@@ -114,3 +114,20 @@ def test_peak_probes_report_positive_throughput(pmg):
     its three probes and reports finite, positive TFLOP/s."""
     fma, dmma, hmma = pmg.measure_peaks()
     assert all(np.isfinite(v) and v > 1.0 for v in (fma, dmma, hmma)), (fma, dmma, hmma)
+
+
+def test_non_parallelepiped_hexahedra_are_rejected(pmg):
+    """The kernels map hexahedra affinely; a cell whose vertices do not form a
+    parallelepiped (it would need HexaTrilinear) is an unsupported mesh, not a
+    silently wrong matrix."""
+    levels = pmg.struct_hierarchy(pmg.Q1_HEX, 2, 1)
+    L = levels[-1]
+    h = pmg.Handle(1)
+    h.set_level_csr(0, L["rowptr"], L["kcol"], L["active_bound"])
+    cv = L["cell_vert"].copy().reshape(-1, 8, 3)
+    cv[0, 6] += 0.05  # move the far corner of cell 0
+    with pytest.raises(pmg.PmgError) as e:
+        h.set_level_mesh(0, pmg.Q1_HEX, L["elem_dof"], cv.ravel(), brick=True)
+    assert e.value.code == pmg.ERR_UNSUPPORTED
+    h.set_level_mesh(0, pmg.Q1_HEX, L["elem_dof"], L["cell_vert"], brick=True)  # the unchanged mesh is fine
+    h.close()
