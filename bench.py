@@ -465,7 +465,7 @@ def bench_ours(args, rank, world, dist):
     line = None
     if rank == 0:
         cpu = None
-        if os.path.exists(REF_BIN) and not args.no_cpu:
+        if os.path.exists(REF_BIN) and not args.no_cpu and world == 1:  # the CPU baseline is an N=1 figure
             # one sequential reference process, one step of the same workload
             # (after the GPU timing, so the two do not share the host)
             r = run_reference(1, 0, max_procs=1)
