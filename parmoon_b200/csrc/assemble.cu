@@ -1065,12 +1065,11 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
   a.qtab = T->qtab.p;
   a.flags = h.d_flags.p;
   // tensor-core kernel: space-constant coefficients (any element), or pure
-  // diffusion with a varying eps on Q1 / P1 / P2 (whose DIFF table fits in
-  // shared memory)
+  // diffusion with a varying eps on Q1 / P1 / P2 (per-cell coefficients at the
+  // quadrature points, then the same contraction)
   const bool pure_diffusion = h.coeff.kind == PMG_COEF_LOGNORMAL && h.coeff.b[0] == 0.0 && h.coeff.b[1] == 0.0 &&
                               h.coeff.b[2] == 0.0 && h.coeff.c == 0.0 && form != PMG_FORM_MASS &&
                               form != PMG_FORM_MASS_SUPG;
-  const int nm = h.coeff.n_modes;
   if (h.prm.assembly_kernel == 0 && constant_matrix_coefficients(h.coeff.kind)) {
     const double *tf = T->tc_const.p;
     switch (L.elem * 1000 + T->nq) {

@@ -572,16 +572,6 @@ int pmg_get_rhs(pmg_handle hh, int level, double *out) {
 }
 
 // ------------------------------------------------------------ host-array kernels
-static int with_pinned(Handle *h, size_t n) {
-  if (h->h_pinned_n >= n) return PMG_OK;
-  if (h->h_pinned) cudaFreeHost(h->h_pinned);
-  h->h_pinned = nullptr;
-  h->h_pinned_n = 0;
-  PMG_CUDA(cudaMallocHost(&h->h_pinned, n * sizeof(double)));
-  h->h_pinned_n = n;
-  return PMG_OK;
-}
-
 int pmg_matvec(pmg_handle hh, int level, const double *x, double *y) {
   Handle *h = H(hh);
   PMG_TRY(check_matrix(h, level, "pmg_matvec"));

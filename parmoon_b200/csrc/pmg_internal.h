@@ -239,8 +239,6 @@ struct Handle {
   // learned-smoother guard: V-cycle graph with SSOR, active choice
   cudaGraphExec_t vgraph_ssor = nullptr;
   unsigned long long vgraph_ssor_kernels = 0;
-  double *h_pinned = nullptr;
-  size_t h_pinned_n = 0;
   // halo of a subdomain (solve_dd): owned dofs packed for the neighbours, ghost rows
   // filled from them; the packing buffers belong to the caller's transport
   bool halo_set = false;
@@ -271,7 +269,6 @@ template <typename T>
 int restrict_defect(cudaStream_t s, const Level &Lf, const Level &Lc, const T *rval, const T *d, T *fc, T *xc = nullptr);
 template <typename T>
 int prolongate_add(cudaStream_t s, const Level &Lf, const T *pval, const T *xc, T *xf, double damp);
-int compute_invdiag(cudaStream_t s, Level &L);
 int convert_f64_f32(cudaStream_t s, const double *a, float *b, size_t n);
 int copy_dirichlet(cudaStream_t s, int Na, int N, const double *f, double *x);
 int dot(Handle &h, const double *a, const double *b, size_t n, double *result_dev);

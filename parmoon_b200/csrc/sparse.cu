@@ -215,10 +215,7 @@ __global__ void k_invdiag(int N, const int *__restrict__ dpos, const double *__r
   if (invd32) invd32[i] = (float)(1.0 / v);
 }
 
-int compute_invdiag(cudaStream_t s, Level &L) {
-  (void)s;
-  return PMG_OK;
-}
+
 
 __global__ void k_f64_to_f32(size_t n, const double *__restrict__ a, float *__restrict__ b) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
