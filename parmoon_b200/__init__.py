@@ -511,7 +511,11 @@ def struct_hierarchy(elem, n_fine, n_levels, jitter=0.0, seed=0):
     for l in range(n_levels):
         n = n_fine >> (n_levels - 1 - l)
         L = struct_level(elem, n, jitter=jitter if l == n_levels - 1 else 0.0, seed=seed)
-        if l > 0:
+        if l > 0 and elem == NQ1_HEX:  # no node lattice: Prolongate's cell average
+            C = levels[-1]
+            L["P"] = cell_prolongation(elem, C["elem_dof"], C["cell_vert"], C["N"], elem, L["elem_dof"],
+                                       L["cell_vert"], struct_parents(n), L["N"])
+        elif l > 0:
             L["P"] = struct_prolongation(elem, n // 2, levels[-1]["dof_lat"], L["dof_lat"])
         levels.append(L)
     return levels

@@ -194,16 +194,19 @@ template int sell_values<double>(Handle &, Level &);
 // Column indices: a slice whose deltas fit (every slice of a lattice-ordered
 // level) is read as 16-bit column - row deltas and gathered through x + row
 // of the lane; the other slices read the 32-bit columns.  The choice is per
-// slice and warp-uniform.
+// slice and warp-uniform.  Matrix values and columns are read once per pass
+// with streaming loads (ld.global.cs, evict-first), so they do not push the
+// gathered iterate out of L1/L2: measured on the 64^3 finest level, FP32 SSOR
+// step 0.490 -> 0.467 ms, FP64 SpMV 0.296 -> 0.272 ms.
 template <int PF, int K>
 __device__ __forceinline__ void sell_load_cols(bool wd, const int *__restrict__ col, const short *__restrict__ c16,
                                                int base, int j0, int lmax, int *ci) {
   if (wd) {
 #pragma unroll
-    for (int u = 0; u < PF; u++) ci[u] = j0 + u * K < lmax ? __ldg(col + base + 32 * K * u) : 0;
+    for (int u = 0; u < PF; u++) ci[u] = j0 + u * K < lmax ? __ldcs(col + base + 32 * K * u) : 0;
   } else {
 #pragma unroll
-    for (int u = 0; u < PF; u++) ci[u] = j0 + u * K < lmax ? (int)__ldg(c16 + base + 32 * K * u) : 0;
+    for (int u = 0; u < PF; u++) ci[u] = j0 + u * K < lmax ? (int)__ldcs(c16 + base + 32 * K * u) : 0;
   }
 }
 
@@ -230,7 +233,7 @@ __global__ void __launch_bounds__(32 * K) k_sell_mv(int s0, int s1, const int *_
     const int j0 = w + c0 * K;
     sell_load_cols<PF, K>(wd, col, c16, off + 32 * j0 + lane, j0, lmax, ci);
 #pragma unroll
-    for (int u = 0; u < PF; u++) cv[u] = j0 + u * K < lmax ? __ldg(val + off + 32 * (j0 + u * K) + lane) : (T)0;
+    for (int u = 0; u < PF; u++) cv[u] = j0 + u * K < lmax ? __ldcs(val + off + 32 * (j0 + u * K) + lane) : (T)0;
   };
   auto start = [&](int sl) {
     off = __ldg(sptr + sl);
@@ -296,7 +299,7 @@ __global__ void __launch_bounds__(32 * K) k_sell_gs(int s0, int s1, const int *_
     sell_load_cols<GS_PF, K>(wd, col, c16, off + 32 * j0 + lane, j0, lmax, ci);
 #pragma unroll
     for (int u = 0; u < GS_PF; u++)
-      cv[u] = j0 + u * K < lmax ? __ldg(val + off + 32 * (j0 + u * K) + lane) : (T)0;
+      cv[u] = j0 + u * K < lmax ? __ldcs(val + off + 32 * (j0 + u * K) + lane) : (T)0;
   };
   auto prefetch = [&](int sl) {
     off = __ldg(sptr + sl);
