@@ -160,23 +160,7 @@ struct Level {
   long sell_nnz_narrow = 0, sell_nnz_wide = 0;  // stored entries with 16-bit / 32-bit columns
   DBuf<float> sell_val32, sell_invd32;
   DBuf<double> sell_val64, sell_invd64;
-  // region sweeps (region_sweep.cu): regions, slice range per (colour, region),
-  // coupled regions, progress counters, the pass lists of the pre / post phase
-  int rs_nreg = 0;
-  DBuf<int> rs_seg, rs_nb_ptr, rs_nb, rs_prog, rs_pass[2];
-  std::vector<int> rs_pass_host[2];
 };
-
-template <typename T>
-inline const T *sell_val(const Level &L) {
-  if (sizeof(T) == 4) return reinterpret_cast<const T *>(L.sell_val32.p);
-  return reinterpret_cast<const T *>(L.sell_val64.p);
-}
-template <typename T>
-inline const T *sell_invd(const Level &L) {
-  if (sizeof(T) == 4) return reinterpret_cast<const T *>(L.sell_invd32.p);
-  return reinterpret_cast<const T *>(L.sell_invd64.p);
-}
 
 // Activations of the stencil network.  The tensor-core forward reads and
 // writes node-major BF16 (32 channels = 64 bytes per lattice node, two
@@ -245,7 +229,6 @@ struct Handle {
   bool use_graph = true;  // PMG_NO_GRAPH=1 launches the V-cycle kernels directly (profilers)
   int cc_top = 0;         // levels 0..cc_top run as one launch (0: none)
   DBuf<int> cc_err;      // set by the one-launch coarse cycle when a bounded wait gives up
-  DBuf<int> rs_err;      // set by a region sweep when a bounded wait gives up
   int cc_ctas = 0;        // CTAs of that launch (1, or a cluster of up to 16)
   // learned smoother: BF16 weights used by the kernels, FP32 master copy, Adam state
   DBuf<uint16_t> lw_bf16;
@@ -299,16 +282,6 @@ int check_finite(cudaStream_t s, const double *x, size_t n, int *flag);
 
 // ------------------------------------------------------------- SELL-32 (sell.cu)
 int build_sell(Handle &h, Level &L);
-template <typename T>
-int sell_copy_dirichlet(cudaStream_t s, const Level &L, const T *f, T *x);
-// region sweeps (region_sweep.cu)
-int region_count(const Handle &h, const Level &L);
-int region_key(int r, int Na, int nreg);
-int region_setup(Handle &h, Level &L, const std::vector<int> &perm, int nreg);
-int region_prepare(Handle &h, Level &L);
-template <typename T>
-int region_ssor_phase(Handle &h, Level &L, const T *f, T *x, double omega, int which, bool dirichlet_first);
-int region_check(Handle &h);
 template <typename T>
 int sell_values(Handle &h, Level &L);
 template <typename T>

@@ -57,25 +57,16 @@ int build_sell(Handle &h, Level &L) {
   std::vector<int> perm;
   std::vector<int> group_slice(nc + 2, 0);
   perm.reserve((size_t)N + 32 * (nc + 1));
-  // with region sweeps (region_sweep.cu) the rows of a colour are ordered by
-  // region first and every region starts a new slice
-  const int nreg = region_count(h, L);
   std::vector<int> rows;
   for (int g = 0; g <= nc; g++) {
     rows.clear();
     if (g < nc) rows.assign(L.h_row_list.begin() + L.rcolor_ptr[g], L.h_row_list.begin() + L.rcolor_ptr[g + 1]);
     else for (int r = Na; r < N; r++) rows.push_back(r);
     std::stable_sort(rows.begin(), rows.end(), [&](int a, int b) {
-      const int ra = region_key(a, Na, nreg), rb = region_key(b, Na, nreg);
-      if (ra != rb) return ra < rb;
       return alen[a] > alen[b] || (alen[a] == alen[b] && a < b);
     });
     group_slice[g] = (int)(perm.size() / 32);
-    for (size_t t = 0; t < rows.size(); t++) {
-      if (nreg > 0 && t > 0 && region_key(rows[t], Na, nreg) != region_key(rows[t - 1], Na, nreg))
-        while (perm.size() % 32) perm.push_back(-1);
-      perm.push_back(rows[t]);
-    }
+    perm.insert(perm.end(), rows.begin(), rows.end());
     while (perm.size() % 32) perm.push_back(-1);
   }
   group_slice[nc + 1] = (int)(perm.size() / 32);
@@ -142,7 +133,7 @@ int build_sell(Handle &h, Level &L) {
   L.sell_nnz_wide = wide_nnz;
   L.sell_ready = true;
   L.sell_val_fresh32 = L.sell_val_fresh64 = false;
-  return region_setup(h, L, perm, nreg);
+  return PMG_OK;
 }
 
 // values of the CSR matrix into the slice layout (and the permuted inverse diagonal)
@@ -368,17 +359,6 @@ __global__ void k_sell_copy_dirichlet(int Na, int N, const T *__restrict__ f, T 
   if (i < N) x[i] = f[i];
 }
 
-template <typename T>
-int sell_copy_dirichlet(cudaStream_t s, const Level &L, const T *f, T *x) {
-  const int nd = L.N - L.Na;
-  if (nd <= 0) return PMG_OK;
-  PMG_CUDA(launch_pdl(k_sell_copy_dirichlet<T>, dim3((nd + 255) / 256), dim3(256), 0, s, L.Na, L.N, f, x));
-  count_launches(1);
-  return PMG_OK;
-}
-template int sell_copy_dirichlet<float>(cudaStream_t, const Level &, const float *, float *);
-template int sell_copy_dirichlet<double>(cudaStream_t, const Level &, const double *, double *);
-
 // y_r -= sum over the Dirichlet columns j of active row r of A_rj v_j (the
 // entries [dd_beg, row end) of the CSR row, FP64 values)
 template <typename T>
@@ -424,6 +404,16 @@ static int slice_grid(int nslices, int num_sms, int k) {
   return (int)std::max(1L, std::min((long)nslices, cap));
 }
 
+template <typename T>
+static const T *sell_val(const Level &L) {
+  if (sizeof(T) == 4) return reinterpret_cast<const T *>(L.sell_val32.p);
+  return reinterpret_cast<const T *>(L.sell_val64.p);
+}
+template <typename T>
+static const T *sell_invd(const Level &L) {
+  if (sizeof(T) == 4) return reinterpret_cast<const T *>(L.sell_invd32.p);
+  return reinterpret_cast<const T *>(L.sell_invd64.p);
+}
 
 template <typename T, int MODE, int K>
 static cudaError_t launch_mv(cudaStream_t s, const Level &L, const T *x, const T *f, T *y, int num_sms, int n = -1,

@@ -600,23 +600,13 @@ static int vcycle(Handle &h, int i, bool learned) {
   const int post = (learned && h.prm.learned_steps > 0) ? h.prm.learned_steps : h.prm.post_smooth;
   const bool slc = h.prm.slc_all || (h.prm.slc_fine && i == (int)h.lv.size() - 1);
   if (slc) PMG_TRY(slc_begin<T>(h, L));
-  // plain SSOR phases of a level with regions: one launch per phase (region_sweep.cu)
-  const bool regions = !learned && h.prm.smoother == PMG_SMOOTHER_SSOR && L.rs_nreg > 0;
-  auto phase = [&](int steps, bool dirichlet_first, int which) -> int {
-    if (regions && steps > 0) {
-      const int rc = region_ssor_phase<T>(h, L, PT::f(L), PT::x(L), h.prm.smooth_omega, which, dirichlet_first);
-      if (rc != PMG_ERR_UNSUPPORTED) return rc;
-    }
-    for (int k = 0; k < steps; k++)
-      PMG_TRY(smooth_step<T>(h, L, learned, dirichlet_first && k == 0, k > 0, h.prm.smoother));
-    return PMG_OK;
-  };
-  PMG_TRY(phase(pre, true, 0));
+  for (int k = 0; k < pre; k++) PMG_TRY(smooth_step<T>(h, L, learned, k == 0, k > 0, h.prm.smoother));
   PMG_TRY(sell_spmv<T>(s, L, PT::x(L), PT::f(L), PT::d(L), 1, h.num_sms));
   PMG_TRY(restrict_defect<T>(s, L, C, PT::R(L), PT::d(L), PT::f(C), PT::x(C)));  // also x_C := 0
   PMG_TRY(vcycle<T>(h, i - 1, learned));
   PMG_TRY(prolongate_add<T>(s, L, PT::P(L), PT::x(C), PT::x(L), h.prm.gmg_damp));
-  PMG_TRY(phase(post, pre == 0, 1));
+  for (int k = 0; k < post; k++)
+    PMG_TRY(smooth_step<T>(h, L, learned, pre == 0 && k == 0, k > 0, h.prm.smoother));
   if (slc) PMG_TRY(slc_end<T>(h, L));
   return PMG_OK;
 }
@@ -670,7 +660,6 @@ static int prepare_levels(Handle &h) {
     } else {
       PMG_TRY(sell_values<double>(h, L));
     }
-    PMG_TRY(region_prepare(h, L));
   }
   // the outer Krylov method multiplies with the FP64 finest matrix
   PMG_TRY(sell_values<double>(h, h.lv.back()));
@@ -929,7 +918,6 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
   if (sol_host) PMG_CUDA(cudaMemcpyAsync(sol_host, h.sol.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
   PMG_CUDA(cudaStreamSynchronize(s));
   PMG_TRY(coarse_cycle_check(h));
-  PMG_TRY(region_check(h));
   if (st) {
     st->iterations = iters;
     st->res0 = res0;
@@ -1152,7 +1140,6 @@ int solve_dd(Handle &h, const pmg_comm *comm, double *sol_host, const double *rh
   if (sol_host) PMG_CUDA(cudaMemcpyAsync(sol_host, h.sol.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
   PMG_CUDA(cudaStreamSynchronize(s));
   PMG_TRY(coarse_cycle_check(h));
-  PMG_TRY(region_check(h));
   if (st) {
     st->iterations = iters;
     st->res0 = res0;
