@@ -213,6 +213,11 @@ int pmg_create(pmg_handle *out, int n_levels, const pmg_params *p) {
   }
   for (int k = 0; k < 10; k++) cudaEventCreate(&h->ev[k]);
   int rc = h->d_flags.alloc(4);
+  if (rc == PMG_OK && cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking) != cudaSuccess) rc = PMG_ERR_CUDA;
+  for (int k = 0; k < 2 && rc == PMG_OK; k++)
+    if (cudaEventCreateWithFlags(&h->aux_ev[k], cudaEventDisableTiming) != cudaSuccess) rc = PMG_ERR_CUDA;
+  if (rc == PMG_OK) rc = h->coarse_flags.alloc(4);
+  if (rc == PMG_OK && cudaMallocHost(&h->h_coarse_flags, sizeof(int) * 4) != cudaSuccess) rc = PMG_ERR_CUDA;
   if (rc == PMG_OK) rc = h->red_partial.alloc(1024);
   if (rc == PMG_OK) rc = h->red_counter.alloc(1);
   if (rc == PMG_OK && cudaMemset(h->red_counter.p, 0, sizeof(unsigned)) != cudaSuccess) rc = PMG_ERR_CUDA;
@@ -233,11 +238,15 @@ int pmg_destroy(pmg_handle hh) {
   Handle *h = H(hh);
   if (!h) return PMG_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->aux) cudaStreamSynchronize(h->aux);
   if (h->vgraph) cudaGraphExecDestroy(h->vgraph);
   if (h->vgraph_ssor) cudaGraphExecDestroy(h->vgraph_ssor);
   for (int k = 0; k < 10; k++) if (h->ev[k]) cudaEventDestroy(h->ev[k]);
   if (h->h_H) cudaFreeHost(h->h_H);
+  if (h->h_coarse_flags) cudaFreeHost(h->h_coarse_flags);
+  for (int k = 0; k < 2; k++) if (h->aux_ev[k]) cudaEventDestroy(h->aux_ev[k]);
   h->lv.clear();
+  if (h->aux) cudaStreamDestroy(h->aux);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return PMG_OK;

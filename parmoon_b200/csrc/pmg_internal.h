@@ -194,6 +194,11 @@ struct Handle {
   DBuf<double> d_modes;
   std::vector<Level> lv;
   cudaStream_t stream = nullptr;
+  // auxiliary stream: the coarsest-level factorisation overlaps the per-solve set-up
+  cudaStream_t aux = nullptr;
+  cudaEvent_t aux_ev[2] = {nullptr, nullptr};
+  DBuf<int> coarse_flags;
+  int *h_coarse_flags = nullptr;  // page-locked, 4 ints
   int device = 0;
   int num_sms = 148;
   // coarsest-level dense inverse (FP64)

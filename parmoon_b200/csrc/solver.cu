@@ -287,7 +287,9 @@ __global__ void k_csr_to_dense_active(int na, const int *__restrict__ rp, const 
     if (kc[k] < na) D[(size_t)i * na + kc[k]] = a[k];
 }
 
-int coarse_factor(Handle &h) {
+// the launches of the factorisation on stream s; the pivot flags are copied
+// to h.h_coarse_flags (page-locked) on s, read by coarse_factor_finish
+static int coarse_factor_launch(Handle &h, cudaStream_t s) {
   Level &L = h.lv[0];
   // Dirichlet rows are identity rows, so only the active block is factored:
   // x_a = A_aa^{-1} (f_a - A_ad f_d), x_d = f_d
@@ -298,14 +300,14 @@ int coarse_factor(Handle &h) {
   }
   PMG_TRY(h.coarse_t.alloc(std::max(n, 1)));
   if (n == 0) {
-    h.coarse_ready = true;
+    h.h_coarse_flags[0] = 0;
     return PMG_OK;
   }
   PMG_TRY(h.coarse_lu.alloc((size_t)n * n));
   PMG_TRY(h.coarse_inv.alloc((size_t)n * n));
   PMG_TRY(h.coarse_piv.alloc(n));
-  PMG_CUDA(cudaMemsetAsync(h.d_flags.p, 0, sizeof(int) * 4, h.stream));
-  k_csr_to_dense_active<<<n, 256, 0, h.stream>>>(n, L.rowptr.p, L.kcol.p, L.A.p, h.coarse_lu.p); count_launches(1);
+  PMG_CUDA(cudaMemsetAsync(h.coarse_flags.p, 0, sizeof(int) * 4, s));
+  k_csr_to_dense_active<<<n, 256, 0, s>>>(n, L.rowptr.p, L.kcol.p, L.A.p, h.coarse_lu.p); count_launches(1);
   static bool attr = false;
   if (!attr) {
     PMG_CUDA(cudaFuncSetAttribute(k_lu_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, LU_MAX_N * (LU_NB + 1) * 8));
@@ -315,32 +317,41 @@ int coarse_factor(Handle &h) {
   }
   for (int k0 = 0; k0 < n; k0 += LU_NB) {
     const int nb = std::min(LU_NB, n - k0);
-    k_lu_panel<<<1, 1024, (size_t)(n - k0) * (nb + 1) * 8, h.stream>>>(n, k0, nb, h.coarse_lu.p, h.coarse_piv.p, h.d_flags.p);
-    k_lu_swap<<<(n + 255) / 256, 256, 0, h.stream>>>(n, k0, nb, h.coarse_lu.p, h.coarse_piv.p);
+    k_lu_panel<<<1, 1024, (size_t)(n - k0) * (nb + 1) * 8, s>>>(n, k0, nb, h.coarse_lu.p, h.coarse_piv.p, h.coarse_flags.p);
+    k_lu_swap<<<(n + 255) / 256, 256, 0, s>>>(n, k0, nb, h.coarse_lu.p, h.coarse_piv.p);
     count_launches(2);
     const int rest = n - k0 - nb;
     if (rest > 0) {
-      k_lu_trsm<<<(rest + 127) / 128, 128, 0, h.stream>>>(n, k0, nb, h.coarse_lu.p);
+      k_lu_trsm<<<(rest + 127) / 128, 128, 0, s>>>(n, k0, nb, h.coarse_lu.p);
       dim3 g((rest + 31) / 32, (rest + 31) / 32);
-      k_lu_gemm<<<g, 256, 0, h.stream>>>(n, k0, nb, h.coarse_lu.p);
+      k_lu_gemm<<<g, 256, 0, s>>>(n, k0, nb, h.coarse_lu.p);
       count_launches(2);
     }
   }
   PMG_TRY(h.coarse_perm.alloc(n));
-  k_lu_perm_identity<<<1, 32, 0, h.stream>>>(n, h.coarse_piv.p, h.coarse_perm.p);
-  k_lu_inverse_slab<<<(n + INV_COLS - 1) / INV_COLS, INV_THREADS, (size_t)n * 2 * INV_COLS * 8, h.stream>>>(
+  k_lu_perm_identity<<<1, 32, 0, s>>>(n, h.coarse_piv.p, h.coarse_perm.p);
+  k_lu_inverse_slab<<<(n + INV_COLS - 1) / INV_COLS, INV_THREADS, (size_t)n * 2 * INV_COLS * 8, s>>>(
       n, h.coarse_lu.p, h.coarse_perm.p, h.coarse_inv.p);
   count_launches(2);
   PMG_CUDA(cudaGetLastError());
-  int flags[4];
-  PMG_CUDA(cudaMemcpyAsync(flags, h.d_flags.p, sizeof(flags), cudaMemcpyDeviceToHost, h.stream));
-  PMG_CUDA(cudaStreamSynchronize(h.stream));
-  if (flags[0] & 16) {
+  PMG_CUDA(cudaMemcpyAsync(h.h_coarse_flags, h.coarse_flags.p, sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
+  return PMG_OK;
+}
+
+// after the launches completed (the caller synchronised s): the pivot check
+static int coarse_factor_finish(Handle &h) {
+  if (h.lv[0].Na > 0 && (h.h_coarse_flags[0] & 16)) {
     set_error("zero pivot in the coarsest-level factorisation");
     return PMG_ERR_SINGULAR;
   }
   h.coarse_ready = true;
   return PMG_OK;
+}
+
+int coarse_factor(Handle &h) {
+  PMG_TRY(coarse_factor_launch(h, h.stream));
+  PMG_CUDA(cudaStreamSynchronize(h.stream));
+  return coarse_factor_finish(h);
 }
 
 // ----------------------------------------------------------------- V-cycle
@@ -633,44 +644,66 @@ __global__ void k_prec_out32(int N, const float *__restrict__ x, double *z) {
 
 static int prepare_levels(Handle &h) {
   bool fp32 = h.prm.precision == PMG_PREC_FP32;
-  for (size_t i = 0; i < h.lv.size(); i++) {
-    Level &L = h.lv[i];
-    if (!L.assembled) {
-      set_error("solve: every level must be assembled (pmg_assemble) first");
-      return PMG_ERR_STATE;
-    }
-    if (i > 0 && !L.has_P) {
-      set_error("solve: missing transfer (pmg_set_transfer) for a level");
-      return PMG_ERR_STATE;
-    }
-    PMG_TRY(L.x64.alloc(L.N)); PMG_TRY(L.f64.alloc(L.N)); PMG_TRY(L.d64.alloc(L.N));
-    const bool slc = i > 0 && (h.prm.slc_all || (h.prm.slc_fine && i + 1 == h.lv.size()));
-    const bool jac = h.prm.smoother == PMG_SMOOTHER_JACOBI || (i == 0 && h.prm.coarse_smoother == PMG_COARSE_JACOBI);
-    for (int k = 0; k < 3 && slc; k++) PMG_TRY(fp32 ? L.slc32[k].alloc(L.N) : L.slc64[k].alloc(L.N));
-    if (jac) PMG_TRY(fp32 ? L.jac32.alloc(L.N) : L.jac64.alloc(L.N));
-    if (fp32) {
-      PMG_TRY(sell_values<float>(h, L));
-      PMG_TRY(L.x32.alloc(L.N)); PMG_TRY(L.f32.alloc(L.N)); PMG_TRY(L.d32.alloc(L.N));
-      if (i > 0 && !L.pval32.p) {
-        PMG_TRY(L.pval32.alloc(L.pval.n));
-        PMG_TRY(convert_f64_f32(h.stream, L.pval.p, L.pval32.p, L.pval.n));
-        PMG_TRY(L.rval32.alloc(L.rval.n));
-        PMG_TRY(convert_f64_f32(h.stream, L.rval.p, L.rval32.p, L.rval.n));
+  // the coarsest level's LU and inverse run on the auxiliary stream while the
+  // level loop below converts the SELL values on the main stream; every path
+  // out of here joins the two streams first
+  const bool factor = h.prm.coarse_smoother == PMG_COARSE_DIRECT && !h.coarse_ready && h.lv[0].assembled;
+  int frc = PMG_OK;
+  if (factor) {
+    PMG_CUDA(cudaEventRecord(h.aux_ev[0], h.stream));
+    PMG_CUDA(cudaStreamWaitEvent(h.aux, h.aux_ev[0], 0));
+    frc = coarse_factor_launch(h, h.aux);
+    PMG_CUDA(cudaEventRecord(h.aux_ev[1], h.aux));
+  }
+  auto body = [&]() -> int {
+    PMG_TRY(frc);
+    for (size_t i = 0; i < h.lv.size(); i++) {
+      Level &L = h.lv[i];
+      if (!L.assembled) {
+        set_error("solve: every level must be assembled (pmg_assemble) first");
+        return PMG_ERR_STATE;
       }
-    } else {
-      PMG_TRY(sell_values<double>(h, L));
+      if (i > 0 && !L.has_P) {
+        set_error("solve: missing transfer (pmg_set_transfer) for a level");
+        return PMG_ERR_STATE;
+      }
+      PMG_TRY(L.x64.alloc(L.N)); PMG_TRY(L.f64.alloc(L.N)); PMG_TRY(L.d64.alloc(L.N));
+      const bool slc = i > 0 && (h.prm.slc_all || (h.prm.slc_fine && i + 1 == h.lv.size()));
+      const bool jac = h.prm.smoother == PMG_SMOOTHER_JACOBI || (i == 0 && h.prm.coarse_smoother == PMG_COARSE_JACOBI);
+      for (int k = 0; k < 3 && slc; k++) PMG_TRY(fp32 ? L.slc32[k].alloc(L.N) : L.slc64[k].alloc(L.N));
+      if (jac) PMG_TRY(fp32 ? L.jac32.alloc(L.N) : L.jac64.alloc(L.N));
+      if (fp32) {
+        PMG_TRY(sell_values<float>(h, L));
+        PMG_TRY(L.x32.alloc(L.N)); PMG_TRY(L.f32.alloc(L.N)); PMG_TRY(L.d32.alloc(L.N));
+        if (i > 0 && !L.pval32.p) {
+          PMG_TRY(L.pval32.alloc(L.pval.n));
+          PMG_TRY(convert_f64_f32(h.stream, L.pval.p, L.pval32.p, L.pval.n));
+          PMG_TRY(L.rval32.alloc(L.rval.n));
+          PMG_TRY(convert_f64_f32(h.stream, L.rval.p, L.rval32.p, L.rval.n));
+        }
+      } else {
+        PMG_TRY(sell_values<double>(h, L));
+      }
     }
+    // the outer Krylov method multiplies with the FP64 finest matrix
+    PMG_TRY(sell_values<double>(h, h.lv.back()));
+    if (h.prm.slc_all || h.prm.slc_fine) PMG_TRY(h.slc_part.alloc(2 * SLC_BLOCKS + 1));
+    if (h.prm.coarse_smoother != PMG_COARSE_DIRECT) {
+      // colour pointers of the coarsest level's row list, and the Jacobi scratch
+      const Level &C = h.lv[0];
+      PMG_TRY(h.coarse_cptr.upload(C.rcolor_ptr.data(), C.rcolor_ptr.size(), h.stream));
+      PMG_TRY(h.coarse_t.alloc(std::max(C.N, 1)));
+    }
+    if (h.prm.smoother == PMG_SMOOTHER_LEARNED) PMG_TRY(learned_prepare(h));
+    return PMG_OK;
+  };
+  int rc = body();
+  if (factor) {
+    PMG_CUDA(cudaStreamWaitEvent(h.stream, h.aux_ev[1], 0));
+    PMG_CUDA(cudaEventSynchronize(h.aux_ev[1]));
+    if (rc == PMG_OK) rc = coarse_factor_finish(h);
   }
-  // the outer Krylov method multiplies with the FP64 finest matrix
-  PMG_TRY(sell_values<double>(h, h.lv.back()));
-  if (h.prm.slc_all || h.prm.slc_fine) PMG_TRY(h.slc_part.alloc(2 * SLC_BLOCKS + 1));
-  if (h.prm.coarse_smoother != PMG_COARSE_DIRECT) {
-    // colour pointers of the coarsest level's row list, and the Jacobi scratch
-    const Level &C = h.lv[0];
-    PMG_TRY(h.coarse_cptr.upload(C.rcolor_ptr.data(), C.rcolor_ptr.size(), h.stream));
-    PMG_TRY(h.coarse_t.alloc(std::max(C.N, 1)));
-  }
-  if (h.prm.smoother == PMG_SMOOTHER_LEARNED) PMG_TRY(learned_prepare(h));
+  PMG_TRY(rc);
   if (h.prm.coarse_smoother == PMG_COARSE_DIRECT && !h.coarse_ready) PMG_TRY(coarse_factor(h));
   const int cc = coarse_cycle_top(h);
   if (cc != h.cc_top) {
