@@ -569,8 +569,8 @@ __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, dou
 // into per-cell buffers.  k_assemble_tc16 (per colour) then only contracts and
 // scatters: per 8 cells a warp loads its B fragments straight from d (8 cells
 // x 4 consecutive k per load), runs the 4-step mma chain per 8-entry block, and
-// adds the local rhs of its cells.  Shared memory holds the table alone, so
-// two blocks of 16 warps fit on an SM even for Q2 (94 KB).
+// adds the local rhs of its cells.  Shared memory holds the table alone
+// (94 KB for Q2).
 template <int E, int NQ>
 __global__ void __launch_bounds__(128) k_tc_setup(AsmArgs a, double *__restrict__ dbuf, double *__restrict__ rbuf,
                                                   const double *__restrict__ rtab) {
@@ -662,14 +662,18 @@ __global__ void __launch_bounds__(128) k_tc_setup_diff(AsmArgs a, double *__rest
   }
 }
 
+// Slot loads of the next MB = 8 entry blocks are in flight while the current
+// ones contract (one 512-thread block per SM, up to 128 registers): measured
+// on the 64^3 Q2 finest level 1.75 -> 1.67 ms against MB = 4 with two blocks
+// per SM (the same loads in flight per SM, half the dependent steps per warp).
 // KS k-steps of 4: KS = 4 for space-constant coefficients (d = the 16
 // coefficients of D), KS = ceil(6 NQ / 4) for pure diffusion (d = the 6
 // entries of w_q |det J| eps(x_q) K per quadrature point, zero-padded)
 template <int E, int KS>
-__global__ void __launch_bounds__(512, 2) k_assemble_tc16(AsmArgs a, const double *__restrict__ tfrag,
+__global__ void __launch_bounds__(512, 1) k_assemble_tc16(AsmArgs a, const double *__restrict__ tfrag,
                                                           const double *__restrict__ dbuf,
                                                           const double *__restrict__ rbuf) {
-  constexpr int NLOC = ET<E>::NLOC, NN = NLOC * NLOC, MT = (NN + 7) / 8, MB = 4, KP = 4 * KS;
+  constexpr int NLOC = ET<E>::NLOC, NN = NLOC * NLOC, MT = (NN + 7) / 8, MB = 8, KP = 4 * KS;
   extern __shared__ double sT[];
   for (int k = threadIdx.x; k < MT * KS * 32; k += blockDim.x) sT[k] = tfrag[k];
   __syncthreads();
