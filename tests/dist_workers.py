@@ -47,6 +47,53 @@ def dp_training(rank, world, port, out_dir):
     dist.destroy_process_group()
 
 
+def learned_problem(seed):
+    """A 3^3-cell Q1 SUPG problem with a curl-field convection and one (e, r) pair (oracle only)."""
+    from oracle import cd3d as O
+    m = O.struct_mesh(O.Q1, 3)
+    rp, kc = O.csr(m["elem_dof"], 8, m["N"], m["active_bound"])
+    rng = np.random.default_rng(seed)
+    modes = np.zeros((2, 8))
+    modes[:, 0:3] = [[1, 0, 1], [0, 1, 1]]
+    modes[:, 3] = [0.7, -0.4]
+    modes[:, 4] = rng.uniform(0, 6, 2)
+    modes[:, 5:8] = rng.normal(size=(2, 3))
+    A, _ = O.assemble(O.Q1, m["elem_dof"], m["cell_vert"], m["N"], m["active_bound"], rp, kc, O.FORM_SUPG,
+                      O.make_coeff(kind=O.COEF_CURL_FOURIER, eps=1e-3, b=(3.0, 0, 0), f=1.0, modes=modes), quad=2,
+                      dir_values=np.zeros(m["N"] - m["active_bound"]))
+    N, Na = m["N"], m["active_bound"]
+    e = rng.standard_normal(N)
+    e[Na:] = 0
+    Ad = np.zeros((N, N))
+    Ad[np.repeat(np.arange(N), np.diff(rp)), kc] = A
+    return m, rp, kc, A, e, Ad @ e
+
+
+def dp_learned(rank, world, port, out_dir):
+    """Data-parallel training of the stencil network with the oracle's gradient
+    (BF16 forward rounding included): each rank its own problem, the gradients
+    averaged over the ranks by train_data_parallel, the same plain update on
+    every rank."""
+    sys.path.insert(0, ROOT)
+    dist = init(rank, world, port)
+    from parmoon_b200 import learned as PL
+    from oracle import learned_oracle as LO
+    m, rp, kc, A, e, r = learned_problem(100 + rank)
+    state = {"w": PL.init_weights(0).astype(np.float32)}
+
+    def grad_fn(it):
+        loss, g = LO.loss_and_grad(LO.bf16_round(state["w"]), 4, rp, kc, A, m["active_bound"], m["dof_lat"], e, r)
+        return loss, g.astype(np.float32)
+
+    def apply_fn(g):
+        state["w"] = (state["w"] - 0.05 * g).astype(np.float32)
+
+    hist = PL.train_data_parallel(grad_fn, apply_fn, 3, dist)
+    np.savez(os.path.join(out_dir, f"learned{rank}.npz"), w=state["w"], hist=np.array(hist))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def dd_partition(rank, world, port, out_dir, elem, n, nl):
     """Subdomain of this rank (parmoon_b200.dd): halo exchange of a global
     vector through gloo, and the owned rows of the subdomain pattern mapped

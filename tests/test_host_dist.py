@@ -1,5 +1,6 @@
 """Host logic of the multi-process paths on CPU (gloo, world size 2): the
-gradient average of data-parallel training of the learned smoother, the
+gradient average of data-parallel training of the learned smoother (on a toy
+quadratic and on the stencil network's own gradient, from the oracle), the
 identical updates it leads to on every rank, the max-over-ranks timing of
 bench.py, and the subdomains of the domain-decomposed solve.  No GPU."""
 import os
@@ -65,3 +66,25 @@ def test_subdomains_partition_and_halo(tmp_path, elem, n, nl):
     for x in r:
         assert np.array_equal(x["x"], x["ref"][x["glob"]])  # ghosts filled from their owners
         assert int(x["bad_rows"]) == 0
+
+
+def test_data_parallel_stencil_network_gradient(tmp_path):
+    """Two ranks, each with its own problem, train the stencil network on the
+    averaged gradient: both end with the same weights, equal to one process
+    that applies the mean of the two ranks' gradients."""
+    from oracle import learned_oracle as LO
+    from parmoon_b200 import learned as PL
+    world = 2
+    mp.start_processes(W.dp_learned, args=(world, free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    r = [np.load(os.path.join(tmp_path, f"learned{k}.npz")) for k in range(world)]
+    assert np.array_equal(r[0]["w"], r[1]["w"])
+    probs = [W.learned_problem(100 + k) for k in range(world)]
+    w = PL.init_weights(0).astype(np.float32)
+    for _ in range(3):
+        gs = []
+        for m, rp, kc, A, e, rr in probs:
+            _, g = LO.loss_and_grad(LO.bf16_round(w), 4, rp, kc, A, m["active_bound"], m["dof_lat"], e, rr)
+            gs.append(g.astype(np.float32))
+        w = (w - 0.05 * np.mean(np.stack(gs), axis=0).astype(np.float32)).astype(np.float32)
+    assert np.allclose(r[0]["w"], w, rtol=1e-5, atol=1e-7)
