@@ -215,6 +215,7 @@ struct AsmArgs {
   const double *utab;  // NQ x NLOC x 4
   const double *qtab;  // NQ x 4 : weight, xi, eta, zeta
   int *flags;
+  int item_chunk;  // k_assemble_tc16: consecutive work items per warp
 };
 
 // affine map of a cell (HexaAffin on vertices 0, 1, 3, 4 over [-1,1]^3;
@@ -625,47 +626,59 @@ __global__ void __launch_bounds__(128) k_tc_setup(AsmArgs a, double *__restrict_
 }
 
 // Pure diffusion with a coefficient eps(x) (b = 0, c = 0): one thread per
-// cell evaluates eps at the cell's NQ quadrature points (all lanes busy, the
-// Fourier modes of the field read through the cache) and stores
+// quadrature point (a block holds CB = 128 / NQ whole cells) evaluates eps and
+// f there (the Fourier modes of the field read through the cache) and stores
 // d[(q, p)] = w_q |det J| eps(x_q) K_p (K = Ji Ji^T, p over 00 11 22 01 02 12,
-// zero-padded to 4 KS) and the local rhs r_i = sum_q w_q |det J| f(x_q) u_i(q);
-// k_assemble_tc16<E, KS> then contracts with the per-point table on DMMA.
+// zero-padded to 4 KS); then the block's threads form the cells' local rhs
+// r_i = sum_q w_q |det J| f(x_q) u_i(q) from the point weights in shared
+// memory.  k_assemble_tc16<E, KS> contracts d with the per-point table on DMMA.
+// A thread per point keeps one point's mode chain per thread: the coarse
+// levels' few cells finish in one chain of n_modes terms instead of NQ.
 template <int E, int NQ>
 __global__ void __launch_bounds__(128) k_tc_setup_diff(AsmArgs a, double *__restrict__ dbuf, double *__restrict__ rbuf) {
-  constexpr int NLOC = ET<E>::NLOC, NV = ET<E>::NV, KD = 6 * NQ, KP = 4 * ((KD + 3) / 4);
+  constexpr int NLOC = ET<E>::NLOC, NV = ET<E>::NV, KD = 6 * NQ, KP = 4 * ((KD + 3) / 4), CB = 128 / NQ;
   constexpr bool HEX = ET<E>::HEX;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= a.n_elems) return;
-  const double *cv = a.cell_vert + (size_t)e * NV * 3;
-  double J[9], x0[3], Ji[9], K[9], adet;
-  cell_map<HEX>(cv, J, x0, Ji, adet, K);
-  const double Kp[6] = {K[0], K[4], K[8], K[1], K[2], K[5]};
-  double *d = dbuf + (size_t)e * KP;
-  double fw[NQ];
-  for (int q = 0; q < NQ; q++) {
+  __shared__ double sfw[CB * NQ];
+  const int e0 = blockIdx.x * CB, t = threadIdx.x;
+  const int lc = t / NQ, q = t - lc * NQ, e = e0 + lc;
+  if (t < CB * NQ && e < a.n_elems) {
+    const double *cv = a.cell_vert + (size_t)e * NV * 3;
+    double J[9], x0[3], Ji[9], K[9], adet;
+    cell_map<HEX>(cv, J, x0, Ji, adet, K);
+    const double Kp[6] = {K[0], K[4], K[8], K[1], K[2], K[5]};
+    double *d = dbuf + (size_t)e * KP;
     const double *qq = a.qtab + q * 4;
     double cf[7];
     coeff_eval(a.coef, x0[0] + J[0] * qq[1] + J[1] * qq[2] + J[2] * qq[3], x0[1] + J[3] * qq[1] + J[4] * qq[2] + J[5] * qq[3],
                x0[2] + J[6] * qq[1] + J[7] * qq[2] + J[8] * qq[3], cf);
     const double w = qq[0] * adet, ew = w * cf[0];
-    fw[q] = w * cf[5];
+    sfw[t] = w * cf[5];
 #pragma unroll
     for (int p = 0; p < 6; p++) d[q * 6 + p] = ew * Kp[p];
+    if (q == 0)
+      for (int k = KD; k < KP; k++) d[k] = 0.0;
   }
-  for (int k = KD; k < KP; k++) d[k] = 0.0;
   if (!rbuf) return;
-  double *r = rbuf + (size_t)e * NLOC;
-  for (int i = 0; i < NLOC; i++) {
+  __syncthreads();
+  const int nc = min(CB, a.n_elems - e0);
+  for (int idx = t; idx < nc * NLOC; idx += blockDim.x) {
+    const int c = idx / NLOC, i = idx - c * NLOC;
     double acc = 0.0;
-    for (int q = 0; q < NQ; q++) acc += fw[q] * __ldg(a.utab + ((size_t)q * NLOC + i) * 4 + 3);
-    r[i] = acc;
+#pragma unroll
+    for (int p = 0; p < NQ; p++) acc += sfw[c * NQ + p] * __ldg(a.utab + ((size_t)p * NLOC + i) * 4 + 3);
+    rbuf[(size_t)e0 * NLOC + idx] = acc;
   }
 }
 
-// Slot loads of the next MB = 8 entry blocks are in flight while the current
-// ones contract (one 512-thread block per SM, up to 128 registers): measured
-// on the 64^3 Q2 finest level 1.75 -> 1.67 ms against MB = 4 with two blocks
-// per SM (the same loads in flight per SM, half the dependent steps per warp).
+// Work items are (group of 8 cells, batch of MB = 8 entry blocks), NB = MT / MB
+// items per group; warp gw takes items [gw per, (gw + 1) per) with per at most
+// NB, so a coarse level's short launch spreads one group's batches over
+// several warps (a chain of ~3 items instead of NB).  The slot loads (and, for
+// KS = 4, the B fragments) of a warp's next item are in flight while the
+// current one contracts and scatters; one 512-thread block per SM, up to 128
+// registers.  The cells of one launch share no row, so every slot is hit
+// at most once per launch whatever warp handles it: the result is the same
+// for any item order.
 // KS k-steps of 4: KS = 4 for space-constant coefficients (d = the 16
 // coefficients of D), KS = ceil(6 NQ / 4) for pure diffusion (d = the 6
 // entries of w_q |det J| eps(x_q) K per quadrature point, zero-padded)
@@ -673,69 +686,75 @@ template <int E, int KS>
 __global__ void __launch_bounds__(512, 1) k_assemble_tc16(AsmArgs a, const double *__restrict__ tfrag,
                                                           const double *__restrict__ dbuf,
                                                           const double *__restrict__ rbuf) {
-  constexpr int NLOC = ET<E>::NLOC, NN = NLOC * NLOC, MT = (NN + 7) / 8, MB = 8, KP = 4 * KS;
+  constexpr int NLOC = ET<E>::NLOC, NN = NLOC * NLOC, MT = (NN + 7) / 8, MB = 8, NB = (MT + MB - 1) / MB, KP = 4 * KS;
+  // B fragments d[cell row][4 s + lane % 4]: held in registers for KS = 4,
+  // re-read through L1 per entry block for the longer diffusion rows
+  constexpr bool REG = KS <= 4;
+  constexpr int NBF = REG ? KS : 1;
   extern __shared__ double sT[];
   for (int k = threadIdx.x; k < MT * KS * 32; k += blockDim.x) sT[k] = tfrag[k];
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  const int row = lane >> 2, c0 = 2 * (lane & 3);
-  for (int base = (blockIdx.x * nwarps + warp) * 8; base < a.n_elems; base += gridDim.x * nwarps * 8) {
-    const int ne = min(8, a.n_elems - base);
-    // B fragments: d[cell row][4 s + lane % 4]; held in registers for KS = 4,
-    // re-read through L1 per entry block for the longer diffusion rows (the
-    // 64-register budget of two 512-thread blocks per SM)
-    constexpr bool REG = KS <= 4;
+  const int lane = threadIdx.x & 31, row = lane >> 2, c0 = 2 * (lane & 3);
+  const int n_items = ((a.n_elems + 7) >> 3) * NB, per = a.item_chunk;  // items [gw per, (gw + 1) per)
+  const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int item_end = min(n_items, (gw + 1) * per);
+  auto load = [&](int it, int (&sl)[MB][2], double (&bf)[NBF]) {
+    const int base = (it / NB) * 8, t0 = (it % NB) * MB, ne = min(8, a.n_elems - base);
+#pragma unroll
+    for (int b = 0; b < MB; b++) {
+      const int m = 8 * (t0 + b) + row;
+#pragma unroll
+      for (int u = 0; u < 2; u++)
+        sl[b][u] = (t0 + b < MT && m < NN && c0 + u < ne) ? __ldg(a.slot + (size_t)(base + c0 + u) * NN + m) : -1;
+    }
+    if (REG) {
+      const double *drow = dbuf + (size_t)(base + (row < ne ? row : 0)) * KP + (lane & 3);
+#pragma unroll
+      for (int s = 0; s < NBF; s++) bf[s] = row < ne ? __ldg(drow + 4 * s) : 0.0;
+    }
+  };
+  int slc[MB][2], sln[MB][2];
+  double bfc[NBF], bfn[NBF];
+  int item = gw * per;
+  if (item < item_end) load(item, slc, bfc);
+  for (; item < item_end; item++) {
+    if (item + 1 < item_end) load(item + 1, sln, bfn);
+    const int base = (item / NB) * 8, t0 = (item % NB) * MB, ne = min(8, a.n_elems - base);
     const double *drow = dbuf + (size_t)(base + (row < ne ? row : 0)) * KP + (lane & 3);
-    double bf[REG ? KS : 1];
+    double acc[MB][2];
 #pragma unroll
-    for (int s = 0; s < (REG ? KS : 1); s++) bf[s] = row < ne ? __ldg(drow + 4 * s) : 0.0;
-    auto load_slots = [&](int t0, int (&sl)[MB][2]) {
+    for (int b = 0; b < MB; b++) {
+      acc[b][0] = 0.0;
+      acc[b][1] = 0.0;
+      if (t0 + b < MT) {
+        const double *tb = sT + (size_t)(t0 + b) * KS * 32 + lane;
 #pragma unroll
-      for (int b = 0; b < MB; b++) {
-        const int m = 8 * (t0 + b) + row;
-#pragma unroll
-        for (int u = 0; u < 2; u++)
-          sl[b][u] = (t0 + b < MT && m < NN && c0 + u < ne) ? __ldg(a.slot + (size_t)(base + c0 + u) * NN + m) : -1;
-      }
-    };
-    int slc[MB][2], sln[MB][2];
-    load_slots(0, slc);
-    for (int t0 = 0; t0 < MT; t0 += MB) {
-      if (t0 + MB < MT) load_slots(t0 + MB, sln);
-      double acc[MB][2];
-#pragma unroll
-      for (int b = 0; b < MB; b++) {
-        acc[b][0] = 0.0;
-        acc[b][1] = 0.0;
-        if (t0 + b < MT) {
-          const double *tb = sT + (size_t)(t0 + b) * KS * 32 + lane;
-#pragma unroll
-          for (int s = 0; s < KS; s++)
-            dmma_8x8x4(acc[b][0], acc[b][1], tb[s * 32], REG ? bf[REG ? s : 0] : (row < ne ? __ldg(drow + 4 * s) : 0.0));
-        }
-      }
-      // L2 reductions (no value returned): the cells of one launch share no
-      // row, so no two adds of a launch meet and the order is the launch order
-#pragma unroll
-      for (int b = 0; b < MB; b++)
-#pragma unroll
-        for (int u = 0; u < 2; u++) {
-          const int q = slc[b][u];
-          if (q >= 0) scatter_entry(a.entries, q, acc[b][u]);
-          else if (q <= -3) a.entries[-3 - q] = 1.0;  // Dirichlet row: unit diagonal (AssembleMat3D.C:840-848)
-        }
-#pragma unroll
-      for (int b = 0; b < MB; b++) {
-        slc[b][0] = sln[b][0];
-        slc[b][1] = sln[b][1];
+        for (int s = 0; s < KS; s++)
+          dmma_8x8x4(acc[b][0], acc[b][1], tb[s * 32], REG ? bfc[REG ? s : 0] : (row < ne ? __ldg(drow + 4 * s) : 0.0));
       }
     }
-    // the cells' local rhs (active rows)
-    if (a.rhs)
+    // L2 reductions (no value returned)
+#pragma unroll
+    for (int b = 0; b < MB; b++)
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const int q = slc[b][u];
+        if (q >= 0) scatter_entry(a.entries, q, acc[b][u]);
+        else if (q <= -3) a.entries[-3 - q] = 1.0;  // Dirichlet row: unit diagonal (AssembleMat3D.C:840-848)
+      }
+    // the cells' local rhs (active rows), once per group
+    if (a.rhs && t0 == 0)
       for (int ci = lane; ci < ne * NLOC; ci += 32) {
         const int di = __ldg(a.elem_dof + (size_t)base * NLOC + ci);
         if (di < a.Na) atomicAdd(a.rhs + di, __ldg(rbuf + (size_t)base * NLOC + ci));
       }
+#pragma unroll
+    for (int b = 0; b < MB; b++) {
+      slc[b][0] = sln[b][0];
+      slc[b][1] = sln[b][1];
+    }
+#pragma unroll
+    for (int s = 0; s < NBF; s++) bfc[s] = bfn[s];
   }
 }
 
@@ -950,12 +969,13 @@ static int launch_assemble_cc(Handle &h, Level &L, AsmArgs a, const double *stab
 // the per-colour contraction launches over the per-cell data in h.tc_dbuf / h.tc_rbuf
 template <int E, int KS>
 static int launch_contract(Handle &h, Level &L, AsmArgs a, const double *tfrag) {
-  constexpr int NLOC = ET<E>::NLOC, NN = NLOC * NLOC, MT = (NN + 7) / 8, WARPS = 16;
+  constexpr int NLOC = ET<E>::NLOC, NN = NLOC * NLOC, MT = (NN + 7) / 8, NB = (MT + 7) / 8, WARPS = 16;
   const size_t smem = sizeof(double) * (size_t)MT * KS * 32;
-  static bool attr_set = false;
-  if (!attr_set) {
+  static int per_sm = 0;  // resident blocks per SM: the grid never exceeds one wave
+  if (!per_sm) {
     PMG_CUDA(cudaFuncSetAttribute(k_assemble_tc16<E, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set = true;
+    PMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_assemble_tc16<E, KS>, WARPS * 32, smem));
+    if (per_sm < 1) per_sm = 1;
   }
   for (size_t c = 0; c + 1 < L.ecolor_ptr.size(); c++) {
     const int beg = L.ecolor_ptr[c], n = L.ecolor_ptr[c + 1] - beg;
@@ -964,7 +984,15 @@ static int launch_contract(Handle &h, Level &L, AsmArgs a, const double *tfrag) 
     b.n_elems = n;
     b.elem_dof = a.elem_dof + (size_t)beg * NLOC;
     b.slot = a.slot + (size_t)beg * NN;
-    const int blocks = std::min((n + WARPS * 8 - 1) / (WARPS * 8), 2 * h.num_sms);
+    // items per warp: spread a short colour over all resident warps, but give
+    // a warp at most one group's NB items (a long colour runs in several
+    // waves of one group per warp: measured 1.651 ms on the 64^3 Q2 finest
+    // level, against 1.701 ms with one wave of ~21 items per warp)
+    const int items = (n + 7) / 8 * NB;
+    const int rw = per_sm * h.num_sms * WARPS;
+    const int per = std::min((items + rw - 1) / rw, NB);
+    b.item_chunk = per;
+    const int blocks = ((items + per - 1) / per + WARPS - 1) / WARPS;
     k_assemble_tc16<E, KS><<<blocks, WARPS * 32, smem, h.stream>>>(b, tfrag, h.tc_dbuf.p + (size_t)beg * 4 * KS,
                                                                    h.tc_rbuf.p + (size_t)beg * NLOC);
     count_launches(1);
@@ -1000,7 +1028,8 @@ static int launch_assemble_diff(Handle &h, Level &L, AsmArgs a, const double *tf
   PMG_TRY(h.tc_rbuf.reserve((size_t)L.n_cells * NLOC));
   AsmArgs all = a;
   all.n_elems = L.n_cells;
-  k_tc_setup_diff<E, NQ><<<(L.n_cells + 127) / 128, 128, 0, h.stream>>>(all, h.tc_dbuf.p, a.rhs ? h.tc_rbuf.p : nullptr);
+  constexpr int CB = 128 / NQ;
+  k_tc_setup_diff<E, NQ><<<(L.n_cells + CB - 1) / CB, 128, 0, h.stream>>>(all, h.tc_dbuf.p, a.rhs ? h.tc_rbuf.p : nullptr);
   count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return launch_contract<E, KS>(h, L, a, tfrag);
@@ -1044,7 +1073,6 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
   }
   PMG_CUDA(cudaMemsetAsync(target, 0, sizeof(double) * L.nnz, h.stream));  // TAssembleMat3D::Reset
   if (rhs_target && zero_rhs) PMG_CUDA(cudaMemsetAsync(rhs_target, 0, sizeof(double) * L.N, h.stream));
-  PMG_CUDA(cudaMemsetAsync(h.d_flags.p, 0, sizeof(int) * 4, h.stream));
   AsmArgs a{};
   a.elem_dof = L.elem_dof.p;
   a.cell_vert = L.cell_vert.p;

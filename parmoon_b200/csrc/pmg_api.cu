@@ -503,10 +503,6 @@ static int assemble_one(Handle *h, int level, int form, double *entries_out, dou
   }
   PMG_TRY(assemble_level(*h, L, form, target, true, L.rhs.p));
   PMG_TRY(set_dirichlet_rows(*h, L, target, L.rhs.p));
-  int flags[4];
-  PMG_CUDA(cudaMemcpyAsync(flags, h->d_flags.p, sizeof(flags), cudaMemcpyDeviceToHost, h->stream));
-  PMG_CUDA(cudaStreamSynchronize(h->stream));
-  if (flags[0] & 1) { set_error("assemble: element coupling missing from the CSR pattern"); return PMG_ERR_SLOT; }
   if (mass && level == (int)h->lv.size() - 1) {
     // f(t_0) of the mass assembly is the first f_old of the theta scheme (AssembleMRhs)
     PMG_TRY(h->tcd_fold.alloc(L.N));
@@ -520,8 +516,7 @@ static int assemble_one(Handle *h, int level, int form, double *entries_out, dou
   }
   if (entries_out) PMG_CUDA(cudaMemcpyAsync(entries_out, target, sizeof(double) * L.nnz, cudaMemcpyDeviceToHost, h->stream));
   if (rhs_out) PMG_CUDA(cudaMemcpyAsync(rhs_out, L.rhs.p, sizeof(double) * L.N, cudaMemcpyDeviceToHost, h->stream));
-  PMG_CUDA(cudaStreamSynchronize(h->stream));
-  return PMG_OK;
+  return PMG_OK;  // pmg_assemble waits for the stream once, after every level
 }
 
 int pmg_assemble(pmg_handle hh, int level, int form, double *entries_out, double *rhs_out) {
