@@ -639,7 +639,7 @@ def run_tcd(steps):
     t = 0.0
     h.set_coefficients(P.coeff(kind=P.COEF_ROTATING, eps=1e-4, f=0.0, t=t))
     h.assemble(-1, P.FORM_MASS_SUPG, copy_out=False)
-    times, its = [], []
+    times, its, t_asm, t_sol = [], [], [], []
     for k in range(steps + 2):
         t += tau
         h.set_coefficients(P.coeff(kind=P.COEF_ROTATING, eps=1e-4, f=0.0, t=t))
@@ -654,10 +654,13 @@ def run_tcd(steps):
             raise RuntimeError(f"tcd: solve status {rc}")
         if k >= 2:
             times.append(t_m + t_a + st.seconds)
+            t_asm.append(t_m + t_a)
+            t_sol.append(st.seconds)
             its.append(st.iterations)
     config_line("tcd_q1_128_cn", {"value": statistics.mean(times), "unit": "s per time step", "steps": steps,
                                   "n_dofs": int(F["N"]), "nnz_fine": int(F["rowptr"][-1]), "levels": nl,
                                   "iterations_mean": float(np.mean(its)),
+                                  "assembly_s": statistics.mean(t_asm), "solve_s": statistics.mean(t_sol),
                                   "projected_200_steps_s": 200 * statistics.mean(times)})
     h.close()
 

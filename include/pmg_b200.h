@@ -140,6 +140,13 @@ typedef struct pmg_params {
                                   smoother and hands back to SSOR as soon as its measured per-cycle
                                   contraction exceeds the plain one; 1: the learned smoother runs in every
                                   cycle (for measuring it alone) */
+    int    assembly_scatter;   /* how local matrices reach the CSR matrix (same sums, same order, bitwise
+                                  equal results): 0 (default) automatic -- the row gather for Q1, N_Q1,
+                                  P1 and P2, the colour scatter for Q2; 1: colour by colour, each colour's
+                                  cells adding into the matrix (TAssembleMat3D::Assemble order); 2: row
+                                  gather -- local matrices of all cells in one pass, then each CSR row
+                                  summed from its cells' rows in colour order and written once (rows up to
+                                  768 / (32 / n_loc) entries; colour scatter otherwise) */
 } pmg_params;
 
 typedef struct pmg_solve_stats {

@@ -43,7 +43,7 @@ class Params(ctypes.Structure):
                 ("precision", _i), ("sdfem_type", _i), ("poly_degree", _i), ("delta0", _d),
                 ("reference_restart_rule", _i), ("problem_linear", _i), ("learned_steps", _i),
                 ("assembly_kernel", _i), ("slc_all", _i), ("slc_fine", _i), ("quad_rule", _i),
-                ("learned_guard_off", _i)]
+                ("learned_guard_off", _i), ("assembly_scatter", _i)]
 
 
 class CoeffDesc(ctypes.Structure):

@@ -80,6 +80,7 @@ static int validate_params(const pmg_params *p) {
   if ((p->slc_all != 0 && p->slc_all != 1) || (p->slc_fine != 0 && p->slc_fine != 1)) return bad("slc_all / slc_fine must be 0 or 1");
   if (p->learned_steps < 0 || p->learned_steps > 64) return bad("learned_steps must be in [0, 64]");
   if (p->learned_guard_off != 0 && p->learned_guard_off != 1) return bad("learned_guard_off must be 0 or 1");
+  if (p->assembly_scatter < 0 || p->assembly_scatter > 2) return bad("assembly_scatter must be 0, 1 or 2");
   if (p->quad_rule != PMG_QUAD_AUTO && p->quad_rule != PMG_QUAD_GAUSS2 && p->quad_rule != PMG_QUAD_GAUSS3 &&
       p->quad_rule != PMG_QUAD_GAUSS4 && p->quad_rule != PMG_QUAD_KEAST4 && p->quad_rule != PMG_QUAD_KEAST5 &&
       p->quad_rule != PMG_QUAD_KEAST11)
@@ -332,6 +333,8 @@ int pmg_set_level_mesh(pmg_handle hh, int level, int elem_type, int n_cells, con
   PMG_TRY(L.elem_dof.upload(ed.data(), ed.size(), h->stream));
   PMG_TRY(L.cell_vert.upload(cv.data(), cv.size(), h->stream));
   L.slot.release();
+  L.inc.release();
+  L.inc_ptr.release();
   PMG_CUDA(cudaStreamSynchronize(h->stream));
   L.has_mesh = true;
   L.assembled = false;
@@ -387,6 +390,8 @@ int pmg_set_level_csr(pmg_handle hh, int level, int n_rows, int active_bound, co
   L.has_csr = true;
   L.has_mesh = false;
   L.slot.release();
+  L.inc.release();
+  L.inc_ptr.release();
   L.assembled = false;
   h->coarse_ready = false;
   invalidate_graphs(h);

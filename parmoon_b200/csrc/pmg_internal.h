@@ -115,6 +115,10 @@ struct Level {
   DBuf<int> elem_dof;       // n_cells x nloc
   DBuf<double> cell_vert;   // n_cells x nvert x 3
   DBuf<int> slot;           // n_cells x nloc x nloc
+  // row gather: the cells holding each dof, as e * nloc + (local index), in
+  // cell (= colour) order; inc_ptr has N + 1 entries; rmax = longest CSR row
+  DBuf<int> inc_ptr, inc;
+  int rmax = 0;
   std::vector<int> ecolor_ptr;  // element colour classes [ecolor_ptr[c], ecolor_ptr[c+1])
   std::vector<int> cell_order;  // colour-sorted position -> caller's cell index
   // tabulated coefficients (PMG_COEF_TABLE): n_cells x ctab_nq x 6, colour order
@@ -227,6 +231,7 @@ struct Handle {
   double t_setup_csr_device = 0, t_setup_csr_install = 0;
   // per-cell coefficients (16) and local rhs of the space-constant tensor-core assembly
   DBuf<double> tc_dbuf, tc_rbuf;
+  DBuf<double> asm_ae, asm_rloc;  // local matrices / rhs of the row-gather assembly
   // V-cycle graph
   cudaGraphExec_t vgraph = nullptr;
   int vgraph_prec = -1;
@@ -260,6 +265,7 @@ int check_matrix(Handle *h, int level, const char *who);
 
 // ------------------------------------------------------------- kernels (assemble.cu)
 int build_slot_map(Handle &h, Level &L);
+int scan_exclusive(cudaStream_t s, int n, const int *in, int *out);
 int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs, double *rhs_target);
 int set_dirichlet_rows(Handle &h, Level &L, double *target, double *rhs_target);
 

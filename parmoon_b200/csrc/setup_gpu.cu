@@ -54,7 +54,7 @@ __global__ void k_scan_add(int n, int *__restrict__ out, const int *__restrict__
 
 // exclusive scan of in[0..n) into out[0..n], out[n] = total; scratch: the
 // block sums (allocated here)
-static int scan_exclusive(cudaStream_t s, int n, const int *in, int *out) {
+int scan_exclusive(cudaStream_t s, int n, const int *in, int *out) {
   const int nb = (n + SCAN_B - 1) / SCAN_B;
   DBuf<int> sums, offs;
   PMG_TRY(sums.alloc(nb + 1));
