@@ -856,6 +856,14 @@ __global__ void k_inc_sort(int N, const int *__restrict__ ptr, int *__restrict__
   }
 }
 
+__global__ void k_slot_gather_order(size_t total, int nloc, const int *__restrict__ inc, const int *__restrict__ slot,
+                                    int *__restrict__ slot_g) {
+  const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= total) return;
+  const size_t p = k / nloc, j = k - p * nloc;
+  slot_g[k] = slot[(size_t)inc[p] * nloc + j];
+}
+
 int build_row_gather(Handle &h, Level &L) {
   const size_t total = (size_t)L.n_cells * L.nloc;
   if (total >= (size_t)INT32_MAX) {
@@ -876,6 +884,11 @@ int build_row_gather(Handle &h, Level &L) {
   k_inc_fill<<<nb, 256, 0, h.stream>>>(total, L.elem_dof.p, cursor.p, L.inc.p); count_launches(1);
   k_inc_sort<<<(L.N + 255) / 256, 256, 0, h.stream>>>(L.N, L.inc_ptr.p, L.inc.p); count_launches(1);
   PMG_CUDA(cudaGetLastError());
+  PMG_TRY(L.slot_g.alloc(total * L.nloc));
+  const size_t tg = total * L.nloc;
+  k_slot_gather_order<<<(unsigned)((tg + 255) / 256), 256, 0, h.stream>>>(tg, L.nloc, L.inc.p, L.slot.p, L.slot_g.p);
+  count_launches(1);
+  PMG_CUDA(cudaGetLastError());
   int rmax = 0;
   for (size_t r = 0; r + 1 < L.h_rowptr.size(); r++) rmax = std::max(rmax, L.h_rowptr[r + 1] - L.h_rowptr[r]);
   L.rmax = rmax;
@@ -890,8 +903,13 @@ int build_row_gather(Handle &h, Level &L) {
 // the row and the active row's rhs once.  Every entry is a sum from zero over
 // the cells in colour order, the order of the colour-by-colour scatter, so the
 // two agree bitwise; the matrix needs no zeroing and no entry is read back.
-// The incident cells' values of a chunk of CH cells are loaded together (one
-// latency per chunk), then added in order with the group in step.
+// The slot map is kept a second time in list order (slot_g), so a row's
+// slots are one contiguous run; the local rows stay in cell order (the first
+// pass writes them in order; storing them in list order instead made that
+// pass scatter and was measured slower: Q2 64^3 finest level 2.57 against
+// 2.06 ms, P2 lognormal 4.72 against 4.45 ms).
+// The values of a chunk of CH cells are loaded together (one latency per
+// chunk), then added in order with the group in step.
 template <int NLOC>
 __global__ void __launch_bounds__(256, (NLOC == 8 || NLOC == 10) ? 3 : 4) k_gather_rows(int N, int Na, int rmax, const int *__restrict__ rowptr,
                                                         const int *__restrict__ inc_ptr, const int *__restrict__ inc,
@@ -935,14 +953,17 @@ __global__ void __launch_bounds__(256, (NLOC == 8 || NLOC == 10) ? 3 : 4) k_gath
       const int fl = k0 == 0 ? cur.fl : ((valid && t < CH && k0 + t < cur.nc) ? __ldg(inc + cur.c0 + k0 + t) : 0);
       // lane t < CH of the group also loads the local rhs of cell k0 + t
       const double rl = (valid && rloc && t < CH && k0 + t < cur.nc) ? __ldcs(rloc + fl) : 0.0;
+      // local row li of cell e (list entry f = e NLOC + li) and its slots,
+      // stored contiguously in list order (positions c0 + k)
       double v[CH];
       int sl[CH];
 #pragma unroll
       for (int j = 0; j < CH; j++) {
-        const int f = __shfl_sync(0xffffffffu, fl, src + j);
         const bool on = valid && k0 + j < cur.nc;
+        const size_t q = (size_t)(cur.c0 + k0 + j) * NLOC + t;
+        const int f = __shfl_sync(0xffffffffu, fl, src + j);
         v[j] = on ? __ldcs(ae + (size_t)f * NLOC + t) : 0.0;
-        sl[j] = on ? __ldg(slot + (size_t)f * NLOC + t) : -1;
+        sl[j] = on ? __ldg(slot + q) : -1;
       }
 #pragma unroll
       for (int j = 0; j < CH; j++) {
@@ -968,7 +989,7 @@ static int launch_gather(Handle &h, Level &L, double *entries, double *rhs, cons
   const size_t smem = sizeof(double) * (size_t)WARPS * GPW * L.rmax;
   const int nb = (int)std::min<long>((L.N + WARPS * GPW - 1) / (WARPS * GPW), (long)h.num_sms * 8);
   k_gather_rows<NLOC><<<nb, WARPS * 32, smem, h.stream>>>(L.N, L.Na, L.rmax, L.rowptr.p, L.inc_ptr.p, L.inc.p,
-                                                          h.asm_ae.p, L.slot.p, rloc, entries, rhs, add_rhs);
+                                                          h.asm_ae.p, L.slot_g.p, rloc, entries, rhs, add_rhs);
   count_launches(1);
   PMG_CUDA(cudaGetLastError());
   return PMG_OK;
@@ -1267,10 +1288,12 @@ int assemble_level(Handle &h, Level &L, int form, double *target, bool zero_rhs,
   // colour-by-colour scatter; the reference-matrix kernel only scatters.
   // Automatic: the gather for the short rows of Q1 / N_Q1 / P1 / P2, whose
   // colour launches each read and write back most of the matrix's sectors;
-  // the scatter for Q2.  Measured on one B200: P2 lognormal 64^3 (5 levels,
-  // 31 colours) 5.62 -> 4.96 ms; Q1 SUPG 128^3 mass + stiffness, per-point
-  // kernel, 7.08 -> 6.48 ms; Q2 SUPG 64^3 finest level 1.66 (scatter) against
-  // 2.36 ms (gather: 0.41 ms local matrices, 1.86 ms row pass).
+  // the scatter for Q2.  Measured on one B200 (scatter -> gather, all
+  // levels): P2 lognormal 64^3 (31 colours per level) 5.63 -> 4.88 ms; Q1
+  // SUPG 128^3 mass + stiffness on the per-point kernel 7.09 -> 6.71 ms; Q1
+  // Poisson 32^3 0.33 -> 0.14 ms; but Q2 SUPG 64^3, finest level, 1.67 ->
+  // 2.06 ms (the DMMA contraction scatters 729 entries per cell at 0.37 of
+  // HBM; the gather's reads of the local rows are scattered).
   bool gather = (h.prm.assembly_scatter == 2 || (h.prm.assembly_scatter == 0 && L.elem != PMG_ELEM_Q2_HEX)) &&
                 h.prm.assembly_kernel != 2;
   if (gather && !L.inc.p) PMG_TRY(build_row_gather(h, L));

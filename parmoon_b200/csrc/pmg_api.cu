@@ -335,6 +335,7 @@ int pmg_set_level_mesh(pmg_handle hh, int level, int elem_type, int n_cells, con
   L.slot.release();
   L.inc.release();
   L.inc_ptr.release();
+  L.slot_g.release();
   PMG_CUDA(cudaStreamSynchronize(h->stream));
   L.has_mesh = true;
   L.assembled = false;
@@ -392,6 +393,7 @@ int pmg_set_level_csr(pmg_handle hh, int level, int n_rows, int active_bound, co
   L.slot.release();
   L.inc.release();
   L.inc_ptr.release();
+  L.slot_g.release();
   L.assembled = false;
   h->coarse_ready = false;
   invalidate_graphs(h);

@@ -116,8 +116,9 @@ struct Level {
   DBuf<double> cell_vert;   // n_cells x nvert x 3
   DBuf<int> slot;           // n_cells x nloc x nloc
   // row gather: the cells holding each dof, as e * nloc + (local index), in
-  // cell (= colour) order; inc_ptr has N + 1 entries; rmax = longest CSR row
-  DBuf<int> inc_ptr, inc;
+  // cell (= colour) order; inc_ptr has N + 1 entries; slot_g[p][j] = the slot
+  // map's row li of cell e at list position p; rmax = longest CSR row
+  DBuf<int> inc_ptr, inc, slot_g;
   int rmax = 0;
   std::vector<int> ecolor_ptr;  // element colour classes [ecolor_ptr[c], ecolor_ptr[c+1])
   std::vector<int> cell_order;  // colour-sorted position -> caller's cell index
