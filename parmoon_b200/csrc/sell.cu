@@ -337,8 +337,8 @@ __global__ void __launch_bounds__(32 * K) k_sell_gs(int s0, int s1, const int *_
 
 // warps per slice for a launch over `slices` slices: the smallest K (>= 4;
 // K = 2 and deeper unrolling measured slower on the 64^3 finest level) that
-// still gives every SM 32 warps
-static int pick_k(int slices, int num_sms) {
+// still gives every SM 32 warps, at most kmax
+static int pick_k(int slices, int num_sms, int kmax = 16) {
   static int kmin = -1;
   if (kmin < 0) {
     const char *e = getenv("PMG_SELL_KMIN");
@@ -347,7 +347,7 @@ static int pick_k(int slices, int num_sms) {
   }
   const long want = 32L * num_sms;  // warps to keep the load pipes busy
   int k = kmin;
-  while (k < 16 && (long)slices * k < want) k *= 2;
+  while (k < kmax && (long)slices * k < want) k *= 2;
   return k;
 }
 
@@ -502,7 +502,11 @@ int sell_ssor(cudaStream_t s, const Level &L, const T *f, T *x, double omega, in
       const int c = pass == 0 ? cc : nc - 1 - cc;
       const int s0 = L.sell_group[c], s1 = L.sell_group[c + 1];
       if (s1 <= s0) continue;
-      const int k = pick_k(s1 - s0, num_sms);
+      // at most 8 warps per slice in FP32, 16 in FP64: the short colours of
+      // levels 2-3 (42 and 318 slices), measured on the 64^3 bench: FP32
+      // V-cycle 3.69 -> 3.61 ms with 8 (4: 3.96 ms); FP64 V-cycle 5.18 ->
+      // 5.57 ms with 8
+      const int k = pick_k(s1 - s0, num_sms, sizeof(T) == 4 ? 8 : 16);
       cudaError_t e;
 #define PMG_GS(K_)                                                                                              \
   launch_pdl(k_sell_gs<T, K_>, dim3(slice_grid<T>(s1 - s0, num_sms, K_)), dim3(32 * K_), 0, s, s0, s1,           \
