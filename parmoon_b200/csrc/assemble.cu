@@ -16,7 +16,10 @@
 //     matrix and accumulates all NLOC rows in registers;
 //   * the element -> CSR slot map (precomputed once per mesh by binary search
 //     in the sorted rows, replacing the linear search of AssembleMat3D.C:795-817)
-//     turns the scatter into plain loads/stores.
+//     turns the scatter into plain loads/stores;
+//   * or, the row gather: the local matrices of all cells in one launch, then
+//     one pass over the CSR rows, each summed from its cells' local rows in
+//     colour order (the scatter's order: the same bits) and written once.
 #include "pmg_internal.h"
 #include "fe_tables.h"
 #include <cstdio>
