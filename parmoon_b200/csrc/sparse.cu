@@ -250,8 +250,18 @@ __global__ void __launch_bounds__(RED_THREADS) k_dot(size_t n, const double *__r
   __shared__ double sh[RED_THREADS / 32];
   __shared__ bool last;
   double s = 0;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    s += a[i] * b[i];
+  // four independent elements per thread and round (more loads in flight)
+  const size_t st = (size_t)gridDim.x * blockDim.x;
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + 3 * st < n; i += 4 * st) {
+    const double a0 = a[i], a1 = a[i + st], a2 = a[i + 2 * st], a3 = a[i + 3 * st];
+    const double b0 = b[i], b1 = b[i + st], b2 = b[i + 2 * st], b3 = b[i + 3 * st];
+    s += a0 * b0;
+    s += a1 * b1;
+    s += a2 * b2;
+    s += a3 * b3;
+  }
+  for (; i < n; i += st) s += a[i] * b[i];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
@@ -292,7 +302,24 @@ __global__ void __launch_bounds__(RED_THREADS) k_mgs_step(size_t n, const double
   const double al = *hk;
   const bool self = u == w;
   double s = 0;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+  // four independent elements per thread and round (more loads in flight)
+  const size_t st = (size_t)gridDim.x * blockDim.x;
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + 3 * st < n; i += 4 * st) {
+    double wv[4], uv[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) wv[q] = w[i + q * st] - al * __ldg(vk + i + q * st);
+    if (!self) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) uv[q] = u[i + q * st];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      w[i + q * st] = wv[q];
+      s += wv[q] * (self ? wv[q] : uv[q]);
+    }
+  }
+  for (; i < n; i += st) {
     const double wi = w[i] - al * __ldg(vk + i);
     w[i] = wi;
     s += wi * (self ? wi : u[i]);
