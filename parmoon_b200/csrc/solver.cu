@@ -877,8 +877,12 @@ int solve(Handle &h, double *sol_host, const double *rhs_host, pmg_solve_stats *
         PMG_CUDA(cudaEventRecord(h.ev[8], s));
         vc_timed = true;
       }
+      // w = A z_i.  The solve copy holds no Dirichlet columns, and none are
+      // needed: the start vector carries the Dirichlet values (copied above),
+      // so the residual and every Krylov vector are exactly 0 on the
+      // Dirichlet rows (identity rows), and every smoother copies f_D = 0
+      // into x_D, so z_i is exactly 0 there too and A_aD z_D adds nothing
       PMG_TRY(sell_spmv<double>(s, F, zi, nullptr, w, 0, h.num_sms));
-      PMG_TRY(dirichlet_cols<double>(s, F, zi, w, true));  // w = A z_i with the Dirichlet columns (z_D = 0 here)
       double *Hc = Hd + (size_t)i * (m + 1);
       // modified Gram-Schmidt (FgmresIte.C): h_k = w.v_k, w -= h_k v_k for
       // k = 0..i, then h_{i+1}^2 = w.w; each update fused with the next product
