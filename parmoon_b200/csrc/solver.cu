@@ -579,11 +579,12 @@ static int vcycle(Handle &h, int i, bool learned) {
   using PT = Prec<T>;
   if (!learned && i >= 1 && i == h.cc_top) return coarse_cycle<T>(h, i);
   // The solve copy of the matrix leaves out the active rows' Dirichlet
-  // columns: on the level the cycle enters, fold them into the right-hand
-  // side (f_a -= A_aD f_D; the smoother keeps x_D = f_D).  Coarser levels need
-  // nothing: the restriction writes 0 into their Dirichlet rows.  The
-  // coarsest-level solves (dense or iterative) read the full CSR rows themselves.
-  if (i == (int)h.lv.size() - 1 && i >= 1) PMG_TRY(dirichlet_cols<T>(s, L, PT::f(L), PT::f(L)));
+  // columns.  The cycle's input has f_D = 0 (an FGMRES vector is exactly 0 on
+  // the Dirichlet rows; pmg_vcycle folds A_aD v_D into the active rows first
+  // and passes f_D = 0 on), so those columns contribute nothing, and the
+  // smoothers keep x_D = f_D = 0.  Coarser levels: the restriction writes 0
+  // into their Dirichlet rows.  The coarsest-level solves (dense or iterative)
+  // read the full CSR rows themselves.
   if (i == 0) {
     if (h.prm.coarse_smoother == PMG_COARSE_DIRECT) {
       PMG_CUDA(launch_pdl(k_coarse_rhs<T>, dim3((L.N * 32 + 255) / 256), dim3(256), 0, s, L.N, L.Na,
@@ -1237,7 +1238,17 @@ extern "C" int pmg_vcycle(pmg_handle hh, const double *v_dev, double *z_dev) {
   if (!h || !v_dev || !z_dev) return PMG_ERR_ARG;
   PMG_TRY(pmg::prepare_levels(*h));
   PMG_TRY(pmg::capture_vcycle(*h));
-  PMG_TRY(pmg::precondition(*h, v_dev, z_dev, h->prm.smoother == PMG_SMOOTHER_LEARNED));
+  // the cycle takes f_D = 0: fold the Dirichlet part of v into the active
+  // rows in FP64 (f_a = v_a - A_aD v_D, f_D = 0), the cycle then keeps
+  // z_D = v_D as the smoothers' x_D = f_D did
+  pmg::Level &F = h->lv.back();
+  PMG_TRY(h->w.alloc(std::max<size_t>(h->w.n, (size_t)F.N)));
+  double *f = h->w.p;
+  PMG_CUDA(cudaMemcpyAsync(f, v_dev, sizeof(double) * F.N, cudaMemcpyDeviceToDevice, h->stream));
+  PMG_TRY(pmg::dirichlet_cols<double>(h->stream, F, v_dev, f, false));
+  PMG_CUDA(cudaMemsetAsync(f + F.Na, 0, sizeof(double) * (F.N - F.Na), h->stream));
+  PMG_TRY(pmg::precondition(*h, f, z_dev, h->prm.smoother == PMG_SMOOTHER_LEARNED));
+  PMG_TRY(pmg::copy_dirichlet(h->stream, F.Na, F.N, v_dev, z_dev));
   PMG_CUDA(cudaStreamSynchronize(h->stream));
   return pmg::coarse_cycle_check(*h);
 }
