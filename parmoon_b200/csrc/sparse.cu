@@ -181,9 +181,10 @@ __global__ void __launch_bounds__(256) k_prolong_add(int Naf, const int *__restr
 
 template <typename T>
 int restrict_defect(cudaStream_t s, const Level &Lf, const Level &Lc, const T *rval, const T *d, T *fc, T *xc) {
-  // R = P^T has up to 27 (Q1) / 125 (Q2) entries per coarse row
-  int g = grid_for(Lc.N, 16, 148);
-  PMG_CUDA(launch_pdl(k_restrict<16, T>, dim3(g), dim3(256), 0, s, Lc.N, Lc.Na, (const int *)Lf.rrp.p,
+  // R = P^T has up to 27 (Q1) / 125 (Q2) entries per coarse row; 8 lanes a
+  // row (64^3 Q2 FP32 V-cycle: 16 lanes 3.57 ms, 8 lanes 3.56, 32 lanes 3.58)
+  int g = grid_for(Lc.N, 8, 148);
+  PMG_CUDA(launch_pdl(k_restrict<8, T>, dim3(g), dim3(256), 0, s, Lc.N, Lc.Na, (const int *)Lf.rrp.p,
                       (const int *)Lf.rcol.p, rval, d, fc, xc));
   count_launches(1);
   PMG_CUDA(cudaGetLastError());
@@ -191,8 +192,10 @@ int restrict_defect(cudaStream_t s, const Level &Lf, const Level &Lc, const T *r
 }
 template <typename T>
 int prolongate_add(cudaStream_t s, const Level &Lf, const T *pval, const T *xc, T *xf, double damp) {
-  int g = grid_for(Lf.Na, 8, 148);
-  PMG_CUDA(launch_pdl(k_prolong_add<8, T>, dim3(g), dim3(256), 0, s, Lf.Na, (const int *)Lf.prp.p,
+  // 4 lanes a fine row (64^3 Q2 FP32 V-cycle: 8 lanes 3.53 ms, 4 lanes 3.47,
+  // 2 lanes 3.46-3.47, 16 lanes 3.64)
+  int g = grid_for(Lf.Na, 4, 148);
+  PMG_CUDA(launch_pdl(k_prolong_add<4, T>, dim3(g), dim3(256), 0, s, Lf.Na, (const int *)Lf.prp.p,
                       (const int *)Lf.pcol.p, pval, xc, xf, (T)damp));
   count_launches(1);
   PMG_CUDA(cudaGetLastError());
