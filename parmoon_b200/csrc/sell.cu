@@ -392,10 +392,10 @@ template int dirichlet_cols<double>(cudaStream_t, const Level &, const double *,
 
 // grid of a SELL launch: one CTA per slice up to a cap, beyond which CTAs loop
 // over slices (loading the next slice's first chunk before the reduction).
-// Measured on the 64^3 Q2 finest level (K = 4): a full FP64 product is fastest
-// with one CTA per slice (0.298 ms against 0.319 ms at 64 CTAs per SM), FP32
-// at 128 CTAs per SM (0.203 / 0.212 ms); a colour sweep stays below the cap.
-// PMG_SELL_CTAS_PER_SM overrides the cap.
+// Measured on the 64^3 Q2 finest level (K = 4, 4 / 8 column steps per chunk):
+// 256 CTAs per SM, FP64 product 0.247 ms (64: 0.268, 1024: 0.252, the earlier
+// 512: 0.252), FP32 defect 0.162 ms (64: 0.173, 128: 0.164, 1024: 0.165); a
+// colour sweep stays below the cap.  PMG_SELL_CTAS_PER_SM overrides the cap.
 template <typename T>
 static int slice_grid(int nslices, int num_sms, int k) {
   static int cps = -1;
@@ -403,7 +403,7 @@ static int slice_grid(int nslices, int num_sms, int k) {
     const char *e = getenv("PMG_SELL_CTAS_PER_SM");
     cps = e ? std::max(0, atoi(e)) : 0;
   }
-  const long cap = cps ? (long)num_sms * cps : (long)num_sms * ((sizeof(T) == 8 ? 2048 : 512) / k);
+  const long cap = (long)num_sms * (cps ? cps : 256);
   return (int)std::max(1L, std::min((long)nslices, cap));
 }
 
