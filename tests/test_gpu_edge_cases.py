@@ -49,6 +49,7 @@ def test_params_and_inputs_are_checked(pmg):
     h = pmg.Handle(2)
     assert code_of(lambda: h.set_params(pmg.default_params(restart=61))) == pmg.ERR_ARG
     assert code_of(lambda: h.set_params(pmg.default_params(assembly_kernel=3))) == pmg.ERR_ARG
+    assert code_of(lambda: h.set_params(pmg.default_params(assembly_scatter=3))) == pmg.ERR_ARG
     pmg.load_hierarchy(h, levels)
     F = levels[-1]
     bad = np.zeros(F["N"] - F["active_bound"])
