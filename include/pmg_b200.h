@@ -170,6 +170,10 @@ typedef struct pmg_handle_s *pmg_handle;
 
 /* ------------------------------------------------------------ lifecycle */
 void        pmg_default_params(pmg_params *p);
+/* sizeof(pmg_params) of this build of the library: pmg_default_params writes
+ * that many bytes, so a program compiled against another revision of this
+ * header (sizeof differs) must check it before the first call */
+int         pmg_params_size(void);
 const char *pmg_last_error(void);
 int         pmg_device_count(int *n);
 

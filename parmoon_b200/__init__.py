@@ -107,6 +107,9 @@ def _out_f64(out, n):
 
 def default_params(**kw):
     p = Params()
+    if lib().pmg_params_size() != ctypes.sizeof(Params):
+        raise RuntimeError(f"libpmg_b200 pmg_params is {lib().pmg_params_size()} bytes, the Params mirror "
+                           f"{ctypes.sizeof(Params)}: the binding and the library are out of step")
     lib().pmg_default_params(ctypes.byref(p))
     for k, v in kw.items():
         setattr(p, k, v)

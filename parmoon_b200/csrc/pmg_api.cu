@@ -168,6 +168,8 @@ int pmg_device_count(int *n) {
   return PMG_OK;
 }
 
+int pmg_params_size(void) { return (int)sizeof(pmg_params); }
+
 void pmg_default_params(pmg_params *p) {
   if (!p) return;
   memset(p, 0, sizeof(*p));

@@ -36,6 +36,11 @@ TPmgSystemCD3D::TPmgSystemCD3D(int N_levels, TFESpace3D **fespaces, double **sol
   }
   // solver knobs from TDatabase::ParamDB (Database.C:660-780)
   pmg_params p;
+  // a program built against another revision of pmg_b200.h: rebuild it
+  if (pmg_params_size() != (int)sizeof(pmg_params)) {
+    check(PMG_ERR_ARG, "pmg_params_size (libpmg_b200 and this program disagree on sizeof(pmg_params))");
+    return;  // no handle: every later call reports the status
+  }
   pmg_default_params(&p);
   TParamDB *db = TDatabase::ParamDB;
   // 1 Jacobi, 2 SOR, 3 SSOR; the sequential reference runs SOR for the codes

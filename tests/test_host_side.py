@@ -179,3 +179,12 @@ def test_output_arrays_are_checked_and_used_in_place():
     for bad in (np.zeros(9), np.zeros(10, dtype=np.float32), np.zeros(20)[::2], [0.0] * 10):
         with pytest.raises(ValueError):
             P._out_f64(bad, 10)
+
+
+def test_params_mirror_matches_the_library():
+    """The ctypes Params mirror has the library's sizeof(pmg_params): a field
+    added on one side only (pmg_default_params writes the whole struct) shows
+    up here rather than as a corrupted stack."""
+    import ctypes
+    import parmoon_b200 as P
+    assert P.lib().pmg_params_size() == ctypes.sizeof(P.Params)
