@@ -188,3 +188,39 @@ def test_params_mirror_matches_the_library():
     import ctypes
     import parmoon_b200 as P
     assert P.lib().pmg_params_size() == ctypes.sizeof(P.Params)
+
+
+def test_host_builders_reject_bad_input():
+    """The host set-up helpers (no GPU) return status codes for bad input:
+    unknown elements, empty meshes, dofs or parents out of range, a jittered
+    N_Q1 mesh, and the N_Q1 space where only the cell-averaged transfer
+    applies."""
+    import parmoon_b200 as P
+    lib = P.lib()
+    i = ctypes.c_int
+    nc, N, nl = i(), i(), i()
+    assert lib.pmg_struct_sizes(99, 4, ctypes.byref(nc), ctypes.byref(N), ctypes.byref(nl)) == P.ERR_ARG
+    assert lib.pmg_struct_sizes(P.Q1_HEX, 0, ctypes.byref(nc), ctypes.byref(N), ctypes.byref(nl)) == P.ERR_ARG
+    with pytest.raises(P.PmgError) as e:
+        P.struct_level(P.NQ1_HEX, 2, jitter=0.1)
+    assert e.value.code == P.ERR_UNSUPPORTED
+    # a pattern whose cells name a dof beyond the level
+    ed = np.array([0, 1, 2, 7], dtype=np.int32)
+    rp = np.zeros(5, dtype=np.int32)
+    rc = lib.pmg_struct_csr(1, 4, ed.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), 4, 4,
+                            rp.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), None)
+    assert rc == P.ERR_ARG
+    # N_Q1 has no node lattice: the lattice transfer refuses it
+    L = P.struct_level(P.NQ1_HEX, 2)
+    assert L["colors"] is None
+    with pytest.raises(P.PmgError) as e:
+        P.struct_prolongation(P.NQ1_HEX, 1, np.zeros(1, dtype=np.int32), np.zeros(1, dtype=np.int32))
+    assert e.value.code == P.ERR_UNSUPPORTED
+    # a fine cell whose parent is not a coarse cell
+    C, F = P.struct_level(P.Q1_HEX, 1), P.struct_level(P.Q1_HEX, 2)
+    parents = P.struct_parents(2)
+    parents[3] = 5
+    with pytest.raises(P.PmgError) as e:
+        P.cell_prolongation(P.Q1_HEX, C["elem_dof"], C["cell_vert"], C["N"], P.Q1_HEX, F["elem_dof"],
+                            F["cell_vert"], parents, F["N"])
+    assert e.value.code == P.ERR_ARG
