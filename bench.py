@@ -740,7 +740,7 @@ def main():
         import torch
         import torch.distributed as tdist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         bench_dd(args, rank, world, tdist)
         tdist.barrier()
         tdist.destroy_process_group()
@@ -750,7 +750,7 @@ def main():
         import torch
         import torch.distributed as tdist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
     elif world > 1:
         pass
